@@ -1,0 +1,12 @@
+"""fargo3d_b200 -- FARGO3D's hydro time step on NVIDIA B200 (sm_100a).
+
+The per-cell work runs in hand-written CUDA kernels behind a C-ABI
+(include/fargo_b200.h, libfargo_b200.so built in-tree); this package is the
+Python host mirror of the reference's run loop over that ABI.
+"""
+from .setups import DiskConfig, Planet, config_fargo2d, config_p3disof, initial_state, geometry
+from .disk import Disk
+from ._abi import FargoError
+
+__all__ = ["DiskConfig", "Planet", "config_fargo2d", "config_p3disof", "initial_state", "geometry",
+           "Disk", "FargoError"]

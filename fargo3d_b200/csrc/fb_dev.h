@@ -1,0 +1,86 @@
+/*
+ * fb_dev.h -- plain-C description of one disk's device state, shared by the C
+ * host driver (fb_host.c) and the CUDA launchers (fb_kernels_*.cu).
+ */
+#ifndef FB_DEV_H
+#define FB_DEV_H
+
+#include "fb_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Geometry tables on the device: one double set and, for FP32 disks, a float
+ * mirror of the same layout (same order of fields as FbGeom<T>). */
+typedef struct {
+  const void *xmin, *ymin, *zmin, *xmed, *ymed, *zmed, *invdiffxmed;
+  const void *sxi, *sxj, *syj, *szj, *sxk, *syk, *szk, *invvj;
+  const void *sin_zmed, *cos_zmed, *sin_zmin, *cos_zmin;
+  const void *cos_xmed, *sin_xmed;
+  const void *visc_j, *viscm_j, *tau_j;
+} fb_geom_dev;
+
+typedef struct {
+  void *rho, *cs, *vx, *vy, *vz;
+  void *vxt, *vyt, *vzt;
+  void *mpx, *mmx, *mpy, *mmy, *mpz, *mmz;   /* transport buffers (set A) */
+  void *rho_a;                               /* transported density (set A) */
+  void *mpx_b, *mmx_b, *mpy_b, *mmy_b, *mpz_b, *mmz_b, *rho_b;  /* set B (3D) */
+  double *vxmed, *vxmed_t;
+  int *nshift;
+  void *rho0, *vx0, *vy0, *vz0;
+  int dust;
+} fb_fluid_dev;
+
+/* Per-step scalars (host-computed in FP64 mode, device-computed in the
+ * batched mode).  Mirrors FbStepScalars in fb_common.cuh. */
+typedef struct {
+  double dt;
+  double omegaframe, omegaframe0, domega;
+  double nu, alpha, cfl;
+  int nplanets;
+  double px[FB_MAXPLANETS], py[FB_MAXPLANETS], pz[FB_MAXPLANETS];
+  double pmass[FB_MAXPLANETS], psmooth2[FB_MAXPLANETS], pdist3[FB_MAXPLANETS];
+  int indirect_term;
+} fb_scalars;
+
+typedef struct {
+  int nx, ny, nz, sy, sz, pitch;
+  long long stride;
+  int is3d, spherical, alpha_visc;
+  int precision;          /* FB_FP64 / FB_FP32 */
+  double xlen;            /* XMAX - XMIN */
+  double ymin_p, ymax_p, zmin_p, zmax_p;  /* YMIN, YMAX, ZMIN, ZMAX */
+  double y_inf, y_sup, z_inf, z_sup;       /* Stockholm ramp limits */
+  double cfl, mindx;
+  int stockholm;
+  double aspectratio, sigmaslope, flaringindex;
+  fb_geom_dev geom;       /* precision of the disk */
+  fb_geom_dev geomd;      /* always double */
+  fb_fluid_dev fl[FB_MAXFLUIDS];
+  int nfluids;
+  double *dtmin;          /* device scalar: CFL minimum (bits as u64 min) */
+  fb_scalars *scal_dev;   /* device copy of the per-step scalars */
+  double *rowmin;         /* per-ring scratch */
+  double *bnd_tab;        /* boundary factor tables (double) */
+  int bnd_tab_n;
+  double *ramps;          /* Stockholm ramps: [sy] radial, [sz] zmed, [sz] zmin */
+} fb_disk_dev;
+
+/* Launchers (fb_kernels_f64.cu / fb_kernels_f32.cu). Return cudaError_t. */
+#define FB_DECL_LAUNCHERS(SUF)                                                       \
+  int fb_launch_rowsum_##SUF(const fb_disk_dev *d, int fluid, int which, void *stream); \
+  int fb_launch_cfl_##SUF(const fb_disk_dev *d, int fluid, void *stream);           \
+  int fb_launch_sources_##SUF(const fb_disk_dev *d, int fluid, void *stream);       \
+  int fb_launch_bnd_##SUF(const fb_disk_dev *d, int fluid, int vtemp, void *stream); \
+  int fb_launch_transport_##SUF(const fb_disk_dev *d, int fluid, void *stream);     \
+  int fb_launch_newvel_##SUF(const fb_disk_dev *d, int fluid, void *stream);
+
+FB_DECL_LAUNCHERS(f64)
+FB_DECL_LAUNCHERS(f32)
+
+#ifdef __cplusplus
+}
+#endif
+#endif

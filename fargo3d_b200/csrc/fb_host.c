@@ -1,0 +1,711 @@
+/*
+ * fb_host.c -- host side of the B200 hydro step (C99 + CUDA runtime API).
+ *
+ * Owns a disk's device memory, the mesh tables, the planetary system and the
+ * order of the stage kernels within one hydro step (main.c:361-448 of the
+ * reference).  The scalar work of a step -- the CFL minimum's clipping to the
+ * DT interval, the planets' RK5 orbit, the frame rotation -- runs here in
+ * FP64, as it does in the reference (potential.c:10-49); everything per cell
+ * runs on the GPU.  There is no CPU path for the per-cell work.
+ */
+#include <math.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cuda_runtime_api.h>
+
+#include "fargo_b200.h"
+#include "fb_dev.h"
+
+#define NG 3
+#define G 1.0
+#define MSTAR 1.0
+#define R0 1.0
+#define SMALLTIME (1e-10 * sqrt(R0 * R0 * R0 / (G * MSTAR)))
+#define MAXALLOC 96
+
+static __thread char g_err[512];
+
+const char *fb_last_error(void) { return g_err; }
+
+static int fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CU(call)                                                                 \
+  do {                                                                           \
+    cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess)                                                       \
+      return fail(FB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+  } while (0)
+
+#define LCH(call)                                                                \
+  do {                                                                           \
+    int e_ = (call);                                                             \
+    if (e_ != 0)                                                                 \
+      return fail(FB_ERR_CUDA, "%s failed: %s", #call,                           \
+                  cudaGetErrorString((cudaError_t)e_));                          \
+  } while (0)
+
+struct fb_disk {
+  fb_params p;
+  fb_disk_dev d;
+  int device;
+  cudaStream_t stream;
+  size_t esz;                   /* element size of the fields */
+  long long ncell;              /* stored cells per field */
+  /* host geometry (double) */
+  double *xmin, *ymin, *zmin, *xmed, *ymed, *zmed, *invdiffxmed;
+  double *sxi, *sxj, *syj, *szj, *sxk, *syk, *szk, *invvj;
+  double mindx;
+  /* planetary system (psys.c) */
+  int np;
+  double px[FB_MAXPLANETS], py[FB_MAXPLANETS], pz[FB_MAXPLANETS];
+  double pvx[FB_MAXPLANETS], pvy[FB_MAXPLANETS], pvz[FB_MAXPLANETS], pmass[FB_MAXPLANETS];
+  int pfeelothers[FB_MAXPLANETS];
+  double xmark, ymark, xaxis_rot;
+  /* scalars */
+  double omegaframe, omegaframe0, domega, phys_time, dtemp, last_dt;
+  long long step_count;
+  fb_scalars sc;
+  double *h_dtmin;              /* pinned */
+  void *allocs[MAXALLOC];
+  int nalloc;
+};
+
+/* ------------------------------------------------------------------------ */
+static int dalloc(fb_disk *D, void **p, size_t bytes) {
+  cudaError_t e;
+  if (D->nalloc >= MAXALLOC) return fail(FB_ERR_NOMEM, "too many device allocations");
+  e = cudaMalloc(p, bytes ? bytes : 16);
+  if (e != cudaSuccess) return fail(FB_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  D->allocs[D->nalloc++] = *p;
+  cudaMemset(*p, 0, bytes ? bytes : 16);
+  return FB_OK;
+}
+
+/* upload a double table, converted to the disk's precision when asked */
+static int upload(fb_disk *D, const void **dst, const double *src, int n, int as_float) {
+  void *p;
+  int rc;
+  if (as_float) {
+    float *tmp = (float *)malloc(sizeof(float) * (n ? n : 1));
+    int i;
+    for (i = 0; i < n; i++) tmp[i] = (float)src[i];
+    rc = dalloc(D, &p, sizeof(float) * n);
+    if (rc) { free(tmp); return rc; }
+    cudaMemcpy(p, tmp, sizeof(float) * n, cudaMemcpyHostToDevice);
+    free(tmp);
+  } else {
+    rc = dalloc(D, &p, sizeof(double) * n);
+    if (rc) return rc;
+    cudaMemcpy(p, src, sizeof(double) * n, cudaMemcpyHostToDevice);
+  }
+  *dst = p;
+  return FB_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Mesh: InitSpace (LowTasks.c:300-383) and InitSurfaces (LowTasks.c:466-563) */
+static void mesh(fb_disk *D) {
+  const fb_params *p = &D->p;
+  int i, j, k, sx = p->nx, sy = D->d.sy, sz = D->d.sz, is3d = D->d.is3d;
+  double dx = (p->xmax - p->xmin) / p->nx, dy = (p->ymax - p->ymin) / p->ny;
+  double dz = is3d ? (p->zmax - p->zmin) / p->nz : 0.0;
+  if (p->log_spacing) {
+    dy = (log(p->ymax) - log(p->ymin)) / p->ny;
+    for (j = 0; j < sy + 1; j++) D->ymin[j] = exp(log(p->ymin) + dy * (j - NG));
+  } else {
+    for (j = 0; j < sy + 1; j++) D->ymin[j] = p->ymin + dy * (j - NG);
+  }
+  for (k = 0; k < sz + 1; k++) D->zmin[k] = is3d ? p->zmin + dz * (k - NG) : 0.0;
+  for (i = 0; i < sx + 1; i++) D->xmin[i] = p->xmin + dx * i;
+  for (i = 0; i < sx; i++) D->xmed[i] = 0.5 * (D->xmin[i + 1] + D->xmin[i]);
+  for (j = 0; j < sy; j++) D->ymed[j] = 0.5 * (D->ymin[j + 1] + D->ymin[j]);
+  for (k = 0; k < sz; k++) D->zmed[k] = 0.5 * (D->zmin[k + 1] + D->zmin[k]);
+  for (i = 1; i < sx; i++) D->invdiffxmed[i] = 1. / (D->xmed[i] - D->xmed[i - 1]);
+  D->invdiffxmed[0] = 1. / (D->xmed[0] - (D->xmed[p->nx - 1] - (p->xmax - p->xmin)));
+  for (i = 0; i < sx; i++) D->sxi[i] = D->xmin[i + 1] - D->xmin[i];
+  D->mindx = D->sxi[0];
+  for (i = 1; i < sx; i++)
+    if (D->sxi[i] < D->mindx) D->mindx = D->sxi[i];
+  if (!p->spherical) {
+    for (j = 0; j < sy; j++) {
+      D->sxj[j] = D->ymin[j + 1] - D->ymin[j];
+      D->syj[j] = D->ymin[j];
+      D->szj[j] = 0.5 * (D->ymin[j + 1] * D->ymin[j + 1] - D->ymin[j] * D->ymin[j]);
+      D->invvj[j] = 1.0 / D->szj[j];
+    }
+    for (k = 0; k < sz; k++) {
+      D->sxk[k] = is3d ? D->zmin[k + 1] - D->zmin[k] : 1.0;
+      D->syk[k] = D->sxk[k];
+      D->szk[k] = 1.0;
+    }
+  } else {
+    for (j = 0; j < sy; j++) {
+      D->sxj[j] = 0.5 * (D->ymin[j + 1] * D->ymin[j + 1] - D->ymin[j] * D->ymin[j]);
+      D->syj[j] = D->ymin[j] * D->ymin[j];
+      D->szj[j] = 0.5 * (D->ymin[j + 1] * D->ymin[j + 1] - D->ymin[j] * D->ymin[j]);
+      D->invvj[j] = 3. / ((D->ymin[j + 1] * D->ymin[j + 1] * D->ymin[j + 1] - D->ymin[j] * D->ymin[j] * D->ymin[j]));
+    }
+    for (k = 0; k < sz; k++) {
+      D->sxk[k] = D->zmin[k + 1] - D->zmin[k];
+      D->syk[k] = cos(D->zmin[k]) - cos(D->zmin[k + 1]);
+      D->szk[k] = sin(D->zmin[k]);
+    }
+  }
+}
+
+/* Upload the mesh and every libm-derived table the kernels read. */
+static int upload_geometry(fb_disk *D) {
+  const fb_params *p = &D->p;
+  int sx = p->nx, sy = D->d.sy, sz = D->d.sz, i, j, k, pass, rc;
+  double *t_szmed = malloc(sizeof(double) * (sz + 1)), *t_czmed = malloc(sizeof(double) * (sz + 1));
+  double *t_szmin = malloc(sizeof(double) * (sz + 1)), *t_czmin = malloc(sizeof(double) * (sz + 1));
+  double *t_cx = malloc(sizeof(double) * sx), *t_sx = malloc(sizeof(double) * sx);
+  double *t_visc = malloc(sizeof(double) * sy), *t_viscm = malloc(sizeof(double) * sy), *t_tau = malloc(sizeof(double) * sy);
+  for (k = 0; k < sz; k++) { t_szmed[k] = sin(D->zmed[k]); t_czmed[k] = cos(D->zmed[k]); }
+  for (k = 0; k < sz + 1; k++) { t_szmin[k] = sin(D->zmin[k]); t_czmin[k] = cos(D->zmin[k]); }
+  t_szmed[sz] = t_czmed[sz] = 0.0;
+  for (i = 0; i < sx; i++) { t_cx[i] = cos(D->xmed[i]); t_sx[i] = sin(D->xmed[i]); }
+  for (j = 0; j < sy; j++) {
+    t_visc[j] = sqrt(D->ymed[j] * D->ymed[j] * D->ymed[j] / (G * MSTAR));   /* visctensor_*.c alpha-nu */
+    t_viscm[j] = sqrt(D->ymin[j] * D->ymin[j] * D->ymin[j] / (G * MSTAR));
+    t_tau[j] = p->tau_damp * sqrt(D->ymed[j] * D->ymed[j] * D->ymed[j] / G / MSTAR); /* stockholm.c:134 */
+  }
+  for (pass = 0; pass < 2; pass++) {
+    /* pass 0: double tables; pass 1: the disk's precision (skipped in FP64) */
+    fb_geom_dev *g = pass == 0 ? &D->d.geomd : &D->d.geom;
+    int f = pass == 1 && D->d.precision == FB_FP32;
+    if (pass == 1 && !f) { D->d.geom = D->d.geomd; break; }
+#define UP(field, arr, n) if ((rc = upload(D, &g->field, arr, n, f))) goto out
+    UP(xmin, D->xmin, sx + 1); UP(ymin, D->ymin, sy + 1); UP(zmin, D->zmin, sz + 1);
+    UP(xmed, D->xmed, sx); UP(ymed, D->ymed, sy); UP(zmed, D->zmed, sz);
+    UP(invdiffxmed, D->invdiffxmed, sx); UP(sxi, D->sxi, sx);
+    UP(sxj, D->sxj, sy); UP(syj, D->syj, sy); UP(szj, D->szj, sy); UP(invvj, D->invvj, sy);
+    UP(sxk, D->sxk, sz); UP(syk, D->syk, sz); UP(szk, D->szk, sz);
+    UP(sin_zmed, t_szmed, sz + 1); UP(cos_zmed, t_czmed, sz + 1);
+    UP(sin_zmin, t_szmin, sz + 1); UP(cos_zmin, t_czmin, sz + 1);
+    UP(cos_xmed, t_cx, sx); UP(sin_xmed, t_sx, sx);
+    UP(visc_j, t_visc, sy); UP(viscm_j, t_viscm, sy); UP(tau_j, t_tau, sy);
+#undef UP
+  }
+  rc = FB_OK;
+out:
+  free(t_szmed); free(t_czmed); free(t_szmin); free(t_czmin); free(t_cx); free(t_sx);
+  free(t_visc); free(t_viscm); free(t_tau);
+  return rc;
+}
+
+/* Boundary-template factors (std/boundaries.txt) and Stockholm ramps
+ * (stockholm.c:113-129), tabulated with the host libm. */
+static int upload_tables(fb_disk *D) {
+  const fb_params *p = &D->p;
+  int sy = D->d.sy, sz = D->d.sz, ny = p->ny, nz = D->d.nz, s, jj, j, k, kk, rc;
+  int n = 18 + 6 * sz + 6 * sy + 6;
+  double *t = calloc(n, sizeof(double));
+  double ss = p->sigmaslope, fi = p->flaringindex, ar = p->aspectratio;
+  double *ramps;
+  for (s = 0; s < 2; s++)
+    for (jj = 0; jj < 3; jj++) {
+      int jgh = s == 0 ? jj : ny + NG + jj, jact = s == 0 ? 2 * NG - jj - 1 : ny + NG - 1 - jj;
+      double ya = D->ymed[jact], yg = D->ymed[jgh];
+      if (!D->d.is3d) {
+        t[s * 3 + jj] = pow(ya / yg, ss);                 /* KEPLERIAN2DDENS */
+        t[6 + s * 3 + jj] = sqrt(ya / yg);                /* KEPLERIAN2DVAZIM */
+        t[12 + s * 3 + jj] = 1.0;
+      } else {
+        t[s * 3 + jj] = pow(ya / yg, ss + fi + 1.);      /* KEPLERIAN3DSPHDENSRAD */
+        t[6 + s * 3 + jj] = sqrt(ya / yg);                /* KEPLERIAN3DSPHVAZIMRAD */
+        t[12 + s * 3 + jj] = (1. + (2. + ss - fi) * (ya - yg) / R0 * fi * ar * ar * pow((yg + ya) / (2. * R0), 2. * fi - 1.));
+        for (k = 0; k < sz; k++)
+          t[18 + (s * 3 + jj) * sz + k] =
+              exp(-pow(cos(D->zmed[k]), 2.) / (ar * ar) * (1. - yg / (.5 * (ya + yg))) * fi * pow(.5 * (yg + ya) / R0, -2. * fi - 1.));
+      }
+    }
+  if (D->d.is3d)
+    for (s = 0; s < 2; s++)
+      for (kk = 0; kk < 3; kk++) {
+        int kgh = s == 0 ? kk : nz + NG + kk, kact = s == 0 ? 2 * NG - kk - 1 : nz + NG - 1 - kk;
+        for (j = 0; j < sy; j++)   /* KEPLERIAN3DSPHDENSCOL */
+          t[18 + 6 * sz + (s * 3 + kk) * sy + j] =
+              pow(sin(D->zmed[kgh]) / sin(D->zmed[kact]), fi - 2. - ss + 1. / (ar * ar) * pow(D->ymed[j] / R0, -2. * fi));
+        /* KEPLERIAN3DSPHVAZIMCOL */
+        t[18 + 6 * sz + 6 * sy + s * 3 + kk] =
+            (1. + fi * cos(.5 * (D->zmed[kgh] + D->zmed[kact])) * (D->zmed[kact] - D->zmed[kgh]));
+      }
+  rc = upload(D, (const void **)&D->d.bnd_tab, t, n, 0);
+  D->d.bnd_tab_n = n;
+  free(t);
+  if (rc) return rc;
+  /* Stockholm ramps */
+  ramps = calloc(sy + 2 * sz, sizeof(double));
+  {
+    double y_inf = p->ymin * pow(p->damping_zone, 2.0 / 3.0), y_sup = p->ymax * pow(p->damping_zone, -2.0 / 3.0);
+    double z_inf, z_sup;
+    if (!p->spherical) {
+      z_inf = p->zmin + (p->zmax - p->zmin) * 0.1;
+      z_sup = p->zmax - (p->zmax - p->zmin) * 0.1;
+    } else {
+      z_inf = M_PI / 2.0 - (M_PI / 2.0 - p->zmin) * (1.0 - p->killing_bc_colatitude);
+      z_sup = M_PI / 2.0 + (M_PI / 2.0 - p->zmin) * (1.0 - p->killing_bc_colatitude);
+    }
+    for (j = 0; j < sy; j++) {
+      double r = 0.0, y = D->ymed[j];
+      if (y > y_sup) r = (y - y_sup) / (p->ymax - y_sup);
+      if (y < y_inf) r = (y_inf - y) / (y_inf - p->ymin);
+      ramps[j] = r * r;
+    }
+    for (k = 0; k < sz && D->d.is3d; k++) {
+      double rz = 0.0, rzz = 0.0, z = D->zmed[k], zm = D->zmin[k];
+      if (z > z_sup) rz = (z - z_sup) / (p->zmax - z_sup);
+      if (z < z_inf) rz = (z_inf - z) / (z_inf - p->zmin);
+      if (zm > z_sup) rzz = (zm - z_sup) / (p->zmax - z_sup);
+      if (zm < z_inf) rzz = (z_inf - zm) / (z_inf - p->zmin);
+      ramps[sy + k] = rz * rz;
+      ramps[sy + sz + k] = rzz * rzz;
+    }
+  }
+  rc = upload(D, (const void **)&D->d.ramps, ramps, sy + 2 * sz, 0);
+  free(ramps);
+  return rc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Planetary system, FP64 on the host: psys.c:141-225 (initial state),
+ * planets.c:116-190 (SV2OE), psys.c:362-415 (GetPsysInfo), psys.c:417-440
+ * (RotatePsys), runge_kutta.c (Cash-Karp RK5, 5 sub-steps per hydro step). */
+typedef struct { double e, a, M, i, phi; } orbit_t;
+
+static orbit_t orbit_of(double x, double y, double z, double vx, double vy, double vz, double m) {
+  orbit_t o;
+  double d = sqrt(x * x + y * y + z * z);
+  double hx = y * vz - z * vy, hy = z * vx - x * vz, hz = x * vy - y * vx;
+  double hhor = sqrt(hx * hx + hy * hy), h = sqrt(hx * hx + hy * hy + hz * hz);
+  double Ax, Ay, Az, E, an, cosan, sinan;
+  o.i = asin(hhor / h);
+  Ax = vy * hz - vz * hy - G * m * x / d;
+  Ay = vz * hx - vx * hz - G * m * y / d;
+  Az = vx * hy - vy * hx - G * m * z / d;
+  o.e = sqrt(Ax * Ax + Ay * Ay + Az * Az) / (G * m);
+  o.a = h * h / (G * m * (1. - o.e * o.e));
+  E = (o.e != 0.0) ? acos((1.0 - d / o.a) / o.e) : 0.0;
+  if (x * vx + y * vy + z * vz < 0) E = -E;
+  if (isnan(E)) E = (d < o.a) ? 0.0 : M_PI;
+  o.M = E - o.e * sin(E);
+  an = 0.0;
+  if (fabs(o.i) > 1e-5) {
+    an = atan2(hy, hx) + M_PI * .5;
+    if (an > 2.0 * M_PI) an -= 2.0 * M_PI;
+  }
+  cosan = cos(an); sinan = sin(an);
+  (void)cosan; (void)sinan;
+  o.phi = (Ax * Ax + Ay * Ay > 0.0) ? atan2(Ay, Ax) : atan2(y, x);
+  return o;
+}
+
+enum { PS_GET = 0, PS_MARK = 1, PS_FREQUENCY = 2 };
+static double psys_info(fb_disk *D, int action) {
+  double x = D->px[0], y = D->py[0], z = D->pz[0], vx = D->pvx[0], vy = D->pvy[0], vz = D->pvz[0];
+  double m = D->pmass[0] + MSTAR, xc = x, yc = y, d1, d2, cross;
+  orbit_t o = orbit_of(x, y, z, vx, vy, vz, m);
+  if (D->p.frame == FB_FRAME_GUIDING) {
+    xc = o.a * cos(o.M + o.phi) * cos(o.i);
+    yc = o.a * sin(o.M + o.phi) * cos(o.i);
+  }
+  if (o.e < 1e-8) { xc = x; yc = y; }
+  if (action == PS_MARK) { D->xmark = xc; D->ymark = yc; return 0.0; }
+  if (action == PS_GET) {
+    x = xc; y = yc;
+    d2 = sqrt(x * x + y * y);
+    d1 = sqrt(D->xmark * D->xmark + D->ymark * D->ymark);
+    cross = D->xmark * y - x * D->ymark;
+    D->xmark = x; D->ymark = y;
+    return asin(cross / (d1 * d2));
+  }
+  if (D->p.frame == FB_FRAME_GUIDING) return sqrt(G * m / pow(o.a, 3.0));
+  return (x * vy - y * vx) / (x * x + y * y);
+}
+
+static void rotate(fb_disk *D, double angle) {
+  int i;
+  double s = sin(angle), c = cos(angle), xt, yt;
+  D->xaxis_rot += angle;
+  if (D->xaxis_rot >= 2.0 * M_PI) D->xaxis_rot -= 2.0 * M_PI;
+  if (D->xaxis_rot < 0.0) D->xaxis_rot += 2.0 * M_PI;
+  for (i = 0; i < D->np; i++) {
+    xt = D->px[i]; yt = D->py[i];
+    D->px[i] = xt * c + yt * s; D->py[i] = -xt * s + yt * c;
+    xt = D->pvx[i]; yt = D->pvy[i];
+    D->pvx[i] = xt * c + yt * s; D->pvy[i] = -xt * s + yt * c;
+  }
+}
+
+static void nbody_deriv(const fb_disk *D, const double *q, const double *ms, double *der, int n, double dt) {
+  const double *x = q, *y = q + n, *z = q + 2 * n, *vx = q + 3 * n, *vy = q + 4 * n, *vz = q + 5 * n;
+  double dist[FB_MAXPLANETS], coef, dd;
+  int i, j;
+  for (i = 0; i < n; i++) dist[i] = sqrt(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+  for (i = 0; i < n; i++) {
+    der[i] = vx[i]; der[i + n] = vy[i]; der[i + 2 * n] = vz[i];
+    coef = -G * MSTAR / dist[i] / dist[i] / dist[i];
+    der[i + 3 * n] = coef * x[i]; der[i + 4 * n] = coef * y[i]; der[i + 5 * n] = coef * z[i];
+    for (j = 0; j < n; j++) {
+      if (D->p.indirect_term) {
+        coef = G * ms[j] / dist[j] / dist[j] / dist[j];
+        der[i + 3 * n] -= coef * x[j]; der[i + 4 * n] -= coef * y[j]; der[i + 5 * n] -= coef * z[j];
+      }
+      if (j != i && D->pfeelothers[i]) {
+        dd = (x[i] - x[j]) * (x[i] - x[j]) + (y[i] - y[j]) * (y[i] - y[j]) + (z[i] - z[j]) * (z[i] - z[j]);
+        dd = sqrt(dd);
+        coef = G * ms[j] / dd / dd / dd;
+        der[i + 3 * n] += coef * (x[j] - x[i]); der[i + 4 * n] += coef * (y[j] - y[i]);
+        der[i + 5 * n] += coef * (z[j] - z[i]);
+      }
+    }
+  }
+  for (i = 0; i < 6 * n; i++) der[i] *= dt;
+}
+
+static void nbody_rk5(fb_disk *D, double dt) {
+  enum { M6 = 6 * FB_MAXPLANETS };
+  int n = D->np, i;
+  double q0[M6] = {0}, q1[M6] = {0}, ms[FB_MAXPLANETS] = {0};
+  double k1[M6] = {0}, k2[M6] = {0}, k3[M6] = {0}, k4[M6] = {0}, k5[M6] = {0}, k6[M6] = {0};
+  if (!n) return;
+  for (i = 0; i < n; i++) {
+    q0[i] = D->px[i]; q0[i + n] = D->py[i]; q0[i + 2 * n] = D->pz[i];
+    q0[i + 3 * n] = D->pvx[i]; q0[i + 4 * n] = D->pvy[i]; q0[i + 5 * n] = D->pvz[i];
+    ms[i] = D->pmass[i];
+  }
+#define STAGE(c1, c2, c3, c4, c5) \
+  for (i = 0; i < 6 * n; i++) q1[i] = q0[i] + c1 * k1[i] + c2 * k2[i] + c3 * k3[i] + c4 * k4[i] + c5 * k5[i]
+  nbody_deriv(D, q0, ms, k1, n, dt);
+  STAGE(0.2, 0.0, 0.0, 0.0, 0.0);
+  nbody_deriv(D, q1, ms, k2, n, dt);
+  STAGE(0.075, 0.225, 0.0, 0.0, 0.0);
+  nbody_deriv(D, q1, ms, k3, n, dt);
+  STAGE(0.3, -0.9, 1.2, 0.0, 0.0);
+  nbody_deriv(D, q1, ms, k4, n, dt);
+  STAGE(-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0.0);
+  nbody_deriv(D, q1, ms, k5, n, dt);
+  STAGE(1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0);
+  nbody_deriv(D, q1, ms, k6, n, dt);
+#undef STAGE
+  for (i = 0; i < 6 * n; i++)
+    q1[i] = (q0[i] + 37.0 / 378.0 * k1[i] + 250.0 / 621.0 * k3[i] + 125.0 / 594.0 * k4[i] + 512.0 / 1771.0 * k6[i]);
+  for (i = 0; i < n; i++) {
+    D->px[i] = q1[i]; D->py[i] = q1[i + n]; D->pz[i] = q1[i + 2 * n];
+    D->pvx[i] = q1[i + 3 * n]; D->pvy[i] = q1[i + 4 * n]; D->pvz[i] = q1[i + 5 * n];
+  }
+}
+
+/* planet terms of Potential_cpu (potential.c:137-160) that do not depend on
+ * the cell: smoothing^2 and the cube of the star-planet distance */
+static void planet_scalars(fb_disk *D) {
+  int n;
+  D->sc.nplanets = D->np;
+  D->sc.indirect_term = D->p.indirect_term;
+  for (n = 0; n < D->np; n++) {
+    double mp = D->pmass[n] * 1.0, pd, rroche, s;
+    pd = sqrt(D->px[n] * D->px[n] + D->py[n] * D->py[n] + D->pz[n] * D->pz[n]);
+    rroche = pd * pow((1.0 / 3.0 * mp / MSTAR), 1.0 / 3.0);
+    if (D->p.roche_smoothing != 0) s = rroche * D->p.roche_smoothing;
+    else s = D->p.aspectratio * pow(pd / R0, D->p.flaringindex) * pd * D->p.thickness_smoothing;
+    D->sc.px[n] = D->px[n]; D->sc.py[n] = D->py[n]; D->sc.pz[n] = D->pz[n];
+    D->sc.pmass[n] = D->pmass[n];
+    D->sc.psmooth2[n] = s * s;
+    D->sc.pdist3[n] = pd * pd * pd;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+#define LAUNCH(name, ...) \
+  (D->d.precision == FB_FP64 ? fb_launch_##name##_f64(__VA_ARGS__) : fb_launch_##name##_f32(__VA_ARGS__))
+
+int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out) {
+  fb_disk *D;
+  int f, n, rc, ndev = 0;
+  long long nc;
+  cudaError_t e;
+  *out = NULL;
+  if (!p || p->nx < 4 || p->ny < 4) return fail(FB_ERR_ARG, "invalid mesh size");
+  if (p->nz > 1 && !p->spherical) return fail(FB_ERR_ARG, "3D meshes are spherical in this library");
+  if (p->nz <= 1 && p->spherical) return fail(FB_ERR_ARG, "2D meshes are cylindrical in this library");
+  if (p->nplanets < 0 || p->nplanets > FB_MAXPLANETS) return fail(FB_ERR_ARG, "nplanets out of range");
+  if (p->nfluids < 1 || p->nfluids > FB_MAXFLUIDS) return fail(FB_ERR_ARG, "nfluids out of range");
+  if (p->frame != FB_FRAME_FIXED && p->nplanets < 1) return fail(FB_ERR_ARG, "rotating frame needs a planet");
+  if (precision != FB_FP64 && precision != FB_FP32) return fail(FB_ERR_ARG, "precision");
+  e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev <= device || device < 0)
+    return fail(FB_ERR_CUDA, "no CUDA device %d available (%s)", device, cudaGetErrorString(e));
+  CU(cudaSetDevice(device));
+  D = (fb_disk *)calloc(1, sizeof(fb_disk));
+  D->p = *p;
+  D->device = device;
+  D->esz = precision == FB_FP64 ? sizeof(double) : sizeof(float);
+  D->d.precision = precision;
+  D->d.nx = p->nx; D->d.ny = p->ny;
+  D->d.is3d = p->nz > 1;
+  D->d.nz = D->d.is3d ? p->nz : 1;
+  D->d.sy = p->ny + 2 * NG;
+  D->d.sz = D->d.is3d ? p->nz + 2 * NG : 1;
+  D->d.pitch = p->nx;
+  D->d.stride = (long long)p->nx * D->d.sy;
+  D->d.spherical = p->spherical;
+  D->d.alpha_visc = p->alpha_visc;
+  D->d.xlen = p->xmax - p->xmin;
+  D->d.cfl = p->cfl;
+  D->d.stockholm = p->stockholm;
+  D->d.nfluids = p->nfluids;
+  D->d.aspectratio = p->aspectratio; D->d.sigmaslope = p->sigmaslope; D->d.flaringindex = p->flaringindex;
+  D->ncell = nc = D->d.stride * D->d.sz;
+  D->xmin = calloc(p->nx + 1, 8); D->ymin = calloc(D->d.sy + 1, 8); D->zmin = calloc(D->d.sz + 1, 8);
+  D->xmed = calloc(p->nx, 8); D->ymed = calloc(D->d.sy, 8); D->zmed = calloc(D->d.sz, 8);
+  D->invdiffxmed = calloc(p->nx, 8); D->sxi = calloc(p->nx, 8);
+  D->sxj = calloc(D->d.sy, 8); D->syj = calloc(D->d.sy, 8); D->szj = calloc(D->d.sy, 8); D->invvj = calloc(D->d.sy, 8);
+  D->sxk = calloc(D->d.sz, 8); D->syk = calloc(D->d.sz, 8); D->szk = calloc(D->d.sz, 8);
+  mesh(D);
+  D->d.mindx = D->mindx;
+  if (cudaStreamCreateWithFlags(&D->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    fb_disk_destroy(D);
+    return fail(FB_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  if ((rc = upload_geometry(D)) || (rc = upload_tables(D))) { fb_disk_destroy(D); return rc; }
+  for (f = 0; f < p->nfluids; f++) {
+    fb_fluid_dev *F = &D->d.fl[f];
+    size_t fb = D->esz * nc, f2 = sizeof(double) * D->d.sy * D->d.sz, e2 = D->esz * D->d.sy * D->d.sz;
+    void **fields[] = {&F->rho, &F->cs, &F->vx, &F->vy, &F->vz, &F->vxt, &F->vyt, &F->vzt,
+                       &F->mpx, &F->mmx, &F->mpy, &F->mmy, &F->mpz, &F->mmz, &F->rho_a};
+    int i;
+    for (i = 0; i < 15; i++) {
+      if (!D->d.is3d && (i == 4 || i == 7 || i == 12 || i == 13)) { *fields[i] = NULL; continue; }
+      if ((rc = dalloc(D, fields[i], fb))) { fb_disk_destroy(D); return rc; }
+    }
+    if (D->d.is3d) {
+      void **b[] = {&F->mpx_b, &F->mmx_b, &F->mpy_b, &F->mmy_b, &F->mpz_b, &F->mmz_b, &F->rho_b};
+      for (i = 0; i < 7; i++)
+        if ((rc = dalloc(D, b[i], fb))) { fb_disk_destroy(D); return rc; }
+    }
+    if ((rc = dalloc(D, (void **)&F->vxmed, f2)) || (rc = dalloc(D, (void **)&F->vxmed_t, f2)) ||
+        (rc = dalloc(D, (void **)&F->nshift, sizeof(int) * D->d.sy * D->d.sz)) ||
+        (rc = dalloc(D, &F->rho0, e2)) || (rc = dalloc(D, &F->vx0, e2)) || (rc = dalloc(D, &F->vy0, e2)) ||
+        (rc = dalloc(D, &F->vz0, e2))) {
+      fb_disk_destroy(D);
+      return rc;
+    }
+    F->dust = f > 0;
+  }
+  if ((rc = dalloc(D, (void **)&D->d.dtmin, 64)) || (rc = dalloc(D, (void **)&D->d.scal_dev, sizeof(fb_scalars)))) {
+    fb_disk_destroy(D);
+    return rc;
+  }
+  if (cudaMallocHost((void **)&D->h_dtmin, 64) != cudaSuccess) { fb_disk_destroy(D); return fail(FB_ERR_CUDA, "pinned"); }
+  /* planets (psys.c:190-210) */
+  D->np = p->nplanets;
+  for (n = 0; n < D->np; n++) {
+    double dist = p->pl_dist[n];
+    D->pmass[n] = p->pl_mass[n];
+    D->px[n] = dist * (1.0 + p->eccentricity);
+    D->py[n] = 0.0; D->pz[n] = 0.0;
+    D->pvy[n] = sqrt(G * (MSTAR + D->pmass[n]) / dist) * sqrt((1.0 - p->eccentricity) / (1.0 + p->eccentricity)) *
+                cos(p->inclination);
+    D->pvx[n] = -0.0000000000 * D->pvy[n];
+    D->pvz[n] = D->pvy[n] * sin(p->inclination) / cos(p->inclination);
+    D->pfeelothers[n] = p->pl_feelothers[n];
+  }
+  D->omegaframe = p->omegaframe;
+  if (p->frame != FB_FRAME_FIXED) D->omegaframe = psys_info(D, PS_FREQUENCY); /* main.c:240-241 */
+  D->omegaframe0 = D->omegaframe;
+  D->step_count = 0;
+  D->sc.nu = p->nu; D->sc.alpha = p->alpha; D->sc.cfl = p->cfl;
+  D->sc.omegaframe = D->omegaframe; D->sc.omegaframe0 = D->omegaframe0;
+  planet_scalars(D);
+  *out = D;
+  return FB_OK;
+}
+
+int fb_disk_destroy(fb_disk *D) {
+  int i;
+  if (!D) return FB_OK;
+  if (D->device >= 0) cudaSetDevice(D->device);
+  if (D->stream) cudaStreamSynchronize(D->stream);
+  for (i = 0; i < D->nalloc; i++) cudaFree(D->allocs[i]);
+  if (D->h_dtmin) cudaFreeHost(D->h_dtmin);
+  if (D->stream) cudaStreamDestroy(D->stream);
+  free(D->xmin); free(D->ymin); free(D->zmin); free(D->xmed); free(D->ymed); free(D->zmed);
+  free(D->invdiffxmed); free(D->sxi); free(D->sxj); free(D->syj); free(D->szj); free(D->invvj);
+  free(D->sxk); free(D->syk); free(D->szk);
+  free(D);
+  return FB_OK;
+}
+
+static int put(fb_disk *D, void *dst, const double *src) {
+  size_t n = (size_t)D->ncell;
+  if (!src || !dst) return FB_OK;
+  if (D->d.precision == FB_FP64) {
+    CU(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, D->stream));
+  } else {
+    float *tmp = (float *)malloc(n * sizeof(float));
+    size_t i;
+    for (i = 0; i < n; i++) tmp[i] = (float)src[i];
+    CU(cudaMemcpyAsync(dst, tmp, n * sizeof(float), cudaMemcpyHostToDevice, D->stream));
+    CU(cudaStreamSynchronize(D->stream));
+    free(tmp);
+  }
+  return FB_OK;
+}
+
+static int get(fb_disk *D, double *dst, const void *src) {
+  size_t n = (size_t)D->ncell;
+  if (!src || !dst) return FB_OK;
+  if (D->d.precision == FB_FP64) {
+    CU(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, D->stream));
+    CU(cudaStreamSynchronize(D->stream));
+  } else {
+    float *tmp = (float *)malloc(n * sizeof(float));
+    size_t i;
+    CU(cudaMemcpyAsync(tmp, src, n * sizeof(float), cudaMemcpyDeviceToHost, D->stream));
+    CU(cudaStreamSynchronize(D->stream));
+    for (i = 0; i < n; i++) dst[i] = tmp[i];
+    free(tmp);
+  }
+  return FB_OK;
+}
+
+int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, const double *vy, const double *vz,
+                      const double *cs) {
+  fb_fluid_dev *F;
+  int rc;
+  if (!D || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
+  CU(cudaSetDevice(D->device));
+  F = &D->d.fl[f];
+  if ((rc = put(D, F->rho, rho)) || (rc = put(D, F->vx, vx)) || (rc = put(D, F->vy, vy)) ||
+      (rc = put(D, F->cs, cs)))
+    return rc;
+  if (D->d.is3d && (rc = put(D, F->vz, vz))) return rc;
+  CU(cudaStreamSynchronize(D->stream));
+  return FB_OK;
+}
+
+int fb_disk_get_state(fb_disk *D, int f, double *rho, double *vx, double *vy, double *vz) {
+  fb_fluid_dev *F;
+  int rc;
+  if (!D || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
+  CU(cudaSetDevice(D->device));
+  F = &D->d.fl[f];
+  if ((rc = get(D, rho, F->rho)) || (rc = get(D, vx, F->vx)) || (rc = get(D, vy, F->vy))) return rc;
+  if (D->d.is3d && (rc = get(D, vz, F->vz))) return rc;
+  if (!D->d.is3d && vz) memset(vz, 0, sizeof(double) * D->ncell);
+  return FB_OK;
+}
+
+static int push_scalars(fb_disk *D) {
+  D->sc.omegaframe = D->omegaframe;
+  D->sc.omegaframe0 = D->omegaframe0;
+  CU(cudaMemcpyAsync(D->d.scal_dev, &D->sc, sizeof(fb_scalars), cudaMemcpyHostToDevice, D->stream));
+  return FB_OK;
+}
+
+int fb_disk_initialize(fb_disk *D) {
+  int f, rc;
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  CU(cudaSetDevice(D->device));
+  if ((rc = push_scalars(D))) return rc;
+  for (f = 0; f < D->p.nfluids; f++) LCH(LAUNCH(bnd, &D->d, f, 0, D->stream));
+  /* init_stockholm (init_stockholm.c:56-105): 2D profiles from column i = 0 */
+  for (f = 0; f < D->p.nfluids; f++) {
+    fb_fluid_dev *F = &D->d.fl[f];
+    void *src[4] = {F->rho, F->vx, F->vy, F->vz}, *dst[4] = {F->rho0, F->vx0, F->vy0, F->vz0};
+    int q;
+    for (q = 0; q < 4; q++) {
+      if (!src[q]) continue;
+      CU(cudaMemcpy2DAsync(dst[q], D->esz, src[q], D->esz * D->d.pitch, D->esz, (size_t)D->d.sy * D->d.sz,
+                           cudaMemcpyDeviceToDevice, D->stream));
+    }
+  }
+  CU(cudaStreamSynchronize(D->stream));
+  return FB_OK;
+}
+
+int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
+  int f, rc;
+  double step, dt;
+  const uint64_t start_bits = 0x4415AF1D78B58C40ULL; /* 1e20, the MIN reduction start (define.h:165) */
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  CU(cudaSetDevice(D->device));
+  if (D->dtemp >= DT) D->dtemp = 0.0;
+  /* ComputeVmed(Vx) + cfl (main.c:366-388) */
+  CU(cudaMemcpyAsync(D->d.dtmin, &start_bits, 8, cudaMemcpyHostToDevice, D->stream));
+  if ((rc = push_scalars(D))) return rc;
+  for (f = 0; f < D->p.nfluids; f++) LCH(LAUNCH(rowsum, &D->d, f, 0, D->stream));
+  for (f = 0; f < D->p.nfluids; f++) LCH(LAUNCH(cfl, &D->d, f, D->stream));
+  CU(cudaMemcpyAsync(D->h_dtmin, D->d.dtmin, 8, cudaMemcpyDeviceToHost, D->stream));
+  CU(cudaStreamSynchronize(D->stream));
+  /* CflFluidsMin (cfl_fluids_min.c:3-22) */
+  step = 1e30;
+  if (step > D->h_dtmin[0]) step = D->h_dtmin[0];
+  if (!(step > SMALLTIME)) return fail(FB_ERR_NULL_DT, "null time step (dt = %g)", step);
+  dt = step;
+  D->dtemp += dt;
+  if (D->dtemp > DT) dt = DT - (D->dtemp - dt);
+  /* compute_potential (potential.c:10-49): the potential is evaluated with the
+   * planet positions before this step's orbit advance */
+  if (D->p.frame != FB_FRAME_FIXED) psys_info(D, PS_MARK);
+  planet_scalars(D);
+  for (f = 0; f < 5; f++) nbody_rk5(D, 1.0 / ((double)(5)) * dt);
+  if (D->p.frame != FB_FRAME_FIXED) {
+    double omeganew = psys_info(D, PS_GET) / dt;
+    D->domega = omeganew - D->omegaframe;
+    D->omegaframe = omeganew;
+  }
+  rotate(D, D->omegaframe * dt);
+  D->sc.dt = dt;
+  D->sc.domega = D->p.frame != FB_FRAME_FIXED ? D->domega : 0.0;
+  if ((rc = push_scalars(D))) return rc;
+  /* Sources (algogas.c:30-120) with its closing FillGhosts on V_temp */
+  for (f = 0; f < D->p.nfluids; f++) {
+    LCH(LAUNCH(sources, &D->d, f, D->stream));
+    LCH(LAUNCH(bnd, &D->d, f, 1, D->stream));
+  }
+  /* Transport (algogas.c:135-159) */
+  for (f = 0; f < D->p.nfluids; f++) {
+    LCH(LAUNCH(rowsum, &D->d, f, 1, D->stream));
+    LCH(LAUNCH(transport, &D->d, f, D->stream));
+  }
+  D->phys_time += dt;
+  D->step_count++;
+  /* NewVelocity + StockholmBoundary + FillGhosts (main.c:427-431) */
+  for (f = 0; f < D->p.nfluids; f++) {
+    LCH(LAUNCH(newvel, &D->d, f, D->stream));
+    LCH(LAUNCH(bnd, &D->d, f, 0, D->stream));
+  }
+  D->last_dt = dt;
+  if (dt_out) *dt_out = dt;
+  return FB_OK;
+}
+
+int fb_disk_get_scalars(fb_disk *D, double *o) {
+  if (!D || !o) return fail(FB_ERR_ARG, "null");
+  o[0] = D->phys_time; o[1] = D->omegaframe; o[2] = D->last_dt;
+  o[3] = D->np ? D->px[0] : 0; o[4] = D->np ? D->py[0] : 0;
+  o[5] = D->np ? D->pvx[0] : 0; o[6] = D->np ? D->pvy[0] : 0; o[7] = D->domega;
+  return FB_OK;
+}
+
+int fb_disk_device_fields(fb_disk *D, int f, void *ptrs[5], size_t *esz) {
+  if (!D || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
+  ptrs[0] = D->d.fl[f].rho; ptrs[1] = D->d.fl[f].vx; ptrs[2] = D->d.fl[f].vy;
+  ptrs[3] = D->d.fl[f].vz; ptrs[4] = D->d.fl[f].cs;
+  if (esz) *esz = D->esz;
+  return FB_OK;
+}
+
+void *fb_disk_stream(fb_disk *D) { return D ? (void *)D->stream : NULL; }

@@ -1,0 +1,1029 @@
+// fb_kernels.cuh -- the hydro-step kernels, templated on the field precision.
+//
+// Stage kernels of one hydro step (FARGO3D main.c:361-448):
+//   rowsum      ring sums of v_phi * dphi (ComputeVmed, compute_vmed.c:10-39)
+//   cfl         per-cell time step, CFL minimum and shear limit (cfl.c, cfl_b.c)
+//   sources     pressure, potential, SubStep1, viscous stress, SubStep2 fused in a
+//               shared-memory tile (algogas.c:30-120)
+//   bnd         ghost rows / layers (generated boundaries, algogas.c:11-27)
+//   sweep_z/y   conservative upwind van Leer transport along a column, one thread
+//               per column marching in its direction (transport.c:24-46, 84-127)
+//   sweep_x     one CTA per ring: FARGO residual, van Leer, PPA and integer shift
+//               in shared memory (transport.c:129-158)
+//   newvel      new velocities and Stockholm damping (newvel_*.c, stockholm.c)
+//
+// Floating-point expressions follow the reference's evaluation order exactly
+// (including the order implied by its geometry macros), so the FP64
+// instantiation, compiled without FMA contraction, reproduces the CPU build.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "fb_dev.h"
+
+#define FB_CVNR 1.41
+#define FB_NGH 3
+
+namespace fb {
+
+template <typename T>
+struct Geo {
+  const T *xmin, *ymin, *zmin, *xmed, *ymed, *zmed, *invdiffxmed;
+  const T *sxi, *sxj, *syj, *szj, *sxk, *syk, *szk, *invvj;
+  const T *sin_zmed, *cos_zmed, *sin_zmin, *cos_zmin;
+  const T *cos_xmed, *sin_xmed;
+  const T *visc_j, *viscm_j, *tau_j;
+};
+
+template <typename T>
+__host__ __device__ inline Geo<T> geo_of(const fb_geom_dev &g) {
+  Geo<T> o;
+  o.xmin = (const T *)g.xmin; o.ymin = (const T *)g.ymin; o.zmin = (const T *)g.zmin;
+  o.xmed = (const T *)g.xmed; o.ymed = (const T *)g.ymed; o.zmed = (const T *)g.zmed;
+  o.invdiffxmed = (const T *)g.invdiffxmed; o.sxi = (const T *)g.sxi;
+  o.sxj = (const T *)g.sxj; o.syj = (const T *)g.syj; o.szj = (const T *)g.szj;
+  o.sxk = (const T *)g.sxk; o.syk = (const T *)g.syk; o.szk = (const T *)g.szk;
+  o.invvj = (const T *)g.invvj;
+  o.sin_zmed = (const T *)g.sin_zmed; o.cos_zmed = (const T *)g.cos_zmed;
+  o.sin_zmin = (const T *)g.sin_zmin; o.cos_zmin = (const T *)g.cos_zmin;
+  o.cos_xmed = (const T *)g.cos_xmed; o.sin_xmed = (const T *)g.sin_xmed;
+  o.visc_j = (const T *)g.visc_j; o.viscm_j = (const T *)g.viscm_j; o.tau_j = (const T *)g.tau_j;
+  return o;
+}
+
+template <typename T>
+__device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
+
+struct Dims {
+  int nx, ny, nz, sy, sz, pitch;
+  long long stride;
+  int is3d, sph, alpha;
+  __device__ __forceinline__ long long l(int i, int j, int k) const {
+    return (long long)i + (long long)j * pitch + (long long)k * stride;
+  }
+};
+
+__host__ __device__ inline Dims dims_of(const fb_disk_dev &d) {
+  Dims m;
+  m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.sy = d.sy; m.sz = d.sz; m.pitch = d.pitch;
+  m.stride = d.stride; m.is3d = d.is3d; m.sph = d.spherical; m.alpha = d.alpha_visc;
+  return m;
+}
+
+__device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }
+
+// ---------------------------------------------------------------------------
+// Ordered ring sums (ComputeVweight + reduction_SUM, compute_vmed.c:42-97,
+// reduction_generic.c:5-23): vmed[j,k] = (sum_i v[i] * (xmin[i+1]-xmin[i])) /
+// (XMAX - XMIN), accumulated sequentially in i as the reference does, one
+// lane per ring; the rings' rows are staged through shared memory so that
+// global loads stay coalesced.  32 rings per CTA of 256 threads.
+template <typename T, bool ORDERED>
+__global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const T *__restrict__ v,
+                                                 double *__restrict__ out, double xlen) {
+  constexpr int R = 32, CH = 128;
+  __shared__ double buf[R][CH + 1];
+  const int nring = m.sy * m.sz;
+  const int r0 = blockIdx.x * R;
+  const int tid = threadIdx.x;
+  double acc = 0.0;
+  const int myring = r0 + (tid & 31);
+  for (int c0 = 0; c0 < m.nx; c0 += CH) {
+    const int cw = min(CH, m.nx - c0);
+    for (int e = tid; e < R * CH; e += blockDim.x) {
+      const int rr = e / CH, ii = e - rr * CH;
+      const int ring = r0 + rr;
+      double val = 0.0;
+      if (ring < nring && ii < cw) {
+        const int j = ring % m.sy, k = ring / m.sy;
+        const int i = c0 + ii;
+        val = (double)v[m.l(i, j, k)] * (ld(gd.xmin + i + 1) - ld(gd.xmin + i));
+      }
+      buf[rr][ii] = val;
+    }
+    __syncthreads();
+    if (ORDERED) {
+      if (tid < R) {
+        for (int ii = 0; ii < cw; ii++) acc = acc + buf[tid][ii];
+      }
+    } else {
+      // warp w sums rings 4w..4w+3 with a shuffle tree (order-free path)
+      const int w = tid >> 5, lane = tid & 31;
+      for (int q = 0; q < 4; q++) {
+        const int rr = w * 4 + q;
+        double s = 0.0;
+        for (int ii = lane; ii < cw; ii += 32) s += buf[rr][ii];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) buf[rr][CH] = (c0 == 0 ? 0.0 : buf[rr][CH]) + s;
+      }
+    }
+    __syncthreads();
+  }
+  if (tid < R && myring < nring) {
+    double tot = ORDERED ? acc : buf[tid][CH];
+    out[myring] = tot / xlen;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CFL (cfl.c:135-258) and cfl_b's shear limit (cfl_b.c:14-39).  One CTA per
+// active ring; the ring minimum (including its shear limit) is folded into a
+// device-wide minimum held as the bit pattern of a positive double.
+__device__ __forceinline__ double dmax2(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmax3(double a, double b, double c) {
+  return (((a) > (b) ? (a) : (b)) > (c) ? ((a) > (b) ? (a) : (b)) : (c));
+}
+
+template <typename T>
+__device__ __forceinline__ T zsx(const Dims &m, const Geo<T> &g, int i, int j, int k) {
+  // zone_size_x (define.h:262-273)
+  if (m.sph) return (ld(g.sxi + i) * ld(g.ymed + j) * ld(g.sin_zmed + k));
+  return (ld(g.sxi + i) * ld(g.ymed + j));
+}
+template <typename T>
+__device__ __forceinline__ T izsxmed(const Dims &m, const Geo<T> &g, int i, int j, int k) {
+  // Inv_zone_size_xmed
+  if (m.sph) return (ld(g.invdiffxmed + i) / ld(g.ymed + j) / ld(g.sin_zmed + k));
+  return (ld(g.invdiffxmed + i) / ld(g.ymed + j));
+}
+template <typename T>
+__device__ __forceinline__ T zsy(const Geo<T> &g, int j) { return (ld(g.ymin + j + 1) - ld(g.ymin + j)); }
+template <typename T>
+__device__ __forceinline__ T zsz(const Dims &m, const Geo<T> &g, int j, int k) {
+  if (m.sph) return ((ld(g.zmin + k + 1) - ld(g.zmin + k)) * ld(g.ymed + j));
+  return (ld(g.zmin + k + 1) - ld(g.zmin + k));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const T *__restrict__ rho, const T *__restrict__ cs,
+                                             const T *__restrict__ vx, const T *__restrict__ vy,
+                                             const T *__restrict__ vz, const double *__restrict__ vxmed,
+                                             const fb_scalars *__restrict__ sc, double cfl_num,
+                                             double mindx, unsigned long long *__restrict__ dtmin) {
+  const int j = FB_NGH + blockIdx.x;
+  const int k = m.is3d ? FB_NGH + blockIdx.y : 0;
+  const double vm = vxmed[j + k * m.sy];
+  const T nu = (T)sc->nu, alpha = (T)sc->alpha;
+  double mn = 1e20;
+  for (int i = threadIdx.x; i < m.nx; i += blockDim.x) {
+    const long long l = m.l(i, j, k);
+    const long long lxp = (i < m.nx - 1) ? l + 1 : l - (m.nx - 1);
+    const T vxx = vx[l] - (T)vm, vxxp = vx[lxp] - (T)vm;
+    const T c = cs[l];
+    const T ss2 = c * c;
+    T visc;
+    if (m.alpha) visc = alpha * c * c * ld(g.visc_j + j);
+    else visc = nu;
+    const T ss = sqrt(ss2);
+    const T zx = zsx(m, g, i, j, k), zy = zsy(g, j);
+    T c1a = ss / zx, c1b = ss / zy, c1c = 0, c4 = 0, c5c = 0, c7c = 0;
+    T zz = 1;
+    if (m.is3d) { zz = zsz(m, g, j, k); c1c = ss / zz; }
+    const T c1 = (T)dmax3(c1a, c1b, c1c);
+    const T c2 = (T)(dmax2(fabs(vxx), fabs(vxxp))) / zx;
+    const T c3 = (T)(dmax2(fabs(vy[l]), fabs(vy[l + m.pitch]))) / zy;
+    if (m.is3d) c4 = (T)(dmax2(fabs(vz[l]), fabs(vz[l + m.stride]))) / zz;
+    const T c5a = fabs(vx[lxp] - vx[l]) / zx;
+    const T c5b = fabs(vy[l + m.pitch] - vy[l]) / zy;
+    if (m.is3d) c5c = fabs(vz[l + m.stride] - vz[l]) / zz;
+    const T c5 = (T)dmax3(c5a, c5b, c5c) * (T)4.0 * (T)FB_CVNR;
+    const T c7a = (T)1.0 / zx, c7b = (T)1.0 / zy;
+    if (m.is3d) c7c = (T)1.0 / zz;
+    const T mx7 = (T)dmax3(c7a, c7b, c7c);
+    const T c7 = (T)4.0 * visc * (mx7 * mx7);
+    const T zero = 0;
+    const T dtc = (T)cfl_num / sqrt(c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4 + c5 * c5 + zero * zero + c7 * c7 +
+                                    zero * zero + zero * zero + zero * zero);
+    mn = fmin(mn, (double)dtc);
+  }
+  // shear limit (cfl_b.c:27-33)
+  if (threadIdx.x == 0) {
+    const double shear =
+        cfl_num * mindx /
+        fabs(vm / (double)ld(g.ymed + j) - vxmed[j + 1 + k * m.sy] / (double)ld(g.ymed + j + 1));
+    if (shear < mn) mn = shear;
+  }
+  for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+  __shared__ double wm[32];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mn;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? wm[threadIdx.x] : 1e20;
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0 && v > 0.0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Potential (potential.c:51-208), FP64, at one cell.
+__device__ __forceinline__ double potential_at(const Dims &m, const Geo<double> &gd,
+                                               const fb_scalars &sc, int i, int j, int k) {
+  double XC, YC, ZC, pot;
+  const double ym = ld(gd.ymed + j);
+  if (m.sph) {
+    XC = ym * ld(gd.cos_xmed + i) * ld(gd.sin_zmed + k);
+    YC = ym * ld(gd.sin_xmed + i) * ld(gd.sin_zmed + k);
+    ZC = ym * ld(gd.cos_zmed + k);
+    pot = -1.0 * 1.0 / ym;
+  } else {
+    XC = ym * ld(gd.cos_xmed + i);
+    YC = ym * ld(gd.sin_xmed + i);
+    ZC = ld(gd.zmed + k);
+    pot = -1.0 * 1.0 / sqrt(ym * ym + ZC * ZC);
+  }
+  for (int n = 0; n < sc.nplanets; n++) {
+    const double mp = sc.pmass[n] * 1.0;
+    const double xp = sc.px[n], yp = sc.py[n], zp = sc.pz[n];
+    const double dist = ((XC - xp) * (XC - xp) + (YC - yp) * (YC - yp) + (ZC - zp) * (ZC - zp));
+    if (sc.indirect_term) pot += 1.0 * mp * (XC * xp + YC * yp + ZC * zp) / sc.pdist3[n];
+    pot += -1.0 * mp / sqrt(dist + sc.psmooth2[n]);
+  }
+  return pot;
+}
+
+}  // namespace fb
+
+namespace fb {
+
+// ---------------------------------------------------------------------------
+// Sources, 2D cylindrical (algogas.c:30-120): ComputePressureFieldIso,
+// compute_potential's Potential, CorrectVtheta, SubStep1_x/y, visctensor_cyl,
+// addviscosity_cyl, SubStep2_a/b, fused over a TX x TY tile of active cells.
+// Inputs (rho, cs, v, P, Pot) are staged with a one-cell halo; the stress
+// tensor is computed once per point into shared memory.
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX *TY) k_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
+    const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx,
+    const T *__restrict__ vy, T *__restrict__ vxt, T *__restrict__ vyt,
+    const fb_scalars *__restrict__ scp, int dust, int viscous) {
+  constexpr int W = TX + 2, H = TY + 2;
+  __shared__ T s_rho[H][W], s_cs[H][W], s_vx[H][W], s_vy[H][W], s_p[H][W];
+  __shared__ double s_pot[H][W];
+  __shared__ T s_txx[H][W], s_tyy[H][W], s_tyx[H][W];
+  __shared__ fb_scalars sc;
+  const int i0 = blockIdx.x * TX, j0 = FB_NGH + blockIdx.y * TY;
+  const int tid = threadIdx.x + threadIdx.y * TX;
+  if (tid == 0) sc = *scp;
+  __syncthreads();
+  const double dt = sc.dt;
+  const T domega = (T)sc.domega, of = (T)sc.omegaframe;
+  const bool corot = sc.domega != 0.0 || true;
+  (void)corot;
+  // stage inputs; vx carries CorrectVtheta (correct_vtheta.c:55-60)
+  for (int e = tid; e < H * W; e += TX * TY) {
+    const int lj = e / W, li = e - lj * W;
+    const int j = j0 - 1 + lj, i = wrapx(i0 - 1 + li, m.nx);
+    if (j < m.sy && i0 - 1 + li <= m.nx) {
+      const long long l = m.l(i, j, 0);
+      const T r = rho[l], c = cs[l];
+      s_rho[lj][li] = r;
+      s_cs[lj][li] = c;
+      s_vx[lj][li] = vx[l] - domega * ld(g.ymed + j);
+      s_vy[lj][li] = vy[l];
+      s_p[lj][li] = r * c * c;
+      s_pot[lj][li] = potential_at(m, gd, sc, i, j, 0);
+    }
+  }
+  __syncthreads();
+  if (viscous) {
+    const T nu = (T)sc.nu, alpha = (T)sc.alpha;
+    for (int e = tid; e < H * W; e += TX * TY) {
+      const int lj = e / W, li = e - lj * W;
+      const int j = j0 - 1 + lj, i = wrapx(i0 - 1 + li, m.nx);
+      if (j >= m.sy - 1 || i0 - 1 + li > m.nx) continue;
+      // tau_xx, tau_yy at (li in [0,TX], lj in [0,TY]); tau_yx at (li,lj >= 1)
+      T visc = nu, viscm = nu;
+      if (m.alpha && lj >= 1 && li >= 1) {
+        const T e0 = s_cs[lj][li], ex = s_cs[lj][li - 1], ey = s_cs[lj - 1][li], exy = s_cs[lj - 1][li - 1];
+        viscm = alpha * (T)0.0625 * (e0 + ex + ey + exy) * (e0 + ex + ey + exy) * ld(g.viscm_j + j);
+      }
+      if (m.alpha) visc = alpha * s_cs[lj][li] * s_cs[lj][li] * ld(g.visc_j + j);
+      if (li <= TX && lj <= TY) {
+        const T r = s_rho[lj][li];
+        const T sxi = ld(g.sxi + i), syk = ld(g.syk + 0), sxk = ld(g.sxk + 0);
+        T div_v = 0.0;
+        div_v += (s_vx[lj][li + 1] - s_vx[lj][li]) * ld(g.sxj + j) * sxk;
+        div_v += (s_vy[lj + 1][li] * ld(g.syj + j + 1) * syk * sxi - s_vy[lj][li] * ld(g.syj + j) * syk * sxi);
+        div_v *= (T)(2.0 / 3.0) * ld(g.invvj + j) / (syk * sxi);
+        T txx = visc * r * ((T)2.0 * (s_vx[lj][li + 1] - s_vx[lj][li]) / zsx(m, g, i, j, 0) - div_v);
+        txx += visc * r * (s_vy[lj + 1][li] + s_vy[lj][li]) / ld(g.ymed + j);
+        s_txx[lj][li] = txx;
+        s_tyy[lj][li] = visc * r * ((T)2.0 * (s_vy[lj + 1][li] - s_vy[lj][li]) / (ld(g.ymin + j + 1) - ld(g.ymin + j)) - div_v);
+      }
+      if (li >= 1 && lj >= 1) {
+        s_tyx[lj][li] = viscm * (T)0.25 * (s_rho[lj][li] + s_rho[lj][li - 1] + s_rho[lj - 1][li] + s_rho[lj - 1][li - 1]) *
+                        ((s_vy[lj][li] - s_vy[lj][li - 1]) * ld(g.invdiffxmed + i) / ld(g.ymin + j) +
+                         (s_vx[lj][li] - s_vx[lj - 1][li]) / (ld(g.ymed + j) - ld(g.ymed + j - 1)) -
+                         (T)0.5 * (s_vx[lj][li] + s_vx[lj - 1][li]) / ld(g.ymin + j));
+      }
+    }
+    __syncthreads();
+  }
+  const int li = threadIdx.x + 1, lj = threadIdx.y + 1;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  if (i >= m.nx || j > m.ny + FB_NGH - 1) return;
+  const int im = wrapx(i - 1, m.nx);
+  const long long l = m.l(i, j, 0);
+  const T r = s_rho[lj][li], rxm = s_rho[lj][li - 1], rym = s_rho[lj - 1][li];
+  const T izx = izsxmed(m, g, i, j, 0);
+  // SubStep1_x (substep1_x.c:107-117)
+  const T dxmed = (T)0.5 * (ld(g.sxi + i) + ld(g.sxi + im));
+  const T dtorx = (T)2. * (T)dt / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * dxmed;
+  T ax = s_vx[lj][li];
+  if (!dust) ax -= dtorx * (s_p[lj][li] - s_p[lj][li - 1]) * izx;
+  ax -= (T)((s_pot[lj][li] - s_pot[lj][li - 1]) * dt) * izx;
+  // SubStep1_y (substep1_y.c:146-192, cylindrical)
+  const T ym = ld(g.ymed + j), ymm = ld(g.ymed + j - 1), yi = ld(g.ymin + j), yip = ld(g.ymin + j + 1),
+          yim = ld(g.ymin + j - 1);
+  const T dtory = (T)2.0 * (T)dt / (r * (yip - yi) + rym * (yi - yim)) * (ym - ymm);
+  T ay = s_vy[lj][li];
+  if (!dust) ay -= dtory * (s_p[lj][li] - s_p[lj - 1][li]) / (ym - ymm);
+  T vphi = (T)0.25 * (s_vx[lj][li] + s_vx[lj][li + 1] + s_vx[lj - 1][li] + s_vx[lj - 1][li + 1]);
+  vphi += yi * of;
+  ay += vphi * vphi / yi * (T)dt;
+  ay -= (T)((s_pot[lj][li] - s_pot[lj - 1][li]) * dt / (double)(ym - ymm));
+  if (viscous) {
+    // addviscosity_cyl (addviscosity_cyl.c:106-124)
+    ax += (T)2.0 * (s_txx[lj][li] - s_txx[lj][li - 1]) * izx / ((r + rxm)) * (T)dt;
+    ax += (T)2.0 * (yip * yip * s_tyx[lj + 1][li] - yi * yi * s_tyx[lj][li]) / ((yip - yi) * ym * ym * (rxm + r)) * (T)dt;
+    ay += (T)2.0 * (ym * s_tyy[lj][li] - ymm * s_tyy[lj - 1][li]) / ((ym - ymm) * (r + rym) * yi) * (T)dt;
+    ay += (T)2.0 * (s_tyx[lj][li + 1] - s_tyx[lj][li]) / ((ld(g.xmin + i + 1) - ld(g.xmin + i)) * yi * (r + rym)) * (T)dt;
+    ay -= (s_txx[lj][li] + s_txx[lj - 1][li]) / (yi * (r + rym)) * (T)dt;
+  }
+  // SubStep2_a / SubStep2_b (substep2_a.c:107-129, substep2_b.c:150-175)
+  const T c2 = (T)FB_CVNR;
+  T dv = s_vx[lj][li + 1] - s_vx[lj][li];
+  const T qx = dv < (T)0.0 ? c2 * c2 * r * dv * dv : (T)0.0;
+  dv = s_vx[lj][li] - s_vx[lj][li - 1];
+  const T qxm = dv < (T)0.0 ? c2 * c2 * rxm * dv * dv : (T)0.0;
+  dv = s_vy[lj + 1][li] - s_vy[lj][li];
+  const T qy = dv < (T)0.0 ? c2 * c2 * r * dv * dv : (T)0.0;
+  dv = s_vy[lj][li] - s_vy[lj - 1][li];
+  const T qym = dv < (T)0.0 ? c2 * c2 * rym * dv * dv : (T)0.0;
+  ax += -(T)2.0 * (T)dt * dxmed * (qx - qxm) / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * izx;
+  ay += -(T)2.0 * (qy - qym) / (r * (yip - yi) + rym * (yi - yim)) * (T)dt;
+  vxt[l] = ax;
+  vyt[l] = ay;
+}
+
+}  // namespace fb
+
+namespace fb {
+
+// ---------------------------------------------------------------------------
+// Ghost cells from the setups' boundary templates (std/boundaries.txt with
+// setups/fargo/fargo.bound in 2D and setups/p3disof/p3disof.bound in 3D;
+// index rules of scripts/boundparser.py:360-398).  All libm factors of the
+// templates are tabulated on the host.  Table layout (doubles):
+//   [0,6)  rho power factor per (side, ghost row)   [6,12) sqrt factor
+//   [12,18) 3D radial v_phi correction factor        [18,18+6*sz) 3D exp factor
+//   then 6*sy colatitude density factors, then 6 colatitude v_phi factors.
+struct BndTab {
+  const double *t;
+  int sy, sz;
+  __device__ double rhof(int s, int jj) const { return t[s * 3 + jj]; }
+  __device__ double sqf(int s, int jj) const { return t[6 + s * 3 + jj]; }
+  __device__ double cf(int s, int jj) const { return t[12 + s * 3 + jj]; }
+  __device__ double rhoe(int s, int jj, int k) const { return t[18 + (s * 3 + jj) * sz + k]; }
+  __device__ double zrho(int s, int kk, int j) const { return t[18 + 6 * sz + (s * 3 + kk) * sy + j]; }
+  __device__ double zw(int s, int kk) const { return t[18 + 6 * sz + 6 * sy + s * 3 + kk]; }
+};
+
+// Radial sides: one thread per (i, ghost row jj, side s, layer k).
+template <typename T>
+__global__ void k_bnd_y(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
+                        T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
+                        int do_rho) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y % 3, s = blockIdx.y / 3, k = blockIdx.z;
+  if (i >= m.nx) return;
+  const T of = (T)scp->omegaframe;
+  const int nghy = FB_NGH, ny = m.ny;
+  int jgh, jact, jlacts, jnull;
+  if (s == 0) { jgh = jj; jact = 2 * nghy - jj - 1; jlacts = 2 * nghy - jj; jnull = nghy; }
+  else { jgh = ny + nghy + jj; jact = ny + nghy - 1 - jj; jlacts = jact; jnull = ny + nghy; }
+  const long long lgh = m.l(i, jgh, k), lact = m.l(i, jact, k);
+  const T yact = ld(g.ymed + jact), ygh = ld(g.ymed + jgh);
+  if (!m.is3d) {
+    if (do_rho) rho[lgh] = rho[lact] * (T)tb.rhof(s, jj);
+    vx[lgh] = (vx[lact] + yact * of) * (T)tb.sqf(s, jj) - ygh * of;
+  } else {
+    const T sz = ld(g.sin_zmed + k);
+    if (do_rho) rho[lgh] = rho[lact] * (T)tb.rhof(s, jj) * (T)tb.rhoe(s, jj, k);
+    vx[lgh] = (vx[lact] + of * yact * sz) * (T)tb.sqf(s, jj) * (T)tb.cf(s, jj) - ygh * of * sz;
+  }
+  // Vy: ANTISYMMETRIC, staggered in y (|-a|0|a|)
+  if (s == 0) vy[lgh] = -vy[m.l(i, jlacts, k)];
+  else if (jj < nghy - 1) vy[m.l(i, ny + nghy + 1 + jj, k)] = -vy[m.l(i, jlacts, k)];
+  vy[m.l(i, jnull, k)] = 0;
+  // Vz: SYMMETRIC, centred in y
+  if (m.is3d) vz[lgh] = vz[lact];
+}
+
+// Colatitude sides (3D): one thread per (i, j, ghost layer kk, side s).
+template <typename T>
+__global__ void k_bnd_z(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
+                        T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
+                        int do_rho) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, kk = blockIdx.z % 3, s = blockIdx.z / 3;
+  if (i >= m.nx) return;
+  const T of = (T)scp->omegaframe;
+  const int nghz = FB_NGH, nz = m.nz;
+  int kgh, kact, klacts, knull;
+  if (s == 0) { kgh = kk; kact = 2 * nghz - kk - 1; klacts = 2 * nghz - kk; knull = nghz; }
+  else { kgh = nz + nghz + kk; kact = nz + nghz - 1 - kk; klacts = kact; knull = nz + nghz; }
+  const long long lgh = m.l(i, j, kgh), lact = m.l(i, j, kact);
+  const T ym = ld(g.ymed + j);
+  if (do_rho) rho[lgh] = rho[lact] * (T)tb.zrho(s, kk, j);
+  vx[lgh] = (vx[lact] + of * ym * ld(g.sin_zmed + kact)) * (T)tb.zw(s, kk) - ym * of * ld(g.sin_zmed + kgh);
+  vy[lgh] = vy[lact];
+  if (s == 0) vz[lgh] = -vz[m.l(i, j, klacts)];
+  else if (kk < nghz - 1) vz[m.l(i, j, nz + nghz + 1 + kk)] = -vz[m.l(i, j, klacts)];
+  vz[m.l(i, j, knull)] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Column sweeps (Y and Z): TransportY/TransportZ (transport.c:24-46) for the
+// density and every momentum, one thread per column marching over a segment
+// of NS rows (layers) with its input window in registers.
+//   VanLeer*_a (vanleer_y_a.c:62-70), VanLeer*_b (vanleer_y_b.c:62-68),
+//   DivideByRho (divrho.c:52), Update* / UpdateDensity* (update_y.c:68-72).
+// DIR 0 = Y (radius), 1 = Z (colatitude).
+template <typename T, int DIR>
+struct ColGeo {
+  Dims m; Geo<T> g; int i, j, k;
+  __device__ T zone(int c) const {  // zone size at cell c along DIR
+    if (DIR == 0) return zsy(g, c);
+    return zsz(m, g, j, c);
+  }
+  __device__ T surf(T v, int c) const {  // v * Surf(c) with the reference's association
+    if (DIR == 0) return v * ld(g.syj + c) * ld(g.syk + k) * ld(g.sxi + i);
+    return v * ld(g.szj + j) * ld(g.szk + c) * ld(g.sxi + i);
+  }
+  __device__ T finish(T flux, T dt, int c) const {  // flux * dt * InvVol(i,j,k)
+    if (DIR == 0) return flux * dt * ld(g.invvj + c) / (ld(g.syk + k) * ld(g.sxi + i));
+    return flux * dt * ld(g.invvj + j) / (ld(g.syk + c) * ld(g.sxi + i));
+  }
+};
+
+template <typename T, int DIR, int NS>
+__device__ __forceinline__ void col_sweep_q(const ColGeo<T, DIR> &cg, int c0, const T *a, const T *vel,
+                                            const T *rs, T dt, T *qs) {
+  // a: NS+4 cell values (c0-2 .. c0+NS+1); vel: NS+1 faces (c0 .. c0+NS)
+  T slope[NS + 2];
+#pragma unroll
+  for (int s = 0; s < NS + 2; s++) {
+    const int c = c0 - 1 + s;
+    const T dqm = (a[s + 1] - a[s]) / cg.zone(c);
+    const T dqp = (a[s + 2] - a[s + 1]) / cg.zone(c + 1);
+    if (dqp * dqm <= 0) slope[s] = 0;
+    else slope[s] = (T)2. * dqp * dqm / (dqm + dqp);
+  }
+#pragma unroll
+  for (int f = 0; f < NS + 1; f++) {
+    const int c = c0 + f;
+    const T v = vel[f];
+    if (v > (T)0.)
+      qs[f] = a[f + 1] + (T)0.5 * (cg.zone(c - 1) - v * dt) * slope[f];
+    else
+      qs[f] = a[f + 2] - (T)0.5 * (cg.zone(c) + v * dt) * slope[f + 1];
+  }
+  (void)rs;
+}
+
+// Quantity sources: 2D Y sweep and 3D Z sweep build the momenta from rho and
+// V_temp (momenta_x.c:76-85, momenta_y.c:65-66, momenta_z.c:61-66); the 3D
+// Y sweep reads them from the Z sweep's output buffers.
+template <typename T>
+struct QSrc {
+  const T *rho, *vxt, *vyt, *vzt;
+  const T *q[6];   // when from buffers: mpx, mmx, mpy, mmy, mpz, mmz
+  int from_v;
+  T of;
+};
+
+template <typename T>
+__device__ __forceinline__ T momentum(const Dims &m, const Geo<T> &g, const QSrc<T> &src, int q, int i, int j,
+                                      int k, long long l, T r) {
+  if (!src.from_v) return src.q[q][l];
+  switch (q) {
+    case 0: case 1: {  // Mpx, Mmx
+      const long long lx = (q == 0) ? ((i < m.nx - 1) ? l + 1 : l - (m.nx - 1)) : l;
+      if (!m.sph) {
+        const T y = ld(g.ymed + j);
+        return (src.vxt[lx] + y * src.of) * y * r;
+      }
+      const T rc = ld(g.ymed + j) * ld(g.sin_zmed + k);
+      return (src.vxt[lx] + rc * src.of) * rc * r;
+    }
+    case 2: return src.vyt[l + m.pitch] * r;  // Mpy
+    case 3: return src.vyt[l] * r;            // Mmy
+    case 4: {                                 // Mpz
+      T v = src.vzt[l + m.stride] * r;
+      if (m.sph) v *= ld(g.ymed + j);
+      return v;
+    }
+    default: {                                // Mmz
+      T v = src.vzt[l] * r;
+      if (m.sph) v *= ld(g.ymed + j);
+      return v;
+    }
+  }
+}
+
+// One launch covers cells [clo, chi] along DIR for every column in range.
+// grid.x: columns along x (blockDim.x threads), grid.y: the other transverse
+// index (row j for Z sweeps, layer k for Y sweeps), grid.z: segments along DIR.
+template <typename T, int DIR, int NS>
+__global__ void __launch_bounds__(128) k_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int nq, int clo, int chi,
+                                                   int t2lo, T *__restrict__ rho_out, T *q_out0, T *q_out1,
+                                                   T *q_out2, T *q_out3, T *q_out4, T *q_out5,
+                                                   const fb_scalars *__restrict__ scp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nx) return;
+  const int t2 = t2lo + blockIdx.y;
+  const int c0 = clo + blockIdx.z * NS;
+  if (c0 > chi) return;
+  const int j = (DIR == 0) ? 0 : t2, k = (DIR == 0) ? t2 : 0;
+  ColGeo<T, DIR> cg{m, g, i, j, k};
+  const T dt = (T)scp->dt;
+  src.of = (T)scp->omegaframe;  // momenta_x.c:77-78 read the current OMEGAFRAME
+  auto cidx = [&](int c) -> long long { return (DIR == 0) ? m.l(i, c, k) : m.l(i, j, c); };
+  // cells beyond chi + 2 (faces beyond chi + 1) never reach an output: clamp
+  const int cmax = chi + 2;
+  T r[NS + 4], vel[NS + 1], rs[NS + 1], a[NS + 4], qs[NS + 1];
+  const T *vface = (DIR == 0) ? src.vyt : src.vzt;
+#pragma unroll
+  for (int w = 0; w < NS + 4; w++) r[w] = src.rho[cidx(min(c0 - 2 + w, cmax))];
+#pragma unroll
+  for (int f = 0; f < NS + 1; f++) vel[f] = vface[cidx(min(c0 + f, cmax - 1))];
+  // density interface values (VanLeer*_a/_b on Density -> DensStar)
+  col_sweep_q<T, DIR, NS>(cg, c0, r, vel, rs, dt, rs);
+  T *qo[6] = {q_out0, q_out1, q_out2, q_out3, q_out4, q_out5};
+  for (int q = 0; q < nq; q++) {
+    T qv[NS + 4];
+#pragma unroll
+    for (int w = 0; w < NS + 4; w++) {
+      const int c = min(c0 - 2 + w, cmax);
+      const int jj = (DIR == 0) ? c : j, kk = (DIR == 0) ? k : c;
+      qv[w] = momentum(m, g, src, q, i, jj, kk, cidx(c), r[w]);
+      a[w] = qv[w] / r[w];
+    }
+    col_sweep_q<T, DIR, NS>(cg, c0, a, vel, rs, dt, qs);
+#pragma unroll
+    for (int u = 0; u < NS; u++) {
+      const int c = c0 + u;
+      if (c <= chi) {
+        const T flux = cg.surf(vel[u] * qs[u] * rs[u], c) - cg.surf(vel[u + 1] * qs[u + 1] * rs[u + 1], c + 1);
+        qo[q][cidx(c)] = qv[u + 2] + cg.finish(flux, dt, c);
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < NS; u++) {
+    const int c = c0 + u;
+    if (c <= chi) {
+      const T flux = cg.surf(vel[u] * rs[u], c) - cg.surf(vel[u + 1] * rs[u + 1], c + 1);
+      rho_out[cidx(c)] = r[u + 2] + cg.finish(flux, dt, c);
+    }
+  }
+}
+
+}  // namespace fb
+
+namespace fb {
+
+// ---------------------------------------------------------------------------
+// Azimuthal sweep, one CTA per ring (transport.c:129-158): ComputeResidual,
+// X_advection with van Leer on the residual velocity, X_advection with PPA on
+// the uniform fractional velocity, then AdvectSHIFT by the integer shift.
+// The ring of the density and of every momentum stays in shared memory
+// across the three passes; only the final shifted values are written.
+// Dynamic shared memory: (8 + nq) * nx elements of T.
+template <typename T>
+struct RingSmem {
+  T *rho, *v, *rs, *a, *slope, *qs, *ql, *qr, *q[6];
+};
+
+template <typename T>
+__device__ __forceinline__ void ring_vl_iface(const Dims &m, const Geo<T> &g, int j, int k, const T *q,
+                                              const T *v, T dt, T *slope, T *qs) {
+  const int nx = m.nx;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // VanLeerX_a (vanleer_x_a.c:58-70)
+    const int im = i > 0 ? i - 1 : nx - 1, ip = i < nx - 1 ? i + 1 : 0;
+    const T dqm = (q[i] - q[im]) / zsx(m, g, i, j, k);
+    const T dqp = (q[ip] - q[i]) / zsx(m, g, ip, j, k);
+    if (dqp * dqm <= (T)0.0) slope[i] = (T)0.0;
+    else slope[i] = ((T)2. * dqp * dqm) / (dqm + dqp);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // VanLeerX_b (vanleer_x_b.c:59-66)
+    const int im = i > 0 ? i - 1 : nx - 1;
+    if (v[i] > (T)0.0) qs[i] = q[im] + (T)0.5 * (zsx(m, g, im, j, k) - v[i] * dt) * slope[im];
+    else qs[i] = q[i] - (T)0.5 * (zsx(m, g, i, j, k) + v[i] * dt) * slope[i];
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ void ring_ppa_iface(const Dims &m, const Geo<T> &g, int j, int k, const T *q,
+                                               const T *v, T dt, T *slope, T *ql, T *qr, T *qs) {
+  const int nx = m.nx;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // VanLeerX_PPA_a (fargo_ppa_a.c:58-72)
+    const int im = i > 0 ? i - 1 : nx - 1, ip = i < nx - 1 ? i + 1 : 0;
+    const T dqm = (q[i] - q[im]), dqp = (q[ip] - q[i]);
+    T sl;
+    if (dqp * dqm <= (T)0.0) sl = (T)0.0;
+    else {
+      sl = (T)0.5 * (q[ip] - q[im]);
+      T work = fabs(sl);
+      if ((T)2.0 * fabs(dqm) < work) work = (T)2.0 * fabs(dqm);
+      if ((T)2.0 * fabs(dqp) < work) work = (T)2.0 * fabs(dqp);
+      if (sl < 0) sl = -work;
+      else sl = work;
+    }
+    slope[i] = sl;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // _b (fargo_ppa_b.c:55-62) and _c (fargo_ppa_c.c:53-67)
+    const int im = i > 0 ? i - 1 : nx - 1, ip = i < nx - 1 ? i + 1 : 0;
+    const T qrr = q[i] + (T)0.5 * (q[ip] - q[i]) - (T)(1.0 / 6.0) * (slope[ip] - slope[i]);
+    const T qll = q[im] + (T)0.5 * (q[i] - q[im]) - (T)(1.0 / 6.0) * (slope[i] - slope[im]);
+    T L = qll, R = qrr;
+    const T qq = q[i];
+    if ((R - qq) * (qq - L) < (T)0.0) { L = qq; R = qq; }
+    const T diff = R - L;
+    const T cord = qq - (T)0.5 * (L + R);
+    if ((T)6.0 * diff * cord > diff * diff) L = (T)3.0 * qq - (T)2.0 * R;
+    if (-diff * diff > (T)6.0 * diff * cord) R = (T)3.0 * qq - (T)2.0 * L;
+    ql[i] = L;
+    qr[i] = R;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // VanLeerX_PPA_d (fargo_ppa_d.c:58-75)
+    const int im = i > 0 ? i - 1 : nx - 1;
+    T ksi, s;
+    if (v[i] > (T)0.0) {
+      ksi = v[i] * dt / zsx(m, g, i, j, k);
+      s = qr[im] + ksi * (q[im] - qr[im]);
+      s += ksi * ((T)1.0 - ksi) * ((T)2.0 * q[im] - qr[im] - ql[im]);
+    } else {
+      ksi = -v[i] * dt / zsx(m, g, i, j, k);
+      s = ql[i] + ksi * (q[i] - ql[i]);
+      s += ksi * ((T)1.0 - ksi) * ((T)2.0 * q[i] - qr[i] - ql[i]);
+    }
+    qs[i] = s;
+  }
+  __syncthreads();
+}
+
+// UpdateX / UpdateDensityX (update_x.c:68-70, update_density_x.c:66-68)
+template <typename T>
+__device__ __forceinline__ T upd_x(const Geo<T> &g, int i, int ip, int j, int k, T v, T qs, T rs, T vp, T qsp,
+                                   T rsp, T dt, bool dens) {
+  const T fl = dens ? (v * rs - vp * rsp) : (v * qs * rs - vp * qsp * rsp);
+  return fl * ld(g.sxj + j) * ld(g.sxk + k) * dt * ld(g.invvj + j) / (ld(g.syk + k) * ld(g.sxi + i));
+}
+
+template <typename T>
+__device__ void ring_pass(const Dims &m, const Geo<T> &g, int j, int k, RingSmem<T> &S, int nq, T dt, bool ppa) {
+  const int nx = m.nx;
+  // density interface values
+  if (!ppa) ring_vl_iface(m, g, j, k, S.rho, S.v, dt, S.slope, S.rs);
+  else ring_ppa_iface(m, g, j, k, S.rho, S.v, dt, S.slope, S.ql, S.qr, S.rs);
+  for (int q = 0; q < nq; q++) {
+    T *Q = S.q[q];
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) S.a[i] = Q[i] / S.rho[i];  // DivideByRho
+    __syncthreads();
+    if (!ppa) ring_vl_iface(m, g, j, k, S.a, S.v, dt, S.slope, S.qs);
+    else ring_ppa_iface(m, g, j, k, S.a, S.v, dt, S.slope, S.ql, S.qr, S.qs);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+      const int ip = i < nx - 1 ? i + 1 : 0;
+      Q[i] = Q[i] + upd_x(g, i, ip, j, k, S.v[i], S.qs[i], S.rs[i], S.v[ip], S.qs[ip], S.rs[ip], dt, false);
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    const int ip = i < nx - 1 ? i + 1 : 0;
+    S.a[i] = S.rho[i] + upd_x(g, i, ip, j, k, S.v[i], (T)0, S.rs[i], S.v[ip], (T)0, S.rs[ip], dt, true);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) S.rho[i] = S.a[i];
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_sweep_x(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
+                                                 T *rho, T *q0, T *q1, T *q2, T *q3, T *q4, T *q5,
+                                                 const T *__restrict__ vxt, const double *__restrict__ vxmed_t,
+                                                 int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  const int nx = m.nx;
+  const int j = jlo + blockIdx.x, k = m.is3d ? klo + blockIdx.y : 0;
+  RingSmem<T> S;
+  S.rho = sm; S.v = sm + nx; S.rs = sm + 2 * nx; S.a = sm + 3 * nx; S.slope = sm + 4 * nx;
+  S.qs = sm + 5 * nx; S.ql = sm + 6 * nx; S.qr = sm + 7 * nx;
+  for (int q = 0; q < nq; q++) S.q[q] = sm + (8 + q) * nx;
+  T *qg[6] = {q0, q1, q2, q3, q4, q5};
+  const double dtd = scp->dt;
+  const T dt = (T)dtd;
+  const double vm = vxmed_t[j + k * m.sy];
+  const long long lr = m.l(0, j, k);
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    S.rho[i] = rho[lr + i];
+    for (int q = 0; q < nq; q++) S.q[q][i] = qg[q][lr + i];
+    // ComputeResidual (compute_residual.c:68-73): residual velocity
+    S.v[i] = (T)((double)vxt[lr + i] - vm);
+  }
+  __syncthreads();
+  ring_pass(m, g, j, k, S, nq, dt, false);
+  // uniform fractional velocity (ntilde - nround) * dx / dt, in FP64
+  __shared__ int s_nsh;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    const double zx = (double)zsx(m, gd, i, j, k);
+    const double ntilde = vm * dtd / zx;
+    const double nround = floor(ntilde + 0.5);
+    S.v[i] = (T)((ntilde - nround) * zx / dtd);
+    if (i == 0) {
+      s_nsh = (int)nround;
+      if (nshift_out) nshift_out[j + k * m.sy] = (int)nround;
+    }
+  }
+  __syncthreads();
+  const int nsh = s_nsh;
+  ring_pass(m, g, j, k, S, nq, dt, true);
+  // AdvectSHIFT (advect_shift.c:49-54)
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    int it = i - nsh;
+    it %= nx;
+    if (it < 0) it += nx;
+    rho[lr + i] = S.rho[it];
+    for (int q = 0; q < nq; q++) qg[q][lr + i] = S.q[q][it];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// NewVelocity_x/y/z (newvel_x.c:81, newvel_y.c:70, newvel_z.c:66-69) and
+// StockholmBoundary (stockholm.c:129-185) on the active cells; writes the
+// new state (rho, vx, vy, vz).
+template <typename T>
+__global__ void __launch_bounds__(256) k_newvel(Dims m, Geo<T> g, const T *__restrict__ rt, const T *__restrict__ mpx,
+                                                const T *__restrict__ mmx, const T *__restrict__ mpy,
+                                                const T *__restrict__ mmy, const T *__restrict__ mpz,
+                                                const T *__restrict__ mmz, T *__restrict__ rho, T *__restrict__ vx,
+                                                T *__restrict__ vy, T *__restrict__ vz, const T *__restrict__ rho0,
+                                                const T *__restrict__ vx0, const T *__restrict__ vy0,
+                                                const T *__restrict__ vz0, const double *__restrict__ ramps,
+                                                int stockholm, const fb_scalars *__restrict__ scp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = FB_NGH + blockIdx.y;
+  const int k = m.is3d ? FB_NGH + blockIdx.z : 0;
+  if (i >= m.nx) return;
+  const long long l = m.l(i, j, k);
+  const int im = i > 0 ? i - 1 : m.nx - 1;
+  const long long lxm = i > 0 ? l - 1 : l + (m.nx - 1);
+  const T of = (T)scp->omegaframe;
+  const T syk = ld(g.syk + k), sxi = ld(g.sxi + i), sxim = ld(g.sxi + im), ivj = ld(g.invvj + j);
+  const T r = rt[l];
+  T nvx, nvy, nvz = 0;
+  {
+    const T rc = m.sph ? ld(g.ymed + j) * ld(g.sin_zmed + k) : ld(g.ymed + j);
+    nvx = (mmx[l] * syk * sxi / ivj + mpx[lxm] * syk * sxim / ivj) /
+              ((r * syk * sxi / ivj + rt[lxm] * syk * sxim / ivj) * rc) - of * rc;
+  }
+  {
+    const T ivjm = ld(g.invvj + j - 1);
+    const long long lym = l - m.pitch;
+    nvy = (mmy[l] * syk * sxi / ivj + mpy[lym] * syk * sxi / ivjm) / (r * syk * sxi / ivj + rt[lym] * syk * sxi / ivjm);
+  }
+  if (m.is3d) {
+    const T sykm = ld(g.syk + k - 1);
+    const long long lzm = l - m.stride;
+    nvz = (mmz[l] * syk * sxi / ivj + mpz[lzm] * sykm * sxi / ivj) / (r * syk * sxi / ivj + rt[lzm] * sykm * sxi / ivj);
+    if (m.sph) nvz /= ld(g.ymed + j);
+  }
+  T nr = r;
+  if (stockholm) {
+    const double dtd = scp->dt;
+    const T dt = (T)dtd;
+    const double rampy = ramps[j], rampz = m.is3d ? ramps[m.sy + k] : 0.0, rampzz = m.is3d ? ramps[m.sy + m.sz + k] : 0.0;
+    const T ramp = (T)(rampy + rampz), rampi = (T)(rampy + rampzz);
+    const T tau = ld(g.tau_j + j);
+    const int l2 = j + k * m.sy;
+    if (ramp > (T)0.0) {
+      const T taud = tau / ramp;
+      nr = (nr * taud + rho0[l2] * dt) / (dt + taud);
+      T radius = ld(g.ymed + j);
+      if (m.sph) radius *= ld(g.sin_zmed + k);
+      T vx0t = vx0[l2];
+      vx0t -= (of - (T)scp->omegaframe0) * radius;
+      nvx = (nvx * taud + vx0t * dt) / (dt + taud);
+      nvy = (nvy * taud + vy0[l2] * dt) / (dt + taud);
+    }
+    if (m.is3d && rampi > (T)0.0) {
+      const T taud = tau / rampi;
+      nvz = (nvz * taud + vz0[l2] * dt) / (dt + taud);
+    }
+  }
+  rho[l] = nr;
+  vx[l] = nvx;
+  vy[l] = nvy;
+  if (m.is3d) vz[l] = nvz;
+}
+
+}  // namespace fb
+
+namespace fb {
+
+// ---------------------------------------------------------------------------
+// Sources, 3D spherical: the same fusion as k_sources_cyl over a TX x TY tile
+// of one colatitude layer, with the inputs of layers k-1..k+1 staged and the
+// six stress components of visctensor_sph (visctensor_sph.c:141-213) computed
+// where addviscosity_sph (addviscosity_sph.c:74-126) reads them.
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX *TY) k_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
+    const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx, const T *__restrict__ vy,
+    const T *__restrict__ vz, T *__restrict__ vxt, T *__restrict__ vyt, T *__restrict__ vzt,
+    const fb_scalars *__restrict__ scp, int dust, int viscous) {
+  constexpr int W = TX + 2, H = TY + 2;
+  __shared__ T s_rho[3][H][W], s_cs[3][H][W], s_vx[3][H][W], s_vy[3][H][W], s_vz[3][H][W];
+  __shared__ double s_pot[2][H][W];   // layers k-1, k
+  __shared__ T t_xx[2][H][W], t_zz[2][H][W], t_yy[H][W];   // planes k-1, k
+  __shared__ T t_xz[2][H][W], t_zy[2][H][W], t_yx[H][W];   // planes k, k+1
+  __shared__ fb_scalars sc;
+  const int i0 = blockIdx.x * TX, j0 = FB_NGH + blockIdx.y * TY, kc = FB_NGH + blockIdx.z;
+  const int tid = threadIdx.x + threadIdx.y * TX;
+  if (tid == 0) sc = *scp;
+  __syncthreads();
+  const double dt = sc.dt;
+  const T domega = (T)sc.domega, of = (T)sc.omegaframe;
+  for (int e = tid; e < 3 * H * W; e += TX * TY) {
+    const int lk = e / (H * W), rem = e - lk * H * W, lj = rem / W, li = rem - lj * W;
+    const int j = j0 - 1 + lj, k = kc - 1 + lk, i = wrapx(i0 - 1 + li, m.nx);
+    if (j < m.sy && i0 - 1 + li <= m.nx) {
+      const long long l = m.l(i, j, k);
+      const T r = rho[l], c = cs[l];
+      s_rho[lk][lj][li] = r;
+      s_cs[lk][lj][li] = c;
+      s_vx[lk][lj][li] = vx[l] - domega * ld(g.ymed + j) * ld(g.sin_zmed + k);
+      s_vy[lk][lj][li] = vy[l];
+      s_vz[lk][lj][li] = vz[l];
+      if (lk < 2) s_pot[lk][lj][li] = potential_at(m, gd, sc, i, j, k);
+    }
+  }
+  __syncthreads();
+  if (viscous) {
+    const T nu = (T)sc.nu, alpha = (T)sc.alpha;
+    for (int e = tid; e < 3 * H * W; e += TX * TY) {
+      const int lk = e / (H * W), rem = e - lk * H * W, lj = rem / W, li = rem - lj * W;
+      const int j = j0 - 1 + lj, k = kc - 1 + lk, i = wrapx(i0 - 1 + li, m.nx);
+      if (j >= m.sy - 1 || i0 - 1 + li > m.nx) continue;
+      const bool diag = (lk <= 1) && li <= TX && lj <= TY && (lk == 1 || (li >= 1 && lj >= 1));
+      const bool offd = (lk >= 1) && li >= 1 && lj >= 1 && (lk == 1 || (li <= TX && lj <= TY));
+      if (!diag && !offd) continue;
+      T visc = nu, viscm = nu, visczm = nu, visczmym = nu;
+      const T e0 = s_cs[lk][lj][li];
+      if (m.alpha) {
+        visc = alpha * e0 * e0 * ld(g.visc_j + j);
+        if (li >= 1 && lj >= 1) {
+          const T s1 = e0 + s_cs[lk][lj][li - 1] + s_cs[lk][lj - 1][li] + s_cs[lk][lj - 1][li - 1];
+          viscm = alpha * (T)0.0625 * s1 * s1 * ld(g.viscm_j + j);
+        }
+        if (lk >= 1 && li >= 1) {
+          const T s2 = e0 + s_cs[lk - 1][lj][li] + s_cs[lk][lj][li - 1] + s_cs[lk - 1][lj][li - 1];
+          visczm = alpha * (T)0.0625 * s2 * s2 * ld(g.visc_j + j);
+        }
+        if (lk >= 1 && lj >= 1) {
+          const T s3 = e0 + s_cs[lk - 1][lj][li] + s_cs[lk][lj - 1][li] + s_cs[lk - 1][lj - 1][li];
+          visczmym = alpha * (T)0.0625 * s3 * s3 * ld(g.viscm_j + j);
+        }
+      }
+      const T r = s_rho[lk][lj][li];
+      const T sxi = ld(g.sxi + i), syk = ld(g.syk + k);
+      const T ym = ld(g.ymed + j), yi = ld(g.ymin + j);
+      const T szm = ld(g.sin_zmed + k), czm = ld(g.cos_zmed + k);
+      if (diag) {
+        const T dvx = s_vx[lk][lj][li + 1] - s_vx[lk][lj][li];
+        T div_v = 0.0;
+        div_v += dvx * ld(g.sxj + j) * ld(g.sxk + k);
+        div_v += (s_vy[lk][lj + 1][li] * ld(g.syj + j + 1) * syk * sxi - s_vy[lk][lj][li] * ld(g.syj + j) * syk * sxi);
+        div_v += (s_vz[lk + 1][lj][li] * ld(g.szj + j) * ld(g.szk + k + 1) * sxi -
+                  s_vz[lk][lj][li] * ld(g.szj + j) * ld(g.szk + k) * sxi);
+        div_v *= (T)(2.0 / 3.0) * ld(g.invvj + j) / (syk * sxi);
+        T txx = visc * r * ((T)2.0 * dvx / zsx(m, g, i, j, k) - div_v);
+        txx += visc * r * (s_vy[lk][lj + 1][li] + s_vy[lk][lj][li]) / ym;
+        txx += visc * r * (s_vz[lk + 1][lj][li] + s_vz[lk][lj][li]) * czm / (szm * ym);
+        T tzz = visc * r * ((T)2.0 * (s_vz[lk + 1][lj][li] - s_vz[lk][lj][li]) / (ym * (ld(g.zmin + k + 1) - ld(g.zmin + k))) - div_v);
+        tzz += visc * r * (s_vy[lk][lj][li] + s_vy[lk][lj + 1][li]) / ym;
+        t_xx[lk][lj][li] = txx;
+        t_zz[lk][lj][li] = tzz;
+        if (lk == 1)
+          t_yy[lj][li] = visc * r * ((T)2.0 * (s_vy[lk][lj + 1][li] - s_vy[lk][lj][li]) / (ld(g.ymin + j + 1) - yi) - div_v);
+      }
+      if (offd) {
+        const T dzm = ld(g.zmed + k) - ld(g.zmed + k - 1), szi = ld(g.sin_zmin + k);
+        const T txz = visczm * (T)0.25 * (r + s_rho[lk - 1][lj][li] + s_rho[lk][lj][li - 1] + s_rho[lk - 1][lj][li - 1]) *
+                      ((s_vx[lk][lj][li] / szm - s_vx[lk - 1][lj][li] / ld(g.sin_zmed + k - 1)) * szi / (ym * dzm) +
+                       ((s_vz[lk][lj][li] - s_vz[lk][lj][li - 1]) * ld(g.invdiffxmed + i) / (szi * ym)));
+        const T tzy = visczmym * (T)0.25 * (r + s_rho[lk][lj - 1][li] + s_rho[lk - 1][lj][li] + s_rho[lk - 1][lj - 1][li]) *
+                      ((s_vz[lk][lj][li] - s_vz[lk][lj - 1][li]) / (ym - ld(g.ymed + j - 1)) -
+                       (T)0.5 * (s_vz[lk][lj][li] + s_vz[lk][lj - 1][li]) / yi +
+                       (s_vy[lk][lj][li] - s_vy[lk - 1][lj][li]) / (yi * dzm));
+        t_xz[lk - 1][lj][li] = txz;
+        t_zy[lk - 1][lj][li] = tzy;
+        if (lk == 1)
+          t_yx[lj][li] = viscm * (T)0.25 * (r + s_rho[lk][lj][li - 1] + s_rho[lk][lj - 1][li] + s_rho[lk][lj - 1][li - 1]) *
+                         ((s_vy[lk][lj][li] - s_vy[lk][lj][li - 1]) * ld(g.invdiffxmed + i) / (yi * szm) +
+                          (s_vx[lk][lj][li] - s_vx[lk][lj - 1][li]) / (ym - ld(g.ymed + j - 1)) -
+                          (T)0.5 * (s_vx[lk][lj][li] + s_vx[lk][lj - 1][li]) / yi);
+      }
+    }
+    __syncthreads();
+  }
+  const int li = threadIdx.x + 1, lj = threadIdx.y + 1;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y, k = kc;
+  if (i >= m.nx || j > m.ny + FB_NGH - 1) return;
+  const int im = wrapx(i - 1, m.nx);
+  const long long l = m.l(i, j, k);
+  auto P = [&](int a, int b, int c) -> T { return s_rho[a][b][c] * s_cs[a][b][c] * s_cs[a][b][c]; };
+  const T r = s_rho[1][lj][li], rxm = s_rho[1][lj][li - 1], rym = s_rho[1][lj - 1][li], rzm = s_rho[0][lj][li];
+  const T izx = izsxmed(m, g, i, j, k);
+  const T ym = ld(g.ymed + j), ymm = ld(g.ymed + j - 1), yi = ld(g.ymin + j), yip = ld(g.ymin + j + 1),
+          yim = ld(g.ymin + j - 1);
+  const T zi = ld(g.zmin + k), zip = ld(g.zmin + k + 1), zim = ld(g.zmin + k - 1);
+  const T zm = ld(g.zmed + k), zmm = ld(g.zmed + k - 1);
+  const T szm = ld(g.sin_zmed + k), czm = ld(g.cos_zmed + k), szi = ld(g.sin_zmin + k), czi = ld(g.cos_zmin + k);
+  // SubStep1_x
+  const T dxmed = (T)0.5 * (ld(g.sxi + i) + ld(g.sxi + im));
+  const T dtorx = (T)2. * (T)dt / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * dxmed;
+  T ax = s_vx[1][lj][li];
+  if (!dust) ax -= dtorx * (P(1, lj, li) - P(1, lj, li - 1)) * izx;
+  ax -= (T)((s_pot[1][lj][li] - s_pot[1][lj][li - 1]) * dt) * izx;
+  // SubStep1_y (spherical branch, substep1_y.c:212-217)
+  const T dtory = (T)2.0 * (T)dt / (r * (yip - yi) + rym * (yi - yim)) * (ym - ymm);
+  T ay = s_vy[1][lj][li];
+  if (!dust) ay -= dtory * (P(1, lj, li) - P(1, lj - 1, li)) / (ym - ymm);
+  {
+    T vphi = (T)0.25 * (s_vx[1][lj][li] + s_vx[1][lj][li + 1] + s_vx[1][lj - 1][li] + s_vx[1][lj - 1][li + 1]);
+    vphi += yi * szm * of;
+    const T vzz = (T)0.25 * (s_vz[1][lj][li] + s_vz[2][lj][li] + s_vz[1][lj - 1][li] + s_vz[2][lj - 1][li]);
+    ay += (vphi * vphi + vzz * vzz) / yi * (T)dt;
+  }
+  ay -= (T)((s_pot[1][lj][li] - s_pot[1][lj - 1][li]) * dt / (double)(ym - ymm));
+  // SubStep1_z (spherical branch, substep1_z.c:172-180)
+  const T dtorz = (T)2.0 * (T)dt / (r * (zip - zi) + rzm * (zi - zim)) * (zm - zmm);
+  T vphz = (T)0.25 * (s_vx[1][lj][li] + s_vx[1][lj][li + 1] + s_vx[0][lj][li] + s_vx[0][lj][li + 1]);
+  vphz += ym * szi * of;
+  T az = s_vz[1][lj][li];
+  if (!dust) az -= dtorz * (P(1, lj, li) - P(0, lj, li)) / (ym * (zm - zmm));
+  az += vphz * vphz * czi / (szi * ym) * (T)dt;
+  az -= (T)((s_pot[1][lj][li] - s_pot[0][lj][li]) * dt / (double)(ym * (zm - zmm)));
+  if (viscous) {
+    // addviscosity_sph
+    const T txx = t_xx[1][lj][li];
+    ax += (T)2.0 * (txx - t_xx[1][lj][li - 1]) * izx / ((r + rxm)) * (T)dt;
+    ax += (T)2.0 * (yip * yip * t_yx[lj + 1][li] - yi * yi * t_yx[lj][li]) / ((yip - yi) * ym * ym * (rxm + r)) * (T)dt;
+    ax += (t_yx[lj + 1][li] + t_yx[lj][li]) / ((rxm + r) * ym) * (T)dt;
+    ax += (T)2.0 * (t_xz[1][lj][li] - t_xz[0][lj][li]) / (zsz(m, g, j, k) * (rxm + r)) * (T)dt;
+    ax += (T)2.0 * (t_xz[1][lj][li] + t_xz[0][lj][li]) * czm / (szm * ym * (rxm + r)) * (T)dt;
+
+    ay += (T)2.0 * (ym * ym * t_yy[lj][li] - ymm * ymm * t_yy[lj - 1][li]) / ((ym - ymm) * (r + rym) * yi * yi) * (T)dt;
+    ay += (T)2.0 * (t_yx[lj][li + 1] - t_yx[lj][li]) / ((ld(g.xmin + i + 1) - ld(g.xmin + i)) * yi * szm * (r + rym)) * (T)dt;
+    ay -= (txx + t_xx[1][lj - 1][li]) / (yi * (r + rym)) * (T)dt;
+    ay -= (t_zz[1][lj][li] + t_zz[1][lj - 1][li]) / (yi * (r + rym)) * (T)dt;
+    ay += (T)2.0 * (t_zy[1][lj][li] * ld(g.sin_zmin + k + 1) - t_zy[0][lj][li] * szi) / ((zip - zi) * yi * szm * (r + rym)) * (T)dt;
+
+    az += (T)2.0 * (t_zz[1][lj][li] * szm - t_zz[0][lj][li] * ld(g.sin_zmed + k - 1)) / ((zm - zmm) * ym * szi * (r + rzm)) * (T)dt;
+    az += (T)2.0 * (t_xz[0][lj][li + 1] - t_xz[0][lj][li]) / ((ld(g.sxi + i) * ym * szi) * (r + rzm)) * (T)dt;
+    az += (T)2.0 * (yip * yip * yip * t_zy[0][lj + 1][li] - yi * yi * yi * t_zy[0][lj][li]) / ((yip - yi) * ym * ym * ym * (r + rzm)) * (T)dt;
+    az -= (txx + t_xx[0][lj][li]) * czi / (ym * szi * (r + rzm)) * (T)dt;
+  }
+  // SubStep2_a / SubStep2_b
+  const T c2 = (T)FB_CVNR;
+  T dv = s_vx[1][lj][li + 1] - s_vx[1][lj][li];
+  const T qx = dv < (T)0.0 ? c2 * c2 * r * dv * dv : (T)0.0;
+  dv = s_vx[1][lj][li] - s_vx[1][lj][li - 1];
+  const T qxm = dv < (T)0.0 ? c2 * c2 * rxm * dv * dv : (T)0.0;
+  dv = s_vy[1][lj + 1][li] - s_vy[1][lj][li];
+  const T qy = dv < (T)0.0 ? c2 * c2 * r * dv * dv : (T)0.0;
+  dv = s_vy[1][lj][li] - s_vy[1][lj - 1][li];
+  const T qym = dv < (T)0.0 ? c2 * c2 * rym * dv * dv : (T)0.0;
+  dv = s_vz[2][lj][li] - s_vz[1][lj][li];
+  const T qz = dv < (T)0.0 ? c2 * c2 * r * dv * dv : (T)0.0;
+  dv = s_vz[1][lj][li] - s_vz[0][lj][li];
+  const T qzm = dv < (T)0.0 ? c2 * c2 * rzm * dv * dv : (T)0.0;
+  ax += -(T)2.0 * (T)dt * dxmed * (qx - qxm) / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * izx;
+  ay += -(T)2.0 * (qy - qym) / (r * (yip - yi) + rym * (yi - yim)) * (T)dt;
+  {
+    const T dzmed = zm - zmm, dzrho1 = zip - zi, dzrho2 = zi - zim;
+    az += -(T)2.0 * dzmed * (qz - qzm) / (r * dzrho1 + rzm * dzrho2) * (T)dt / (ym * (zm - zmm));
+  }
+  vxt[l] = ax;
+  vyt[l] = ay;
+  vzt[l] = az;
+}
+
+}  // namespace fb

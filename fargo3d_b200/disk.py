@@ -1,0 +1,85 @@
+"""Python mirror of the reference's run loop over the C-ABI.
+
+`Disk` plays the part of one FARGO3D run (main.c): it owns a disk's device
+state, applies the initial boundaries and Stockholm profiles (main.c:311-316)
+and advances hydro steps (main.c:361-448) on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .setups import DiskConfig, initial_state
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+class Disk:
+    def __init__(self, cfg: DiskConfig, precision: str = "fp64", device: int = 0):
+        self.cfg = cfg
+        self.precision = precision
+        L = _abi.lib()
+        self._p = _abi.params_of(cfg)
+        h = C.c_void_p()
+        prec = _abi.FB_FP64 if precision == "fp64" else _abi.FB_FP32
+        _abi.check(L.fb_disk_create(C.byref(self._p), prec, device, C.byref(h)))
+        self._h = h
+        self.shape = cfg.shape
+
+    # ------------------------------------------------------------------ state
+    def set_state(self, rho, vx, vy, vz, cs, fluid: int = 0):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(self.shape)
+                for a in (rho, vx, vy, vz, cs)]
+        _abi.check(_abi.lib().fb_disk_set_state(self._h, fluid, *[_ptr(a) for a in arrs]))
+
+    def state(self, fluid: int = 0):
+        out = [np.empty(self.shape) for _ in range(4)]
+        _abi.check(_abi.lib().fb_disk_get_state(self._h, fluid, *[_ptr(a) for a in out]))
+        return {"rho": out[0], "vx": out[1], "vy": out[2], "vz": out[3]}
+
+    def initialize(self):
+        _abi.check(_abi.lib().fb_disk_initialize(self._h))
+
+    def load_initial_state(self):
+        for f in range(self.cfg.nfluids):
+            self.set_state(*initial_state(self.cfg, f), fluid=f)
+        self.initialize()
+
+    # ------------------------------------------------------------------ steps
+    def step(self, dt_interval: float = 1e30) -> float:
+        dt = C.c_double()
+        _abi.check(_abi.lib().fb_disk_step(self._h, dt_interval, C.byref(dt)))
+        return dt.value
+
+    def run(self, nsteps: int, dt_interval: float = 1e30):
+        return [self.step(dt_interval) for _ in range(nsteps)]
+
+    def scalars(self):
+        o = np.zeros(8)
+        _abi.check(_abi.lib().fb_disk_get_scalars(self._h, _ptr(o)))
+        return o
+
+    def device_fields(self, fluid: int = 0):
+        ptrs = (C.c_void_p * 5)()
+        esz = C.c_size_t()
+        _abi.check(_abi.lib().fb_disk_device_fields(self._h, fluid, ptrs, C.byref(esz)))
+        return [p for p in ptrs], esz.value
+
+    @property
+    def stream(self) -> int:
+        return _abi.lib().fb_disk_stream(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _abi.lib().fb_disk_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

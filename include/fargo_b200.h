@@ -1,0 +1,95 @@
+/*
+ * fargo_b200.h -- C-ABI of the B200 FARGO3D hydro step (libfargo_b200.so).
+ *
+ * The library advances protoplanetary disks with FARGO3D's hydro time step
+ * (main.c:361-448 of the reference): CFL time step, sources (SubStep1/2,
+ * viscosity, potential), FARGO transport (van Leer in r / theta, residual van
+ * Leer + PPA + integer shift in phi), Stockholm damping and ghost boundaries.
+ * Fields live in device memory in the reference's layout (x fastest, then y,
+ * then z; NGHY = NGHZ = 3 ghost rows/layers, periodic x without ghosts).
+ *
+ * Every entry point returns FB_OK (0) or a negative FB_ERR_* code from
+ * fb_abi.h; fb_last_error() describes the last failure of the calling thread.
+ * The product path has no CPU fallback: without a usable CUDA device every
+ * call fails with FB_ERR_CUDA.
+ *
+ * Reference interfaces replaced (paths inside the reference's src/):
+ *   fb_disk_step        one pass of the DT loop body, main.c:366-431, i.e.
+ *                       ComputeVmed + cfl + CflFluidsMin + Sources (algogas.c:30)
+ *                       + Collisions + Transport (algogas.c:135) +
+ *                       StockholmBoundary + FillGhosts, the functions bound by
+ *                       ChangeArch (change_arch.c:163-567) to their _gpu flavours
+ *   fb_disk_initialize  FillGhosts + init_stockholm (main.c:311-316)
+ *   fb_disk_set_state /
+ *   fb_disk_get_state   Input_GPU / Output_GPU host<->device transfers of the
+ *                       primitive Fields (fresh.c:187-276)
+ */
+#ifndef FARGO_B200_H
+#define FARGO_B200_H
+
+#include <stddef.h>
+#include "fb_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Run-time parameters of one disk.  Field names follow the reference's .par
+ * keys (std/stdpar.par); the layout is stable (append-only). */
+typedef struct {
+  int nx, ny, nz;              /* Nx, Ny, Nz; nz <= 1 selects a 2D (X,Y) mesh   */
+  int spherical;               /* 0: CYLINDRICAL (2D), 1: SPHERICAL (3D)        */
+  int log_spacing;             /* Spacing Log                                   */
+  double xmin, xmax, ymin, ymax, zmin, zmax;
+  double aspectratio, sigmaslope, flaringindex;
+  double nu;                   /* Nu (VISCOSITY)                                */
+  double alpha; int alpha_visc;/* Alpha (ALPHAVISCOSITY when alpha_visc != 0)   */
+  double cfl;                  /* CFL                                           */
+  double omegaframe; int frame;/* OmegaFrame, Frame (FB_FRAME_*)                */
+  int indirect_term;           /* IndirectTerm                                  */
+  double thickness_smoothing, roche_smoothing, mass_taper;
+  double damping_zone, tau_damp, killing_bc_colatitude;
+  int nplanets;
+  double pl_dist[FB_MAXPLANETS], pl_mass[FB_MAXPLANETS];
+  int pl_feeldisk[FB_MAXPLANETS], pl_feelothers[FB_MAXPLANETS];
+  double eccentricity, inclination;
+  int nfluids;                 /* 1: gas; >1: gas + dust with implicit drag      */
+  double invstokes[FB_MAXFLUIDS];
+  int stockholm;               /* STOCKHOLM damping                             */
+} fb_params;
+
+typedef struct fb_disk fb_disk;
+
+/* Create a disk on CUDA device `device` with FB_FP64 or FB_FP32 fields. */
+int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out);
+int fb_disk_destroy(fb_disk *d);
+
+/* Host <-> device copies of one fluid's state, full stored arrays with ghosts
+ * ((Nz+6 or 1) x (Ny+6) x Nx doubles).  Null pointers are skipped; cs only on
+ * set (isothermal sound speed, FARGO3D's Energy field). */
+int fb_disk_set_state(fb_disk *d, int fluid, const double *rho, const double *vx, const double *vy,
+                      const double *vz, const double *cs);
+int fb_disk_get_state(fb_disk *d, int fluid, double *rho, double *vx, double *vy, double *vz);
+
+int fb_disk_initialize(fb_disk *d);
+
+/* One hydro step: dt = min(CFL dt, what is left of a DT interval of length
+ * dt_interval), exactly as main.c:388-395.  *dt_out receives dt. */
+int fb_disk_step(fb_disk *d, double dt_interval, double *dt_out);
+
+/* [0] PhysicalTime [1] OMEGAFRAME [2] last dt [3..6] planet 0 x, y, vx, vy [7] Domega */
+int fb_disk_get_scalars(fb_disk *d, double out8[8]);
+
+/* Device pointers of one fluid's state (rho, vx, vy, vz, cs) and the element
+ * size, for callers that keep their inputs on the device. */
+int fb_disk_device_fields(fb_disk *d, int fluid, void *ptrs5[5], size_t *elem_size);
+
+/* Stream the disk's kernels run on (a cudaStream_t). */
+void *fb_disk_stream(fb_disk *d);
+
+const char *fb_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -99,13 +99,17 @@ class Disk:
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         if kind == "ref":
-            # Each reference library holds one disk in its globals: load a
-            # fresh private copy per Disk (dlopen of a per-instance symlink).
+            # Each reference library holds one disk in its globals (and in
+            # function-level statics such as potential.c's alreadycalculated):
+            # load a fresh private copy per Disk.  dlopen identifies a library
+            # by its inode, so the copy must be a new file, not a link.
+            import shutil
             import tempfile
             tmp = tempfile.mkdtemp(prefix="fargo_ref_")
-            link = os.path.join(tmp, os.path.basename(path))
-            os.symlink(path, link)
-            lib = C.CDLL(link, mode=os.RTLD_NOW | os.RTLD_LOCAL)
+            copy = os.path.join(tmp, os.path.basename(path))
+            shutil.copyfile(path, copy)
+            lib = C.CDLL(copy, mode=os.RTLD_NOW | os.RTLD_LOCAL)
+            shutil.rmtree(tmp, ignore_errors=True)
         else:
             lib = Disk._libs.get(path)
             if lib is None:
