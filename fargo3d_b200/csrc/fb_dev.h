@@ -74,7 +74,8 @@ typedef struct {
   int fb_launch_cfl_##SUF(const fb_disk_dev *d, int fluid, void *stream);           \
   int fb_launch_sources_##SUF(const fb_disk_dev *d, int fluid, void *stream);       \
   int fb_launch_bnd_##SUF(const fb_disk_dev *d, int fluid, int vtemp, void *stream); \
-  int fb_launch_transport_##SUF(const fb_disk_dev *d, int fluid, void *stream);     \
+  int fb_launch_sweep_cols_##SUF(const fb_disk_dev *d, int fluid, void *stream);    \
+  int fb_launch_sweep_x_##SUF(const fb_disk_dev *d, int fluid, void *stream);       \
   int fb_launch_newvel_##SUF(const fb_disk_dev *d, int fluid, void *stream);
 
 FB_DECL_LAUNCHERS(f64)

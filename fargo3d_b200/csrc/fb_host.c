@@ -78,7 +78,24 @@ struct fb_disk {
   double *h_dtmin;              /* pinned */
   void *allocs[MAXALLOC];
   int nalloc;
+  /* optional per-launch timing (fb_disk_profile) */
+  int prof;
+  int nev;
+  cudaEvent_t ev[32];
+  const char *evname[32];
+  float prof_ms[32];
+  int prof_n;
 };
+
+/* record an event after a launch when profiling; names label the interval
+ * that ends at this event */
+static void mark(fb_disk *D, const char *name) {
+  if (!D->prof || D->nev >= 32) return;
+  if (!D->ev[D->nev]) cudaEventCreate(&D->ev[D->nev]);
+  cudaEventRecord(D->ev[D->nev], D->stream);
+  D->evname[D->nev] = name;
+  D->nev++;
+}
 
 /* ------------------------------------------------------------------------ */
 static int dalloc(fb_disk *D, void **p, size_t bytes) {
@@ -539,6 +556,8 @@ int fb_disk_destroy(fb_disk *D) {
   if (D->stream) cudaStreamSynchronize(D->stream);
   for (i = 0; i < D->nalloc; i++) cudaFree(D->allocs[i]);
   if (D->h_dtmin) cudaFreeHost(D->h_dtmin);
+  for (i = 0; i < 32; i++)
+    if (D->ev[i]) cudaEventDestroy(D->ev[i]);
   if (D->stream) cudaStreamDestroy(D->stream);
   free(D->xmin); free(D->ymin); free(D->zmin); free(D->xmed); free(D->ymed); free(D->zmed);
   free(D->invdiffxmed); free(D->sxi); free(D->sxj); free(D->syj); free(D->szj); free(D->invvj);
@@ -645,8 +664,12 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   /* ComputeVmed(Vx) + cfl (main.c:366-388) */
   CU(cudaMemcpyAsync(D->d.dtmin, &start_bits, 8, cudaMemcpyHostToDevice, D->stream));
   if ((rc = push_scalars(D))) return rc;
+  D->nev = 0;
+  mark(D, "start");
   for (f = 0; f < D->p.nfluids; f++) LCH(LAUNCH(rowsum, &D->d, f, 0, D->stream));
+  mark(D, "rowsum");
   for (f = 0; f < D->p.nfluids; f++) LCH(LAUNCH(cfl, &D->d, f, D->stream));
+  mark(D, "cfl");
   CU(cudaMemcpyAsync(D->h_dtmin, D->d.dtmin, 8, cudaMemcpyDeviceToHost, D->stream));
   CU(cudaStreamSynchronize(D->stream));
   /* CflFluidsMin (cfl_fluids_min.c:3-22) */
@@ -671,21 +694,36 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   D->sc.domega = D->p.frame != FB_FRAME_FIXED ? D->domega : 0.0;
   if ((rc = push_scalars(D))) return rc;
   /* Sources (algogas.c:30-120) with its closing FillGhosts on V_temp */
+  mark(D, "host_scalars");
   for (f = 0; f < D->p.nfluids; f++) {
     LCH(LAUNCH(sources, &D->d, f, D->stream));
+    mark(D, "sources");
     LCH(LAUNCH(bnd, &D->d, f, 1, D->stream));
+    mark(D, "bnd_vtemp");
   }
   /* Transport (algogas.c:135-159) */
   for (f = 0; f < D->p.nfluids; f++) {
     LCH(LAUNCH(rowsum, &D->d, f, 1, D->stream));
-    LCH(LAUNCH(transport, &D->d, f, D->stream));
+    mark(D, "rowsum_vtemp");
+    LCH(LAUNCH(sweep_cols, &D->d, f, D->stream));
+    mark(D, "sweep_cols");
+    LCH(LAUNCH(sweep_x, &D->d, f, D->stream));
+    mark(D, "sweep_x");
   }
   D->phys_time += dt;
   D->step_count++;
   /* NewVelocity + StockholmBoundary + FillGhosts (main.c:427-431) */
   for (f = 0; f < D->p.nfluids; f++) {
     LCH(LAUNCH(newvel, &D->d, f, D->stream));
+    mark(D, "newvel");
     LCH(LAUNCH(bnd, &D->d, f, 0, D->stream));
+    mark(D, "bnd");
+  }
+  if (D->prof && D->nev > 1) {
+    int i;
+    CU(cudaEventSynchronize(D->ev[D->nev - 1]));
+    D->prof_n = D->nev - 1;
+    for (i = 1; i < D->nev; i++) cudaEventElapsedTime(&D->prof_ms[i - 1], D->ev[i - 1], D->ev[i]);
   }
   D->last_dt = dt;
   if (dt_out) *dt_out = dt;
@@ -709,3 +747,20 @@ int fb_disk_device_fields(fb_disk *D, int f, void *ptrs[5], size_t *esz) {
 }
 
 void *fb_disk_stream(fb_disk *D) { return D ? (void *)D->stream : NULL; }
+
+int fb_disk_profile(fb_disk *D, int enable) {
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  D->prof = enable;
+  return FB_OK;
+}
+
+int fb_disk_profile_read(fb_disk *D, float *ms, const char **names, int max) {
+  int i, n;
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  n = D->prof_n < max ? D->prof_n : max;
+  for (i = 0; i < n; i++) {
+    ms[i] = D->prof_ms[i];
+    names[i] = D->evname[i + 1];
+  }
+  return n;
+}

@@ -84,7 +84,7 @@ static int launch_bnd(const fb_disk_dev *d, int f, int vtemp, cudaStream_t st) {
 }
 
 template <typename T>
-static int launch_transport(const fb_disk_dev *d, int f, cudaStream_t st) {
+static int launch_sweep_cols(const fb_disk_dev *d, int f, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
   Geo<T> g = geo_of<T>(d->geom);
@@ -95,6 +95,7 @@ static int launch_transport(const fb_disk_dev *d, int f, cudaStream_t st) {
   T *rho_out;
   T *q[6];
   int nq;
+  (void)gd;
   if (!m.is3d) {
     nq = 4;
     QSrc<T> src = qsrc_from_v<T>(F, (T)0);
@@ -124,6 +125,21 @@ static int launch_transport(const fb_disk_dev *d, int f, cudaStream_t st) {
     k_sweep_col<T, 0, NS><<<gy, bx, 0, st>>>(m, g, sa, nq, ylo, yhi, zlo, rho_out, q[0], q[1], q[2], q[3], q[4],
                                              q[5], d->scal_dev);
   }
+  return (int)cudaGetLastError();
+}
+
+template <typename T>
+static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
+  const fb_fluid_dev &F = d->fl[f];
+  Dims m = dims_of(*d);
+  Geo<T> g = geo_of<T>(d->geom);
+  Geo<double> gd = geo_of<double>(d->geomd);
+  const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;
+  const bool b = m.is3d;
+  const int nq = b ? 6 : 4;
+  T *rho_out = (T *)(b ? F.rho_b : F.rho_a);
+  T *q[6] = {(T *)(b ? F.mpx_b : F.mpx), (T *)(b ? F.mmx_b : F.mmx), (T *)(b ? F.mpy_b : F.mpy),
+             (T *)(b ? F.mmy_b : F.mmy), (T *)(b ? F.mpz_b : F.mpz), (T *)(b ? F.mmz_b : F.mmz)};
   // azimuthal sweep, one CTA per ring
   const size_t smem = (size_t)(8 + nq) * m.nx * sizeof(T);
   static size_t configured = 0;
@@ -175,8 +191,11 @@ int FB_CAT(fb_launch_sources, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) 
 int FB_CAT(fb_launch_bnd, FB_SUF)(const fb_disk_dev *d, int fluid, int vtemp, void *s) {
   return fb::launch_bnd<FB_REAL>(d, fluid, vtemp, (cudaStream_t)s);
 }
-int FB_CAT(fb_launch_transport, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_transport<FB_REAL>(d, fluid, (cudaStream_t)s);
+int FB_CAT(fb_launch_sweep_cols, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
+  return fb::launch_sweep_cols<FB_REAL>(d, fluid, (cudaStream_t)s);
+}
+int FB_CAT(fb_launch_sweep_x, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
+  return fb::launch_sweep_x<FB_REAL>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_newvel, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
   return fb::launch_newvel<FB_REAL>(d, fluid, (cudaStream_t)s);

@@ -87,6 +87,12 @@ int fb_disk_device_fields(fb_disk *d, int fluid, void *ptrs5[5], size_t *elem_si
 /* Stream the disk's kernels run on (a cudaStream_t). */
 void *fb_disk_stream(fb_disk *d);
 
+/* Per-launch device timing of the following steps (CUDA events on the disk's
+ * stream).  fb_disk_profile_read returns the number of intervals written:
+ * ms[i] is the time of the launch group names[i] in the last profiled step. */
+int fb_disk_profile(fb_disk *d, int enable);
+int fb_disk_profile_read(fb_disk *d, float *ms, const char **names, int max);
+
 const char *fb_last_error(void);
 
 #ifdef __cplusplus
