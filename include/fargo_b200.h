@@ -93,6 +93,30 @@ void *fb_disk_stream(fb_disk *d);
 int fb_disk_profile(fb_disk *d, int enable);
 int fb_disk_profile_read(fb_disk *d, float *ms, const char **names, int max);
 
+/* CFL time step without allocating: for callers that own all device memory
+ * and cannot let a library call cudaMalloc (FARGO3D's own GPU build, whose
+ * Fields CreateField allocates once; applications on a fixed memory pool).
+ * No counterpart in the reference: it computes what ComputeVmed + cfl + cfl_b
+ * + CflFluidsMin compute at the start of a step (main.c:366-390), for one FP64
+ * fluid whose fields and mesh edges the caller holds in device memory, and
+ * writes StepTime to the caller's device double *dt_out on `stream`.  Its
+ * scratch is a fixed file-scope device array: meshes with more than
+ * FB_NOALLOC_MAX_RINGS rings ((Ny+6) x (Nz+6 or 1)) are rejected with
+ * FB_ERR_TOO_LARGE.  The first call on each device looks the array up and must
+ * come before any stream capture; calls that overlap on the GPU race. */
+#define FB_NOALLOC_MAX_RINGS 65536
+typedef struct {
+  int nx, ny, nz;              /* active zones; nz <= 1: 2D                      */
+  int spherical, alpha_visc;
+  const double *rho, *cs, *vx, *vy, *vz;  /* device fields, [nz+6|1][ny+6][nx] */
+  const double *xmin, *ymin, *zmin;       /* device mesh edges (Xmin, Ymin, Zmin) */
+  const double *sin_zmed;                 /* device sin(Zmed(k)) (spherical only) */
+  double cfl, nu, alpha;
+  double mindx;                /* min_i (Xmin[i+1] - Xmin[i])                     */
+  double xlen;                 /* XMAX - XMIN                                     */
+} fb_cfl_static_args;
+int fb_cfl_dt_static(const fb_cfl_static_args *args, double *dt_out, void *stream);
+
 const char *fb_last_error(void);
 
 #ifdef __cplusplus
