@@ -101,3 +101,19 @@ def check(rc: int):
     if rc != FB_OK:
         raise FargoError(rc, lib().fb_last_error().decode(errors="replace"))
     return rc
+
+
+def bind_batch(L):
+    if getattr(L, "_batch_bound", False):
+        return L
+    L.fb_batch_create.argtypes = [C.POINTER(FbParams), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    L.fb_batch_destroy.argtypes = [C.c_void_p]
+    L.fb_batch_disk.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]
+    L.fb_batch_initialize.argtypes = [C.c_void_p]
+    L.fb_batch_run.argtypes = [C.c_void_p, C.c_int, C.c_double]
+    L.fb_batch_sync.argtypes = [C.c_void_p]
+    L.fb_batch_get_scalars.argtypes = [C.c_void_p, C.c_int, _D, C.POINTER(C.c_int)]
+    L.fb_batch_stream.restype = C.c_void_p
+    L.fb_batch_stream.argtypes = [C.c_void_p]
+    L._batch_bound = True
+    return L

@@ -1,0 +1,93 @@
+"""Many independent disks advanced together (C-ABI fb_batch_*).
+
+Each stage of a hydro step is one launch over the tiles of every disk; the
+scalar work of a step runs on the device and sequences of steps replay from a
+captured CUDA graph, so `run` enqueues work without host round trips.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .setups import initial_state
+
+
+class _Member:
+    """A disk owned by a batch (state access through the one-disk C-ABI)."""
+
+    def __init__(self, h, shape):
+        self._h, self.shape = h, shape
+
+
+class Batch:
+    def __init__(self, cfgs, precision: str = "fp32", device: int = 0):
+        L = _abi.bind_batch(_abi.lib())
+        self.cfgs = list(cfgs)
+        arr = (_abi.FbParams * len(self.cfgs))(*[_abi.params_of(c) for c in self.cfgs])
+        h = C.c_void_p()
+        prec = _abi.FB_FP64 if precision == "fp64" else _abi.FB_FP32
+        _abi.check(L.fb_batch_create(arr, len(self.cfgs), prec, device, C.byref(h)))
+        self._h = h
+        self.precision = precision
+        self._members = []
+        for i, c in enumerate(self.cfgs):
+            dh = C.c_void_p()
+            _abi.check(L.fb_batch_disk(h, i, C.byref(dh)))
+            self._members.append(_Member(dh, c.shape))
+
+    def __len__(self):
+        return len(self.cfgs)
+
+    def set_state(self, i, rho, vx, vy, vz, cs, fluid: int = 0):
+        m = self._members[i]
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(m.shape)
+                for a in (rho, vx, vy, vz, cs)]
+        p = [None if a is None else a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+        _abi.check(_abi.lib().fb_disk_set_state(m._h, fluid, *p))
+
+    def load_initial_states(self):
+        for i, c in enumerate(self.cfgs):
+            for f in range(c.nfluids):
+                self.set_state(i, *initial_state(c, f), fluid=f)
+        self.initialize()
+
+    def initialize(self):
+        _abi.check(_abi.lib().fb_batch_initialize(self._h))
+
+    def run(self, nsteps: int, dt_interval: float = 1e30):
+        _abi.check(_abi.lib().fb_batch_run(self._h, nsteps, dt_interval))
+
+    def sync(self):
+        _abi.check(_abi.lib().fb_batch_sync(self._h))
+
+    def state(self, i, fluid: int = 0):
+        self.sync()
+        m = self._members[i]
+        out = [np.empty(m.shape) for _ in range(4)]
+        p = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in out]
+        _abi.check(_abi.lib().fb_disk_get_state(m._h, fluid, *p))
+        return {"rho": out[0], "vx": out[1], "vy": out[2], "vz": out[3]}
+
+    def scalars(self, i):
+        o = np.zeros(8)
+        st = C.c_int()
+        _abi.check(_abi.lib().fb_batch_get_scalars(self._h, i, o.ctypes.data_as(C.POINTER(C.c_double)),
+                                                   C.byref(st)))
+        return o, st.value
+
+    @property
+    def stream(self) -> int:
+        return _abi.lib().fb_batch_stream(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _abi.lib().fb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

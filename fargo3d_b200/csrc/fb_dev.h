@@ -43,6 +43,7 @@ typedef struct {
   double px[FB_MAXPLANETS], py[FB_MAXPLANETS], pz[FB_MAXPLANETS];
   double pmass[FB_MAXPLANETS], psmooth2[FB_MAXPLANETS], pdist3[FB_MAXPLANETS];
   int indirect_term;
+  int skip;               /* batched runs: this disk is frozen (error status) */
 } fb_scalars;
 
 typedef struct {
@@ -80,6 +81,13 @@ typedef struct {
 
 FB_DECL_LAUNCHERS(f64)
 FB_DECL_LAUNCHERS(f32)
+
+/* Internal accessors of a disk (fb_host.c) for the batched driver. */
+struct fb_disk;
+fb_disk_dev *fb_disk_internal_dev(struct fb_disk *d);
+struct fb_psys_s *fb_disk_internal_psys(struct fb_disk *d);
+void *fb_disk_internal_scalars(struct fb_disk *d);
+size_t fb_disk_internal_esz(struct fb_disk *d);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@
 
 #include "fargo_b200.h"
 #include "fb_dev.h"
+#include "fb_psys.h"
 
 #define NG 3
 #define G 1.0
@@ -65,15 +66,8 @@ struct fb_disk {
   double *xmin, *ymin, *zmin, *xmed, *ymed, *zmed, *invdiffxmed;
   double *sxi, *sxj, *syj, *szj, *sxk, *syk, *szk, *invvj;
   double mindx;
-  /* planetary system (psys.c) */
-  int np;
-  double px[FB_MAXPLANETS], py[FB_MAXPLANETS], pz[FB_MAXPLANETS];
-  double pvx[FB_MAXPLANETS], pvy[FB_MAXPLANETS], pvz[FB_MAXPLANETS], pmass[FB_MAXPLANETS];
-  int pfeelothers[FB_MAXPLANETS];
-  double xmark, ymark, xaxis_rot;
-  /* scalars */
-  double omegaframe, omegaframe0, domega, phys_time, dtemp, last_dt;
-  long long step_count;
+  /* planetary system, frame and time (fb_psys.h) */
+  fb_psys ps;
   fb_scalars sc;
   double *h_dtmin;              /* pinned */
   void *allocs[MAXALLOC];
@@ -296,154 +290,6 @@ static int upload_tables(fb_disk *D) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* Planetary system, FP64 on the host: psys.c:141-225 (initial state),
- * planets.c:116-190 (SV2OE), psys.c:362-415 (GetPsysInfo), psys.c:417-440
- * (RotatePsys), runge_kutta.c (Cash-Karp RK5, 5 sub-steps per hydro step). */
-typedef struct { double e, a, M, i, phi; } orbit_t;
-
-static orbit_t orbit_of(double x, double y, double z, double vx, double vy, double vz, double m) {
-  orbit_t o;
-  double d = sqrt(x * x + y * y + z * z);
-  double hx = y * vz - z * vy, hy = z * vx - x * vz, hz = x * vy - y * vx;
-  double hhor = sqrt(hx * hx + hy * hy), h = sqrt(hx * hx + hy * hy + hz * hz);
-  double Ax, Ay, Az, E, an, cosan, sinan;
-  o.i = asin(hhor / h);
-  Ax = vy * hz - vz * hy - G * m * x / d;
-  Ay = vz * hx - vx * hz - G * m * y / d;
-  Az = vx * hy - vy * hx - G * m * z / d;
-  o.e = sqrt(Ax * Ax + Ay * Ay + Az * Az) / (G * m);
-  o.a = h * h / (G * m * (1. - o.e * o.e));
-  E = (o.e != 0.0) ? acos((1.0 - d / o.a) / o.e) : 0.0;
-  if (x * vx + y * vy + z * vz < 0) E = -E;
-  if (isnan(E)) E = (d < o.a) ? 0.0 : M_PI;
-  o.M = E - o.e * sin(E);
-  an = 0.0;
-  if (fabs(o.i) > 1e-5) {
-    an = atan2(hy, hx) + M_PI * .5;
-    if (an > 2.0 * M_PI) an -= 2.0 * M_PI;
-  }
-  cosan = cos(an); sinan = sin(an);
-  (void)cosan; (void)sinan;
-  o.phi = (Ax * Ax + Ay * Ay > 0.0) ? atan2(Ay, Ax) : atan2(y, x);
-  return o;
-}
-
-enum { PS_GET = 0, PS_MARK = 1, PS_FREQUENCY = 2 };
-static double psys_info(fb_disk *D, int action) {
-  double x = D->px[0], y = D->py[0], z = D->pz[0], vx = D->pvx[0], vy = D->pvy[0], vz = D->pvz[0];
-  double m = D->pmass[0] + MSTAR, xc = x, yc = y, d1, d2, cross;
-  orbit_t o = orbit_of(x, y, z, vx, vy, vz, m);
-  if (D->p.frame == FB_FRAME_GUIDING) {
-    xc = o.a * cos(o.M + o.phi) * cos(o.i);
-    yc = o.a * sin(o.M + o.phi) * cos(o.i);
-  }
-  if (o.e < 1e-8) { xc = x; yc = y; }
-  if (action == PS_MARK) { D->xmark = xc; D->ymark = yc; return 0.0; }
-  if (action == PS_GET) {
-    x = xc; y = yc;
-    d2 = sqrt(x * x + y * y);
-    d1 = sqrt(D->xmark * D->xmark + D->ymark * D->ymark);
-    cross = D->xmark * y - x * D->ymark;
-    D->xmark = x; D->ymark = y;
-    return asin(cross / (d1 * d2));
-  }
-  if (D->p.frame == FB_FRAME_GUIDING) return sqrt(G * m / pow(o.a, 3.0));
-  return (x * vy - y * vx) / (x * x + y * y);
-}
-
-static void rotate(fb_disk *D, double angle) {
-  int i;
-  double s = sin(angle), c = cos(angle), xt, yt;
-  D->xaxis_rot += angle;
-  if (D->xaxis_rot >= 2.0 * M_PI) D->xaxis_rot -= 2.0 * M_PI;
-  if (D->xaxis_rot < 0.0) D->xaxis_rot += 2.0 * M_PI;
-  for (i = 0; i < D->np; i++) {
-    xt = D->px[i]; yt = D->py[i];
-    D->px[i] = xt * c + yt * s; D->py[i] = -xt * s + yt * c;
-    xt = D->pvx[i]; yt = D->pvy[i];
-    D->pvx[i] = xt * c + yt * s; D->pvy[i] = -xt * s + yt * c;
-  }
-}
-
-static void nbody_deriv(const fb_disk *D, const double *q, const double *ms, double *der, int n, double dt) {
-  const double *x = q, *y = q + n, *z = q + 2 * n, *vx = q + 3 * n, *vy = q + 4 * n, *vz = q + 5 * n;
-  double dist[FB_MAXPLANETS], coef, dd;
-  int i, j;
-  for (i = 0; i < n; i++) dist[i] = sqrt(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
-  for (i = 0; i < n; i++) {
-    der[i] = vx[i]; der[i + n] = vy[i]; der[i + 2 * n] = vz[i];
-    coef = -G * MSTAR / dist[i] / dist[i] / dist[i];
-    der[i + 3 * n] = coef * x[i]; der[i + 4 * n] = coef * y[i]; der[i + 5 * n] = coef * z[i];
-    for (j = 0; j < n; j++) {
-      if (D->p.indirect_term) {
-        coef = G * ms[j] / dist[j] / dist[j] / dist[j];
-        der[i + 3 * n] -= coef * x[j]; der[i + 4 * n] -= coef * y[j]; der[i + 5 * n] -= coef * z[j];
-      }
-      if (j != i && D->pfeelothers[i]) {
-        dd = (x[i] - x[j]) * (x[i] - x[j]) + (y[i] - y[j]) * (y[i] - y[j]) + (z[i] - z[j]) * (z[i] - z[j]);
-        dd = sqrt(dd);
-        coef = G * ms[j] / dd / dd / dd;
-        der[i + 3 * n] += coef * (x[j] - x[i]); der[i + 4 * n] += coef * (y[j] - y[i]);
-        der[i + 5 * n] += coef * (z[j] - z[i]);
-      }
-    }
-  }
-  for (i = 0; i < 6 * n; i++) der[i] *= dt;
-}
-
-static void nbody_rk5(fb_disk *D, double dt) {
-  enum { M6 = 6 * FB_MAXPLANETS };
-  int n = D->np, i;
-  double q0[M6] = {0}, q1[M6] = {0}, ms[FB_MAXPLANETS] = {0};
-  double k1[M6] = {0}, k2[M6] = {0}, k3[M6] = {0}, k4[M6] = {0}, k5[M6] = {0}, k6[M6] = {0};
-  if (!n) return;
-  for (i = 0; i < n; i++) {
-    q0[i] = D->px[i]; q0[i + n] = D->py[i]; q0[i + 2 * n] = D->pz[i];
-    q0[i + 3 * n] = D->pvx[i]; q0[i + 4 * n] = D->pvy[i]; q0[i + 5 * n] = D->pvz[i];
-    ms[i] = D->pmass[i];
-  }
-#define STAGE(c1, c2, c3, c4, c5) \
-  for (i = 0; i < 6 * n; i++) q1[i] = q0[i] + c1 * k1[i] + c2 * k2[i] + c3 * k3[i] + c4 * k4[i] + c5 * k5[i]
-  nbody_deriv(D, q0, ms, k1, n, dt);
-  STAGE(0.2, 0.0, 0.0, 0.0, 0.0);
-  nbody_deriv(D, q1, ms, k2, n, dt);
-  STAGE(0.075, 0.225, 0.0, 0.0, 0.0);
-  nbody_deriv(D, q1, ms, k3, n, dt);
-  STAGE(0.3, -0.9, 1.2, 0.0, 0.0);
-  nbody_deriv(D, q1, ms, k4, n, dt);
-  STAGE(-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0.0);
-  nbody_deriv(D, q1, ms, k5, n, dt);
-  STAGE(1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0);
-  nbody_deriv(D, q1, ms, k6, n, dt);
-#undef STAGE
-  for (i = 0; i < 6 * n; i++)
-    q1[i] = (q0[i] + 37.0 / 378.0 * k1[i] + 250.0 / 621.0 * k3[i] + 125.0 / 594.0 * k4[i] + 512.0 / 1771.0 * k6[i]);
-  for (i = 0; i < n; i++) {
-    D->px[i] = q1[i]; D->py[i] = q1[i + n]; D->pz[i] = q1[i + 2 * n];
-    D->pvx[i] = q1[i + 3 * n]; D->pvy[i] = q1[i + 4 * n]; D->pvz[i] = q1[i + 5 * n];
-  }
-}
-
-/* planet terms of Potential_cpu (potential.c:137-160) that do not depend on
- * the cell: smoothing^2 and the cube of the star-planet distance */
-static void planet_scalars(fb_disk *D) {
-  int n;
-  D->sc.nplanets = D->np;
-  D->sc.indirect_term = D->p.indirect_term;
-  for (n = 0; n < D->np; n++) {
-    double mp = D->pmass[n] * 1.0, pd, rroche, s;
-    pd = sqrt(D->px[n] * D->px[n] + D->py[n] * D->py[n] + D->pz[n] * D->pz[n]);
-    rroche = pd * pow((1.0 / 3.0 * mp / MSTAR), 1.0 / 3.0);
-    if (D->p.roche_smoothing != 0) s = rroche * D->p.roche_smoothing;
-    else s = D->p.aspectratio * pow(pd / R0, D->p.flaringindex) * pd * D->p.thickness_smoothing;
-    D->sc.px[n] = D->px[n]; D->sc.py[n] = D->py[n]; D->sc.pz[n] = D->pz[n];
-    D->sc.pmass[n] = D->pmass[n];
-    D->sc.psmooth2[n] = s * s;
-    D->sc.pdist3[n] = pd * pd * pd;
-  }
-}
-
-/* ------------------------------------------------------------------------ */
 #define LAUNCH(name, ...) \
   (D->d.precision == FB_FP64 ? fb_launch_##name##_f64(__VA_ARGS__) : fb_launch_##name##_f32(__VA_ARGS__))
 
@@ -525,26 +371,12 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
     return rc;
   }
   if (cudaMallocHost((void **)&D->h_dtmin, 64) != cudaSuccess) { fb_disk_destroy(D); return fail(FB_ERR_CUDA, "pinned"); }
-  /* planets (psys.c:190-210) */
-  D->np = p->nplanets;
-  for (n = 0; n < D->np; n++) {
-    double dist = p->pl_dist[n];
-    D->pmass[n] = p->pl_mass[n];
-    D->px[n] = dist * (1.0 + p->eccentricity);
-    D->py[n] = 0.0; D->pz[n] = 0.0;
-    D->pvy[n] = sqrt(G * (MSTAR + D->pmass[n]) / dist) * sqrt((1.0 - p->eccentricity) / (1.0 + p->eccentricity)) *
-                cos(p->inclination);
-    D->pvx[n] = -0.0000000000 * D->pvy[n];
-    D->pvz[n] = D->pvy[n] * sin(p->inclination) / cos(p->inclination);
-    D->pfeelothers[n] = p->pl_feelothers[n];
-  }
-  D->omegaframe = p->omegaframe;
-  if (p->frame != FB_FRAME_FIXED) D->omegaframe = psys_info(D, PS_FREQUENCY); /* main.c:240-241 */
-  D->omegaframe0 = D->omegaframe;
-  D->step_count = 0;
+  fb_psys_init(&D->ps, p->nplanets, p->pl_dist, p->pl_mass, p->pl_feelothers, p->eccentricity, p->inclination,
+               p->frame, p->omegaframe, p->indirect_term, p->roche_smoothing, p->aspectratio, p->flaringindex,
+               p->thickness_smoothing);
   D->sc.nu = p->nu; D->sc.alpha = p->alpha; D->sc.cfl = p->cfl;
-  D->sc.omegaframe = D->omegaframe; D->sc.omegaframe0 = D->omegaframe0;
-  planet_scalars(D);
+  D->sc.omegaframe = D->ps.omegaframe; D->sc.omegaframe0 = D->ps.omegaframe0;
+  fb_psys_fill_scalars(&D->ps, &D->sc);
   *out = D;
   return FB_OK;
 }
@@ -627,8 +459,8 @@ int fb_disk_get_state(fb_disk *D, int f, double *rho, double *vx, double *vy, do
 }
 
 static int push_scalars(fb_disk *D) {
-  D->sc.omegaframe = D->omegaframe;
-  D->sc.omegaframe0 = D->omegaframe0;
+  D->sc.omegaframe = D->ps.omegaframe;
+  D->sc.omegaframe0 = D->ps.omegaframe0;
   CU(cudaMemcpyAsync(D->d.scal_dev, &D->sc, sizeof(fb_scalars), cudaMemcpyHostToDevice, D->stream));
   return FB_OK;
 }
@@ -656,11 +488,10 @@ int fb_disk_initialize(fb_disk *D) {
 
 int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   int f, rc;
-  double step, dt;
+  double dt;
   const uint64_t start_bits = 0x4415AF1D78B58C40ULL; /* 1e20, the MIN reduction start (define.h:165) */
   if (!D) return fail(FB_ERR_ARG, "null disk");
   CU(cudaSetDevice(D->device));
-  if (D->dtemp >= DT) D->dtemp = 0.0;
   /* ComputeVmed(Vx) + cfl (main.c:366-388) */
   CU(cudaMemcpyAsync(D->d.dtmin, &start_bits, 8, cudaMemcpyHostToDevice, D->stream));
   if ((rc = push_scalars(D))) return rc;
@@ -670,28 +501,14 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   mark(D, "rowsum");
   for (f = 0; f < D->p.nfluids; f++) LCH(LAUNCH(cfl, &D->d, f, D->stream));
   mark(D, "cfl");
-  CU(cudaMemcpyAsync(D->h_dtmin, D->d.dtmin, 8, cudaMemcpyDeviceToHost, D->stream));
+  CU(cudaMemcpyAsync(D->h_dtmin, D->d.dtmin, 16, cudaMemcpyDeviceToHost, D->stream));
   CU(cudaStreamSynchronize(D->stream));
-  /* CflFluidsMin (cfl_fluids_min.c:3-22) */
-  step = 1e30;
-  if (step > D->h_dtmin[0]) step = D->h_dtmin[0];
-  if (!(step > SMALLTIME)) return fail(FB_ERR_NULL_DT, "null time step (dt = %g)", step);
-  dt = step;
-  D->dtemp += dt;
-  if (D->dtemp > DT) dt = DT - (D->dtemp - dt);
-  /* compute_potential (potential.c:10-49): the potential is evaluated with the
-   * planet positions before this step's orbit advance */
-  if (D->p.frame != FB_FRAME_FIXED) psys_info(D, PS_MARK);
-  planet_scalars(D);
-  for (f = 0; f < 5; f++) nbody_rk5(D, 1.0 / ((double)(5)) * dt);
-  if (D->p.frame != FB_FRAME_FIXED) {
-    double omeganew = psys_info(D, PS_GET) / dt;
-    D->domega = omeganew - D->omegaframe;
-    D->omegaframe = omeganew;
-  }
-  rotate(D, D->omegaframe * dt);
-  D->sc.dt = dt;
-  D->sc.domega = D->p.frame != FB_FRAME_FIXED ? D->domega : 0.0;
+  if (((const uint64_t *)D->h_dtmin)[1] != 0)
+    return fail(FB_ERR_NONFINITE, "non-finite time step or non-positive density in the state");
+  /* CflFluidsMin (cfl_fluids_min.c:3-22), the DT clip (main.c:388-395) and
+   * compute_potential's planetary update (potential.c:10-49) */
+  dt = fb_psys_step(&D->ps, D->h_dtmin[0], DT, &D->sc);
+  if (dt < 0.0) return fail(FB_ERR_NULL_DT, "null time step (CFL minimum %g)", D->h_dtmin[0]);
   if ((rc = push_scalars(D))) return rc;
   /* Sources (algogas.c:30-120) with its closing FillGhosts on V_temp */
   mark(D, "host_scalars");
@@ -710,8 +527,6 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
     LCH(LAUNCH(sweep_x, &D->d, f, D->stream));
     mark(D, "sweep_x");
   }
-  D->phys_time += dt;
-  D->step_count++;
   /* NewVelocity + StockholmBoundary + FillGhosts (main.c:427-431) */
   for (f = 0; f < D->p.nfluids; f++) {
     LCH(LAUNCH(newvel, &D->d, f, D->stream));
@@ -725,16 +540,16 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
     D->prof_n = D->nev - 1;
     for (i = 1; i < D->nev; i++) cudaEventElapsedTime(&D->prof_ms[i - 1], D->ev[i - 1], D->ev[i]);
   }
-  D->last_dt = dt;
   if (dt_out) *dt_out = dt;
   return FB_OK;
 }
 
 int fb_disk_get_scalars(fb_disk *D, double *o) {
   if (!D || !o) return fail(FB_ERR_ARG, "null");
-  o[0] = D->phys_time; o[1] = D->omegaframe; o[2] = D->last_dt;
-  o[3] = D->np ? D->px[0] : 0; o[4] = D->np ? D->py[0] : 0;
-  o[5] = D->np ? D->pvx[0] : 0; o[6] = D->np ? D->pvy[0] : 0; o[7] = D->domega;
+  const fb_psys *S = &D->ps;
+  o[0] = S->phys_time; o[1] = S->omegaframe; o[2] = S->last_dt;
+  o[3] = S->np ? S->px[0] : 0; o[4] = S->np ? S->py[0] : 0;
+  o[5] = S->np ? S->pvx[0] : 0; o[6] = S->np ? S->pvy[0] : 0; o[7] = S->domega;
   return FB_OK;
 }
 
@@ -764,3 +579,8 @@ int fb_disk_profile_read(fb_disk *D, float *ms, const char **names, int max) {
   }
   return n;
 }
+
+fb_disk_dev *fb_disk_internal_dev(fb_disk *D) { return &D->d; }
+struct fb_psys_s *fb_disk_internal_psys(fb_disk *D) { return &D->ps; }
+void *fb_disk_internal_scalars(fb_disk *D) { return &D->sc; }
+size_t fb_disk_internal_esz(fb_disk *D) { return D->esz; }

@@ -80,12 +80,12 @@ __device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i
 // lane per ring; the rings' rows are staged through shared memory so that
 // global loads stay coalesced.  32 rings per CTA of 256 threads.
 template <typename T, bool ORDERED>
-__global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const T *__restrict__ v,
-                                                 double *__restrict__ out, double xlen) {
+__device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const T *__restrict__ v,
+                                                 double *__restrict__ out, double xlen, uint3 bid) {
   constexpr int R = 32, CH = 128;
   __shared__ double buf[R][CH + 1];
   const int nring = m.sy * m.sz;
-  const int r0 = blockIdx.x * R;
+  const int r0 = bid.x * R;
   const int tid = threadIdx.x;
   double acc = 0.0;
   const int myring = r0 + (tid & 31);
@@ -125,6 +125,11 @@ __global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const T 
     out[myring] = tot / xlen;
   }
 }
+template <typename T, bool ORDERED>
+__global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const T *__restrict__ v,
+                                                 double *__restrict__ out, double xlen) {
+  b_rowsum<T, ORDERED>(m, gd, v, out, xlen, blockIdx);
+}
 
 // ---------------------------------------------------------------------------
 // CFL (cfl.c:135-258) and cfl_b's shear limit (cfl_b.c:14-39).  One CTA per
@@ -156,13 +161,13 @@ __device__ __forceinline__ T zsz(const Dims &m, const Geo<T> &g, int j, int k) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const T *__restrict__ rho, const T *__restrict__ cs,
+__device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const T *__restrict__ rho, const T *__restrict__ cs,
                                              const T *__restrict__ vx, const T *__restrict__ vy,
                                              const T *__restrict__ vz, const double *__restrict__ vxmed,
                                              const fb_scalars *__restrict__ sc, double cfl_num,
-                                             double mindx, unsigned long long *__restrict__ dtmin) {
-  const int j = FB_NGH + blockIdx.x;
-  const int k = m.is3d ? FB_NGH + blockIdx.y : 0;
+                                             double mindx, unsigned long long *__restrict__ dtmin, uint3 bid) {
+  const int j = FB_NGH + bid.x;
+  const int k = m.is3d ? FB_NGH + bid.y : 0;
   const double vm = vxmed[j + k * m.sy];
   const T nu = (T)sc->nu, alpha = (T)sc->alpha;
   double mn = 1e20;
@@ -196,6 +201,9 @@ __global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const T *__restri
     const T dtc = (T)cfl_num / sqrt(c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4 + c5 * c5 + zero * zero + c7 * c7 +
                                     zero * zero + zero * zero + zero * zero);
     mn = fmin(mn, (double)dtc);
+    // failure detection: a non-finite time step or a non-positive density
+    // flags the disk (dtmin[1]); the host or the batch scalar kernel reacts
+    if (!(dtc == dtc) || !(rho[l] > (T)0)) atomicOr(dtmin + 1, 1ull);
   }
   // shear limit (cfl_b.c:27-33)
   if (threadIdx.x == 0) {
@@ -213,6 +221,14 @@ __global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const T *__restri
     for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (threadIdx.x == 0 && v > 0.0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const T *__restrict__ rho, const T *__restrict__ cs,
+                                             const T *__restrict__ vx, const T *__restrict__ vy,
+                                             const T *__restrict__ vz, const double *__restrict__ vxmed,
+                                             const fb_scalars *__restrict__ sc, double cfl_num,
+                                             double mindx, unsigned long long *__restrict__ dtmin) {
+  b_cfl<T>(m, g, rho, cs, vx, vy, vz, vxmed, sc, cfl_num, mindx, dtmin, blockIdx);
 }
 
 // ---------------------------------------------------------------------------
@@ -253,16 +269,16 @@ namespace fb {
 // Inputs (rho, cs, v, P, Pot) are staged with a one-cell halo; the stress
 // tensor is computed once per point into shared memory.
 template <typename T, int TX, int TY>
-__global__ void __launch_bounds__(TX *TY) k_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
+__device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
     const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx,
     const T *__restrict__ vy, T *__restrict__ vxt, T *__restrict__ vyt,
-    const fb_scalars *__restrict__ scp, int dust, int viscous) {
+    const fb_scalars *__restrict__ scp, int dust, int viscous, uint3 bid) {
   constexpr int W = TX + 2, H = TY + 2;
   __shared__ T s_rho[H][W], s_cs[H][W], s_vx[H][W], s_vy[H][W], s_p[H][W];
   __shared__ double s_pot[H][W];
   __shared__ T s_txx[H][W], s_tyy[H][W], s_tyx[H][W];
   __shared__ fb_scalars sc;
-  const int i0 = blockIdx.x * TX, j0 = FB_NGH + blockIdx.y * TY;
+  const int i0 = bid.x * TX, j0 = FB_NGH + bid.y * TY;
   const int tid = threadIdx.x + threadIdx.y * TX;
   if (tid == 0) sc = *scp;
   __syncthreads();
@@ -366,6 +382,13 @@ __global__ void __launch_bounds__(TX *TY) k_sources_cyl(Dims m, Geo<T> g, Geo<do
   vxt[l] = ax;
   vyt[l] = ay;
 }
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX *TY) k_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
+    const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx,
+    const T *__restrict__ vy, T *__restrict__ vxt, T *__restrict__ vyt,
+    const fb_scalars *__restrict__ scp, int dust, int viscous) {
+  b_sources_cyl<T, TX, TY>(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, blockIdx);
+}
 
 }  // namespace fb
 
@@ -392,11 +415,11 @@ struct BndTab {
 
 // Radial sides: one thread per (i, ghost row jj, side s, layer k).
 template <typename T>
-__global__ void k_bnd_y(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
+__device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
                         T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
-                        int do_rho) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int jj = blockIdx.y % 3, s = blockIdx.y / 3, k = blockIdx.z;
+                        int do_rho, uint3 bid) {
+  const int i = bid.x * blockDim.x + threadIdx.x;
+  const int jj = bid.y % 3, s = bid.y / 3, k = bid.z;
   if (i >= m.nx) return;
   const T of = (T)scp->omegaframe;
   const int nghy = FB_NGH, ny = m.ny;
@@ -420,14 +443,20 @@ __global__ void k_bnd_y(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__r
   // Vz: SYMMETRIC, centred in y
   if (m.is3d) vz[lgh] = vz[lact];
 }
+template <typename T>
+__global__ void k_bnd_y(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
+                        T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
+                        int do_rho) {
+  b_bnd_y<T>(m, g, tb, rho, vx, vy, vz, scp, do_rho, blockIdx);
+}
 
 // Colatitude sides (3D): one thread per (i, j, ghost layer kk, side s).
 template <typename T>
-__global__ void k_bnd_z(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
+__device__ __forceinline__ void b_bnd_z(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
                         T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
-                        int do_rho) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, kk = blockIdx.z % 3, s = blockIdx.z / 3;
+                        int do_rho, uint3 bid) {
+  const int i = bid.x * blockDim.x + threadIdx.x;
+  const int j = bid.y, kk = bid.z % 3, s = bid.z / 3;
   if (i >= m.nx) return;
   const T of = (T)scp->omegaframe;
   const int nghz = FB_NGH, nz = m.nz;
@@ -442,6 +471,12 @@ __global__ void k_bnd_z(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__r
   if (s == 0) vz[lgh] = -vz[m.l(i, j, klacts)];
   else if (kk < nghz - 1) vz[m.l(i, j, nz + nghz + 1 + kk)] = -vz[m.l(i, j, klacts)];
   vz[m.l(i, j, knull)] = 0;
+}
+template <typename T>
+__global__ void k_bnd_z(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
+                        T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
+                        int do_rho) {
+  b_bnd_z<T>(m, g, tb, rho, vx, vy, vz, scp, do_rho, blockIdx);
 }
 
 // ---------------------------------------------------------------------------
@@ -537,14 +572,14 @@ __device__ __forceinline__ T momentum(const Dims &m, const Geo<T> &g, const QSrc
 // grid.x: columns along x (blockDim.x threads), grid.y: the other transverse
 // index (row j for Z sweeps, layer k for Y sweeps), grid.z: segments along DIR.
 template <typename T, int DIR, int NS>
-__global__ void __launch_bounds__(128) k_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int nq, int clo, int chi,
+__device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int nq, int clo, int chi,
                                                    int t2lo, T *__restrict__ rho_out, T *q_out0, T *q_out1,
                                                    T *q_out2, T *q_out3, T *q_out4, T *q_out5,
-                                                   const fb_scalars *__restrict__ scp) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                                                   const fb_scalars *__restrict__ scp, uint3 bid) {
+  const int i = bid.x * blockDim.x + threadIdx.x;
   if (i >= m.nx) return;
-  const int t2 = t2lo + blockIdx.y;
-  const int c0 = clo + blockIdx.z * NS;
+  const int t2 = t2lo + bid.y;
+  const int c0 = clo + bid.z * NS;
   if (c0 > chi) return;
   const int j = (DIR == 0) ? 0 : t2, k = (DIR == 0) ? t2 : 0;
   ColGeo<T, DIR> cg{m, g, i, j, k};
@@ -589,6 +624,13 @@ __global__ void __launch_bounds__(128) k_sweep_col(Dims m, Geo<T> g, QSrc<T> src
       rho_out[cidx(c)] = r[u + 2] + cg.finish(flux, dt, c);
     }
   }
+}
+template <typename T, int DIR, int NS>
+__global__ void __launch_bounds__(128) k_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int nq, int clo, int chi,
+                                                   int t2lo, T *__restrict__ rho_out, T *q_out0, T *q_out1,
+                                                   T *q_out2, T *q_out3, T *q_out4, T *q_out5,
+                                                   const fb_scalars *__restrict__ scp) {
+  b_sweep_col<T, DIR, NS>(m, g, src, nq, clo, chi, t2lo, rho_out, q_out0, q_out1, q_out2, q_out3, q_out4, q_out5, scp, blockIdx);
 }
 
 }  // namespace fb
@@ -715,14 +757,14 @@ __device__ void ring_pass(const Dims &m, const Geo<T> &g, int j, int k, RingSmem
 }
 
 template <typename T>
-__global__ void __launch_bounds__(512) k_sweep_x(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
+__device__ __forceinline__ void b_sweep_x(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
                                                  T *rho, T *q0, T *q1, T *q2, T *q3, T *q4, T *q5,
                                                  const T *__restrict__ vxt, const double *__restrict__ vxmed_t,
-                                                 int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp) {
+                                                 int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp, uint3 bid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
   const int nx = m.nx;
-  const int j = jlo + blockIdx.x, k = m.is3d ? klo + blockIdx.y : 0;
+  const int j = jlo + bid.x, k = m.is3d ? klo + bid.y : 0;
   RingSmem<T> S;
   S.rho = sm; S.v = sm + nx; S.rs = sm + 2 * nx; S.a = sm + 3 * nx; S.slope = sm + 4 * nx;
   S.qs = sm + 5 * nx; S.ql = sm + 6 * nx; S.qr = sm + 7 * nx;
@@ -764,23 +806,30 @@ __global__ void __launch_bounds__(512) k_sweep_x(Dims m, Geo<T> g, Geo<double> g
     for (int q = 0; q < nq; q++) qg[q][lr + i] = S.q[q][it];
   }
 }
+template <typename T>
+__global__ void __launch_bounds__(512) k_sweep_x(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
+                                                 T *rho, T *q0, T *q1, T *q2, T *q3, T *q4, T *q5,
+                                                 const T *__restrict__ vxt, const double *__restrict__ vxmed_t,
+                                                 int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp) {
+  b_sweep_x<T>(m, g, gd, nq, jlo, klo, rho, q0, q1, q2, q3, q4, q5, vxt, vxmed_t, nshift_out, scp, blockIdx);
+}
 
 // ---------------------------------------------------------------------------
 // NewVelocity_x/y/z (newvel_x.c:81, newvel_y.c:70, newvel_z.c:66-69) and
 // StockholmBoundary (stockholm.c:129-185) on the active cells; writes the
 // new state (rho, vx, vy, vz).
 template <typename T>
-__global__ void __launch_bounds__(256) k_newvel(Dims m, Geo<T> g, const T *__restrict__ rt, const T *__restrict__ mpx,
+__device__ __forceinline__ void b_newvel(Dims m, Geo<T> g, const T *__restrict__ rt, const T *__restrict__ mpx,
                                                 const T *__restrict__ mmx, const T *__restrict__ mpy,
                                                 const T *__restrict__ mmy, const T *__restrict__ mpz,
                                                 const T *__restrict__ mmz, T *__restrict__ rho, T *__restrict__ vx,
                                                 T *__restrict__ vy, T *__restrict__ vz, const T *__restrict__ rho0,
                                                 const T *__restrict__ vx0, const T *__restrict__ vy0,
                                                 const T *__restrict__ vz0, const double *__restrict__ ramps,
-                                                int stockholm, const fb_scalars *__restrict__ scp) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = FB_NGH + blockIdx.y;
-  const int k = m.is3d ? FB_NGH + blockIdx.z : 0;
+                                                int stockholm, const fb_scalars *__restrict__ scp, uint3 bid) {
+  const int i = bid.x * blockDim.x + threadIdx.x;
+  const int j = FB_NGH + bid.y;
+  const int k = m.is3d ? FB_NGH + bid.z : 0;
   if (i >= m.nx) return;
   const long long l = m.l(i, j, k);
   const int im = i > 0 ? i - 1 : m.nx - 1;
@@ -833,6 +882,17 @@ __global__ void __launch_bounds__(256) k_newvel(Dims m, Geo<T> g, const T *__res
   vy[l] = nvy;
   if (m.is3d) vz[l] = nvz;
 }
+template <typename T>
+__global__ void __launch_bounds__(256) k_newvel(Dims m, Geo<T> g, const T *__restrict__ rt, const T *__restrict__ mpx,
+                                                const T *__restrict__ mmx, const T *__restrict__ mpy,
+                                                const T *__restrict__ mmy, const T *__restrict__ mpz,
+                                                const T *__restrict__ mmz, T *__restrict__ rho, T *__restrict__ vx,
+                                                T *__restrict__ vy, T *__restrict__ vz, const T *__restrict__ rho0,
+                                                const T *__restrict__ vx0, const T *__restrict__ vy0,
+                                                const T *__restrict__ vz0, const double *__restrict__ ramps,
+                                                int stockholm, const fb_scalars *__restrict__ scp) {
+  b_newvel<T>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, rho, vx, vy, vz, rho0, vx0, vy0, vz0, ramps, stockholm, scp, blockIdx);
+}
 
 }  // namespace fb
 
@@ -844,17 +904,17 @@ namespace fb {
 // six stress components of visctensor_sph (visctensor_sph.c:141-213) computed
 // where addviscosity_sph (addviscosity_sph.c:74-126) reads them.
 template <typename T, int TX, int TY>
-__global__ void __launch_bounds__(TX *TY) k_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
+__device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
     const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx, const T *__restrict__ vy,
     const T *__restrict__ vz, T *__restrict__ vxt, T *__restrict__ vyt, T *__restrict__ vzt,
-    const fb_scalars *__restrict__ scp, int dust, int viscous) {
+    const fb_scalars *__restrict__ scp, int dust, int viscous, uint3 bid) {
   constexpr int W = TX + 2, H = TY + 2;
   __shared__ T s_rho[3][H][W], s_cs[3][H][W], s_vx[3][H][W], s_vy[3][H][W], s_vz[3][H][W];
   __shared__ double s_pot[2][H][W];   // layers k-1, k
   __shared__ T t_xx[2][H][W], t_zz[2][H][W], t_yy[H][W];   // planes k-1, k
   __shared__ T t_xz[2][H][W], t_zy[2][H][W], t_yx[H][W];   // planes k, k+1
   __shared__ fb_scalars sc;
-  const int i0 = blockIdx.x * TX, j0 = FB_NGH + blockIdx.y * TY, kc = FB_NGH + blockIdx.z;
+  const int i0 = bid.x * TX, j0 = FB_NGH + bid.y * TY, kc = FB_NGH + bid.z;
   const int tid = threadIdx.x + threadIdx.y * TX;
   if (tid == 0) sc = *scp;
   __syncthreads();
@@ -1024,6 +1084,13 @@ __global__ void __launch_bounds__(TX *TY) k_sources_sph(Dims m, Geo<T> g, Geo<do
   vxt[l] = ax;
   vyt[l] = ay;
   vzt[l] = az;
+}
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX *TY) k_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
+    const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx, const T *__restrict__ vy,
+    const T *__restrict__ vz, T *__restrict__ vxt, T *__restrict__ vyt, T *__restrict__ vzt,
+    const fb_scalars *__restrict__ scp, int dust, int viscous) {
+  b_sources_sph<T, TX, TY>(m, g, gd, rho, cs, vx, vy, vz, vxt, vyt, vzt, scp, dust, viscous, blockIdx);
 }
 
 }  // namespace fb

@@ -170,3 +170,23 @@ def initial_state(cfg: DiskConfig, fluid: int = 0):
         cs = np.zeros(cfg.shape)
     return (np.ascontiguousarray(rho), np.ascontiguousarray(vx), np.ascontiguousarray(vy),
             np.ascontiguousarray(vz), np.ascontiguousarray(cs))
+
+
+def config_batched(ndisks: int = 64, seed: int = 0):
+    """Independent 2D disks of uneven sizes (the batched workload): N_phi in
+    {128, 256, 512, 1024}, N_r in {64, 128, 256, 512}, planet mass ratio
+    log-uniform in [1e-5, 3e-3], alpha viscosity log-uniform in [1e-4, 1e-2],
+    aspect ratio uniform in [0.03, 0.08], Sigma ~ r^-p with p uniform in
+    [0, 1.5].  Seeded numpy default_rng."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for d in range(ndisks):
+        nx = int(rng.choice([128, 256, 512, 1024]))
+        ny = int(rng.choice([64, 128, 256, 512]))
+        q = float(np.exp(rng.uniform(np.log(1e-5), np.log(3e-3))))
+        alpha = float(np.exp(rng.uniform(np.log(1e-4), np.log(1e-2))))
+        h = float(rng.uniform(0.03, 0.08))
+        p = float(rng.uniform(0.0, 1.5))
+        out.append(DiskConfig(nx=nx, ny=ny, aspectratio=h, sigmaslope=p, alpha=alpha, alpha_visc=True, nu=0.0,
+                              planets=[Planet(1.0, q)], seed=seed * 100000 + d))
+    return out

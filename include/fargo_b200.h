@@ -93,6 +93,27 @@ void *fb_disk_stream(fb_disk *d);
 int fb_disk_profile(fb_disk *d, int enable);
 int fb_disk_profile_read(fb_disk *d, float *ms, const char **names, int max);
 
+/* ---- many independent disks advanced together (fargo3d_b200/csrc/fb_batch.cu).
+ * Each stage of a step is ONE launch over the tiles of all disks; the step's
+ * scalar work (time step, planets, frame) runs on the device, one thread per
+ * disk, and sequences of steps replay from a captured CUDA graph.  All disks
+ * share a precision, a dimensionality and a fluid count.  A disk whose state
+ * turns non-finite, or whose time step collapses, is frozen with that status
+ * while the others continue.  No counterpart in the reference (one disk per
+ * run); each disk's step is the one of fb_disk_step. */
+typedef struct fb_batch fb_batch;
+int fb_batch_create(const fb_params *ps, int ndisks, int precision, int device, fb_batch **out);
+int fb_batch_destroy(fb_batch *b);
+/* the disk object of member i: use fb_disk_set_state / fb_disk_get_state on it
+ * (call fb_batch_sync first when reading) */
+int fb_batch_disk(fb_batch *b, int i, fb_disk **d);
+int fb_batch_initialize(fb_batch *b);
+/* enqueue nsteps hydro steps of every disk; returns without waiting */
+int fb_batch_run(fb_batch *b, int nsteps, double dt_interval);
+int fb_batch_sync(fb_batch *b);
+int fb_batch_get_scalars(fb_batch *b, int i, double out8[8], int *status);
+void *fb_batch_stream(fb_batch *b);
+
 /* CFL time step without allocating: for callers that own all device memory
  * and cannot let a library call cudaMalloc (FARGO3D's own GPU build, whose
  * Fields CreateField allocates once; applications on a fixed memory pool).
