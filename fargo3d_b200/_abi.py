@@ -115,5 +115,6 @@ def bind_batch(L):
     L.fb_batch_get_scalars.argtypes = [C.c_void_p, C.c_int, _D, C.POINTER(C.c_int)]
     L.fb_batch_stream.restype = C.c_void_p
     L.fb_batch_stream.argtypes = [C.c_void_p]
+    L.fb_batch_profile_step.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.c_int]
     L._batch_bound = True
     return L

@@ -200,9 +200,24 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
   return (int)v.size();
 }
 
+// optional per-launch timing of an eager (uncaptured) step
+struct Prof {
+  cudaEvent_t ev[40];
+  const char *name[40];
+  int n;
+};
+static Prof *g_prof = nullptr;
+static void pmark(cudaStream_t st, const char *name) {
+  if (!g_prof || g_prof->n >= 40) return;
+  cudaEventCreate(&g_prof->ev[g_prof->n]);
+  cudaEventRecord(g_prof->ev[g_prof->n], st);
+  g_prof->name[g_prof->n++] = name;
+}
+
 template <typename T>
 static int launch_step(fb_batch *B, double DT) {
   cudaStream_t st = B->stream;
+  pmark(st, "start");
   const fb_disk_dev *ds = B->d_disks;
   const int nf = B->nfluids;
   auto grid = [&](int s) { return dim3((unsigned)B->nitems[s]); };
@@ -210,25 +225,35 @@ static int launch_step(fb_batch *B, double DT) {
     if (B->precision == FB_FP64) kb_rowsum<T, true><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
     else kb_rowsum<T, false><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
   }
+  pmark(st, "rowsum");
   for (int f = 0; f < nf; f++) kb_cfl<T><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
+  pmark(st, "cfl");
   kb_scalars<<<(B->n + 63) / 64, 64, 0, st>>>(ds, B->d_psys, B->n, DT);
+  pmark(st, "scalars");
   for (int f = 0; f < nf; f++) {
     if (B->is3d) kb_sources_sph<T><<<grid(ST_SOURCES), dim3(SRC3_TX, SRC3_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
     else kb_sources_cyl<T><<<grid(ST_SOURCES), dim3(SRC2_TX, SRC2_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
+    pmark(st, "sources");
     if (B->is3d) kb_bnd<T><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 1, 1);
     kb_bnd<T><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 1, 0);
+    pmark(st, "bnd_vtemp");
   }
   for (int f = 0; f < nf; f++) {
     if (B->precision == FB_FP64) kb_rowsum<T, true><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
     else kb_rowsum<T, false><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
+    pmark(st, "rowsum_vtemp");
     if (B->is3d) kb_sweep_col<T, 1><<<grid(ST_SWEEP_Z), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Z], f);
     kb_sweep_col<T, 0><<<grid(ST_SWEEP_Y), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Y], f);
+    pmark(st, "sweep_cols");
     kb_sweep_x<T><<<grid(ST_SWEEP_X), 512, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f);
+    pmark(st, "sweep_x");
   }
   for (int f = 0; f < nf; f++) {
     kb_newvel<T><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
+    pmark(st, "newvel");
     if (B->is3d) kb_bnd<T><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 0, 1);
     kb_bnd<T><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 0, 0);
+    pmark(st, "bnd");
   }
   return (int)cudaGetLastError();
 }
@@ -329,8 +354,8 @@ int fb_batch_initialize(fb_batch *B) {
 int fb_batch_run(fb_batch *B, int nsteps, double DT) {
   if (!B || nsteps < 0) return FB_ERR_ARG;
   if (cudaSetDevice(B->device) != cudaSuccess) return FB_ERR_CUDA;
-  const int chunk = nsteps >= 10 ? 10 : (nsteps > 0 ? nsteps : 1);
-  if (!B->exec || B->graph_steps != chunk || B->graph_dt != DT) {
+  const int chunk = 10;  // steps per captured graph; a remainder runs eagerly
+  if (nsteps >= chunk && (!B->exec || B->graph_steps != chunk || B->graph_dt != DT)) {
     if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
     cudaGraph_t g;
     if (cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FB_ERR_CUDA;
@@ -381,5 +406,26 @@ int fb_batch_get_scalars(fb_batch *B, int i, double *o, int *status) {
 }
 
 void *fb_batch_stream(fb_batch *B) { return B ? (void *)B->stream : nullptr; }
+
+// One eager step of every disk with CUDA events between the launch groups;
+// ms[i] is the device time of group names[i].  Returns the group count.
+int fb_batch_profile_step(fb_batch *B, double DT, float *ms, const char **names, int max) {
+  if (!B) return FB_ERR_ARG;
+  cudaSetDevice(B->device);
+  Prof P;
+  P.n = 0;
+  g_prof = &P;
+  int rc = B->precision == FB_FP64 ? launch_step<double>(B, DT) : launch_step<float>(B, DT);
+  g_prof = nullptr;
+  if (rc) return FB_ERR_CUDA;
+  cudaEventSynchronize(P.ev[P.n - 1]);
+  int k = 0;
+  for (int i = 1; i < P.n && k < max; i++, k++) {
+    cudaEventElapsedTime(&ms[k], P.ev[i - 1], P.ev[i]);
+    names[k] = P.name[i];
+  }
+  for (int i = 0; i < P.n; i++) cudaEventDestroy(P.ev[i]);
+  return k;
+}
 
 }  // extern "C"

@@ -113,6 +113,8 @@ int fb_batch_run(fb_batch *b, int nsteps, double dt_interval);
 int fb_batch_sync(fb_batch *b);
 int fb_batch_get_scalars(fb_batch *b, int i, double out8[8], int *status);
 void *fb_batch_stream(fb_batch *b);
+/* one eager step with per-launch-group device timing (see fb_disk_profile_read) */
+int fb_batch_profile_step(fb_batch *b, double dt_interval, float *ms, const char **names, int max);
 
 /* CFL time step without allocating: for callers that own all device memory
  * and cannot let a library call cudaMalloc (FARGO3D's own GPU build, whose
