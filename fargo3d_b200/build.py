@@ -57,7 +57,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     objs = []
-    cu_flags = {"fb_kernels_f64.cu": ["--fmad=false"], "fb_kernels_f32.cu": [], "fb_noalloc.cu": ["--fmad=false"]}
+    fast32 = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+    cu_flags = {"fb_kernels_f64.cu": ["--fmad=false"], "fb_kernels_f32.cu": fast32, "fb_noalloc.cu": ["--fmad=false"],
+                "fb_batch_f64.cu": ["--fmad=false"], "fb_batch_f32.cu": fast32}
     for f in sorted(os.listdir(CSRC)):
         src = os.path.join(CSRC, f)
         obj = os.path.join(BUILD, f + ".o")

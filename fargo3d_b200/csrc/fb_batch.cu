@@ -1,4 +1,4 @@
-// fb_batch.cu -- many independent disks advanced together.
+// fb_batch.cu -- many independent disks advanced together (host side).
 //
 // Every stage of a hydro step runs as ONE launch over the tiles of all disks:
 // the host enumerates each stage's tiles (disk, bx, by, bz) once into a work
@@ -8,254 +8,17 @@
 // fb_psys.h) runs on the device, one thread per disk, so a step needs no host
 // round trip and whole sequences of steps are captured into one CUDA graph.
 // A disk whose state goes non-finite or whose time step collapses is frozen
-// (its tiles return immediately) while the others continue.
-#include <cuda_runtime.h>
+// (its tiles return immediately) while the others continue.  The stage
+// kernels are compiled per precision (fb_batch_f64.cu, fb_batch_f32.cu).
+#include "fb_batch.cuh"
 
-#include <stdlib.h>
-#include <string.h>
-#include <vector>
+Prof *g_prof = nullptr;
 
-#include "fargo_b200.h"
-#include "fb_kernels.cuh"
-#include "fb_psys.h"
+extern "C" int fb_batch_launch_step_f64(fb_batch *B, double DT);
+extern "C" int fb_batch_launch_step_f32(fb_batch *B, double DT);
 
-namespace fb {
-
-enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_SWEEP_Z, ST_SWEEP_Y, ST_SWEEP_X, ST_NEWVEL, ST_N };
-
-// tile shapes shared with the one-disk launchers (fb_launch.cuh)
-constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_NS = 8, COL_BX = 128, BND_BX = 128,
-              NV_BX = 128;
-
-#define FB_TILE                                        \
-  const int4 w = items[blockIdx.x];                    \
-  const fb_disk_dev &D = ds[w.x];                      \
-  const fb_scalars *scp = D.scal_dev;                  \
-  if (scp->skip) return;                               \
-  const uint3 bid = make_uint3(w.y, w.z, w.w);         \
-  const fb_fluid_dev &F = D.fl[f];                     \
-  (void)F;
-
-template <typename T, bool ORDERED>
-__global__ void __launch_bounds__(256) kb_rowsum(const fb_disk_dev *ds, const int4 *items, int f, int which) {
-  FB_TILE
-  b_rowsum<T, ORDERED>(dims_of(D), geo_of<double>(D.geomd), (const T *)(which == 0 ? F.vx : F.vxt),
-                       which == 0 ? F.vxmed : F.vxmed_t, D.xlen, bid);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 *items, int f) {
-  FB_TILE
-  b_cfl<T>(dims_of(D), geo_of<T>(D.geom), (const T *)F.rho, (const T *)F.cs, (const T *)F.vx, (const T *)F.vy,
-           (const T *)F.vz, F.vxmed, scp, D.cfl, D.mindx, (unsigned long long *)D.dtmin, bid);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(SRC2_TX *SRC2_TY) kb_sources_cyl(const fb_disk_dev *ds, const int4 *items, int f) {
-  FB_TILE
-  b_sources_cyl<T, SRC2_TX, SRC2_TY>(dims_of(D), geo_of<T>(D.geom), geo_of<double>(D.geomd), (const T *)F.rho,
-                                     (const T *)F.cs, (const T *)F.vx, (const T *)F.vy, (T *)F.vxt, (T *)F.vyt, scp,
-                                     F.dust, !F.dust, bid);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(SRC3_TX *SRC3_TY) kb_sources_sph(const fb_disk_dev *ds, const int4 *items, int f) {
-  FB_TILE
-  b_sources_sph<T, SRC3_TX, SRC3_TY>(dims_of(D), geo_of<T>(D.geom), geo_of<double>(D.geomd), (const T *)F.rho,
-                                     (const T *)F.cs, (const T *)F.vx, (const T *)F.vy, (const T *)F.vz, (T *)F.vxt,
-                                     (T *)F.vyt, (T *)F.vzt, scp, F.dust, !F.dust, bid);
-}
-
-template <typename T>
-__global__ void kb_bnd(const fb_disk_dev *ds, const int4 *items, int f, int vtemp, int zside) {
-  FB_TILE
-  Dims m = dims_of(D);
-  BndTab tb{D.bnd_tab, m.sy, m.sz};
-  T *vx = (T *)(vtemp ? F.vxt : F.vx), *vy = (T *)(vtemp ? F.vyt : F.vy), *vz = (T *)(vtemp ? F.vzt : F.vz);
-  if (zside) b_bnd_z<T>(m, geo_of<T>(D.geom), tb, (T *)F.rho, vx, vy, vz, scp, !vtemp, bid);
-  else b_bnd_y<T>(m, geo_of<T>(D.geom), tb, (T *)F.rho, vx, vy, vz, scp, !vtemp, bid);
-}
-
-template <typename T, int DIR>
-__global__ void __launch_bounds__(COL_BX) kb_sweep_col(const fb_disk_dev *ds, const int4 *items, int f) {
-  FB_TILE
-  Dims m = dims_of(D);
-  const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;
-  QSrc<T> src;
-  src.vxt = (const T *)F.vxt; src.vyt = (const T *)F.vyt; src.vzt = (const T *)F.vzt; src.of = (T)0;
-  if (!m.is3d || DIR == 1) {
-    src.rho = (const T *)F.rho;
-    for (int q = 0; q < 6; q++) src.q[q] = nullptr;
-    src.from_v = 1;
-  } else {
-    src.rho = (const T *)F.rho_a;
-    src.q[0] = (const T *)F.mpx; src.q[1] = (const T *)F.mmx; src.q[2] = (const T *)F.mpy;
-    src.q[3] = (const T *)F.mmy; src.q[4] = (const T *)F.mpz; src.q[5] = (const T *)F.mmz;
-    src.from_v = 0;
-  }
-  if (!m.is3d) {
-    b_sweep_col<T, 0, COL_NS>(m, geo_of<T>(D.geom), src, 4, ylo, yhi, 0, (T *)F.rho_a, (T *)F.mpx, (T *)F.mmx,
-                              (T *)F.mpy, (T *)F.mmy, nullptr, nullptr, scp, bid);
-  } else if (DIR == 1) {
-    b_sweep_col<T, 1, COL_NS>(m, geo_of<T>(D.geom), src, 6, FB_NGH - 1, m.nz + FB_NGH - 1, 0, (T *)F.rho_a,
-                              (T *)F.mpx, (T *)F.mmx, (T *)F.mpy, (T *)F.mmy, (T *)F.mpz, (T *)F.mmz, scp, bid);
-  } else {
-    b_sweep_col<T, 0, COL_NS>(m, geo_of<T>(D.geom), src, 6, ylo, yhi, FB_NGH - 1, (T *)F.rho_b, (T *)F.mpx_b,
-                              (T *)F.mmx_b, (T *)F.mpy_b, (T *)F.mmy_b, (T *)F.mpz_b, (T *)F.mmz_b, scp, bid);
-  }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(512) kb_sweep_x(const fb_disk_dev *ds, const int4 *items, int f) {
-  FB_TILE
-  Dims m = dims_of(D);
-  const bool b = m.is3d;
-  b_sweep_x<T>(m, geo_of<T>(D.geom), geo_of<double>(D.geomd), b ? 6 : 4, FB_NGH - 1, b ? FB_NGH - 1 : 0,
-               (T *)(b ? F.rho_b : F.rho_a), (T *)(b ? F.mpx_b : F.mpx), (T *)(b ? F.mmx_b : F.mmx),
-               (T *)(b ? F.mpy_b : F.mpy), (T *)(b ? F.mmy_b : F.mmy), (T *)(b ? F.mpz_b : F.mpz),
-               (T *)(b ? F.mmz_b : F.mmz), (const T *)F.vxt, F.vxmed_t, F.nshift, scp, bid);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(NV_BX) kb_newvel(const fb_disk_dev *ds, const int4 *items, int f) {
-  FB_TILE
-  Dims m = dims_of(D);
-  const bool b = m.is3d;
-  b_newvel<T>(m, geo_of<T>(D.geom), (const T *)(b ? F.rho_b : F.rho_a), (const T *)(b ? F.mpx_b : F.mpx),
-              (const T *)(b ? F.mmx_b : F.mmx), (const T *)(b ? F.mpy_b : F.mpy), (const T *)(b ? F.mmy_b : F.mmy),
-              (const T *)(b ? F.mpz_b : F.mpz), (const T *)(b ? F.mmz_b : F.mmz), (T *)F.rho, (T *)F.vx,
-              (T *)F.vy, (T *)F.vz, (const T *)F.rho0, (const T *)F.vx0, (const T *)F.vy0, (const T *)F.vz0,
-              D.ramps, D.stockholm, scp, bid);
-}
-
-// The scalar work of the step for every disk, one thread per disk; then the
-// CFL minimum is reset for the next step.  dtmin[1] carries the kernels'
-// non-finite flag.
-__global__ void kb_scalars(const fb_disk_dev *ds, fb_psys *ps, int n, double DT) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const fb_disk_dev &D = ds[i];
-  unsigned long long *dm = (unsigned long long *)D.dtmin;
-  fb_scalars sc = *D.scal_dev;
-  if (!sc.skip) {
-    fb_psys S = ps[i];
-    const double cflmin = __longlong_as_double((long long)dm[0]);
-    if (dm[1] != 0ull) {
-      S.status = FB_ERR_NONFINITE;
-      sc.skip = 1;
-    } else if (fb_psys_step(&S, cflmin, DT, &sc) < 0.0) {
-      sc.skip = 1;
-    }
-    ps[i] = S;
-    *D.scal_dev = sc;
-  }
-  dm[0] = 0x4415AF1D78B58C40ULL;  // 1e20, the MIN reduction start (define.h:165)
-}
-
-}  // namespace fb
-
-using namespace fb;
-
-struct fb_batch {
-  int n, precision, device, is3d, nfluids;
-  cudaStream_t stream;
-  std::vector<fb_disk *> disks;
-  fb_disk_dev *d_disks;
-  fb_psys *d_psys;
-  int4 *items[ST_N];
-  int nitems[ST_N];
-  size_t smem_x;
-  cudaGraphExec_t exec;
-  int graph_steps;
-  double graph_dt;
-};
-
-static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
-  for (int di = 0; di < B->n; di++) {
-    const fb_disk_dev &D = *fb_disk_internal_dev(B->disks[di]);
-    const int nx = D.nx, ny = D.ny, nz = D.nz, sy = D.sy, sz = D.sz;
-    dim3 g(1, 1, 1);
-    switch (st) {
-      case ST_ROWSUM: g = dim3((sy * sz + 31) / 32); break;
-      case ST_CFL: g = dim3(ny, D.is3d ? nz : 1); break;
-      case ST_SOURCES:
-        g = D.is3d ? dim3((nx + SRC3_TX - 1) / SRC3_TX, (ny + SRC3_TY - 1) / SRC3_TY, nz)
-                   : dim3((nx + SRC2_TX - 1) / SRC2_TX, (ny + SRC2_TY - 1) / SRC2_TY);
-        break;
-      case ST_BND_Z: g = D.is3d ? dim3((nx + BND_BX - 1) / BND_BX, sy, 6) : dim3(0); break;
-      case ST_BND_Y: g = dim3((nx + BND_BX - 1) / BND_BX, 6, sz); break;
-      case ST_SWEEP_Z:
-        g = D.is3d ? dim3((nx + COL_BX - 1) / COL_BX, sy - 1, (nz + 1 + COL_NS - 1) / COL_NS) : dim3(0);
-        break;
-      case ST_SWEEP_Y:
-        g = dim3((nx + COL_BX - 1) / COL_BX, D.is3d ? nz + 1 : 1, (ny + 1 + COL_NS - 1) / COL_NS);
-        break;
-      case ST_SWEEP_X: g = dim3(ny + 1, D.is3d ? nz + 1 : 1); break;
-      case ST_NEWVEL: g = dim3((nx + NV_BX - 1) / NV_BX, ny, D.is3d ? nz : 1); break;
-    }
-    for (unsigned z = 0; z < g.z; z++)
-      for (unsigned y = 0; y < g.y; y++)
-        for (unsigned x = 0; x < g.x; x++) v.push_back(make_int4(di, (int)x, (int)y, (int)z));
-  }
-  return (int)v.size();
-}
-
-// optional per-launch timing of an eager (uncaptured) step
-struct Prof {
-  cudaEvent_t ev[40];
-  const char *name[40];
-  int n;
-};
-static Prof *g_prof = nullptr;
-static void pmark(cudaStream_t st, const char *name) {
-  if (!g_prof || g_prof->n >= 40) return;
-  cudaEventCreate(&g_prof->ev[g_prof->n]);
-  cudaEventRecord(g_prof->ev[g_prof->n], st);
-  g_prof->name[g_prof->n++] = name;
-}
-
-template <typename T>
-static int launch_step(fb_batch *B, double DT) {
-  cudaStream_t st = B->stream;
-  pmark(st, "start");
-  const fb_disk_dev *ds = B->d_disks;
-  const int nf = B->nfluids;
-  auto grid = [&](int s) { return dim3((unsigned)B->nitems[s]); };
-  for (int f = 0; f < nf; f++) {
-    if (B->precision == FB_FP64) kb_rowsum<T, true><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
-    else kb_rowsum<T, false><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
-  }
-  pmark(st, "rowsum");
-  for (int f = 0; f < nf; f++) kb_cfl<T><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
-  pmark(st, "cfl");
-  kb_scalars<<<(B->n + 63) / 64, 64, 0, st>>>(ds, B->d_psys, B->n, DT);
-  pmark(st, "scalars");
-  for (int f = 0; f < nf; f++) {
-    if (B->is3d) kb_sources_sph<T><<<grid(ST_SOURCES), dim3(SRC3_TX, SRC3_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
-    else kb_sources_cyl<T><<<grid(ST_SOURCES), dim3(SRC2_TX, SRC2_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
-    pmark(st, "sources");
-    if (B->is3d) kb_bnd<T><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 1, 1);
-    kb_bnd<T><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 1, 0);
-    pmark(st, "bnd_vtemp");
-  }
-  for (int f = 0; f < nf; f++) {
-    if (B->precision == FB_FP64) kb_rowsum<T, true><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
-    else kb_rowsum<T, false><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
-    pmark(st, "rowsum_vtemp");
-    if (B->is3d) kb_sweep_col<T, 1><<<grid(ST_SWEEP_Z), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Z], f);
-    kb_sweep_col<T, 0><<<grid(ST_SWEEP_Y), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Y], f);
-    pmark(st, "sweep_cols");
-    kb_sweep_x<T><<<grid(ST_SWEEP_X), 512, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f);
-    pmark(st, "sweep_x");
-  }
-  for (int f = 0; f < nf; f++) {
-    kb_newvel<T><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
-    pmark(st, "newvel");
-    if (B->is3d) kb_bnd<T><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 0, 1);
-    kb_bnd<T><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 0, 0);
-    pmark(st, "bnd");
-  }
-  return (int)cudaGetLastError();
+static int launch_step_any(fb_batch *B, double DT) {
+  return B->precision == FB_FP64 ? fb_batch_launch_step_f64(B, DT) : fb_batch_launch_step_f32(B, DT);
 }
 
 extern "C" {
@@ -309,6 +72,18 @@ int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_ba
   }
   cudaMemcpy(B->d_disks, hd.data(), sizeof(fb_disk_dev) * n, cudaMemcpyHostToDevice);
   cudaMemcpy(B->d_psys, hp.data(), sizeof(fb_psys) * n, cudaMemcpyHostToDevice);
+  // one chunk width for the whole batch: the first of 4, 8, 16, 2, 1 that
+  // every ring fits
+  {
+    const int cs[5] = {4, 8, 16, 2, 1};
+    B->cx = 0;
+    for (int t = 0; t < 5 && !B->cx; t++) {
+      bool ok = true;
+      for (int i = 0; i < n; i++) ok = ok && hd[i].nx % cs[t] == 0 && hd[i].nx / cs[t] <= 256;
+      if (ok) B->cx = cs[t];
+    }
+    if (!B->cx) { fb_batch_destroy(B); return FB_ERR_ARG; }
+  }
   for (int s = 0; s < ST_N; s++) {
     std::vector<int4> v;
     B->nitems[s] = tiles(B, s, v);
@@ -318,11 +93,12 @@ int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_ba
     }
   }
   const size_t esz = precision == FB_FP64 ? 8 : 4;
-  B->smem_x = (size_t)(8 + (B->is3d ? 6 : 4)) * maxnx * esz;
-  if (precision == FB_FP64)
-    cudaFuncSetAttribute(kb_sweep_x<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x);
-  else
-    cudaFuncSetAttribute(kb_sweep_x<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x);
+  B->smem_x = 0;
+  (void)maxnx;
+  for (int i = 0; i < n; i++) {
+    size_t s = sweep_x2_smem(hd[i].nx, B->cx, 256, B->is3d ? 6 : 4, esz);
+    if (s > B->smem_x) B->smem_x = s;
+  }
   *out = B;
   return FB_OK;
 }
@@ -359,10 +135,7 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
     if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
     cudaGraph_t g;
     if (cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FB_ERR_CUDA;
-    for (int s = 0; s < chunk; s++) {
-      if (B->precision == FB_FP64) launch_step<double>(B, DT);
-      else launch_step<float>(B, DT);
-    }
+    for (int s = 0; s < chunk; s++) launch_step_any(B, DT);
     if (cudaStreamEndCapture(B->stream, &g) != cudaSuccess) return FB_ERR_CUDA;
     if (cudaGraphInstantiate(&B->exec, g, 0) != cudaSuccess) { cudaGraphDestroy(g); return FB_ERR_CUDA; }
     cudaGraphDestroy(g);
@@ -375,8 +148,7 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
     done += chunk;
   }
   for (; done < nsteps; done++) {
-    int rc = B->precision == FB_FP64 ? launch_step<double>(B, DT) : launch_step<float>(B, DT);
-    if (rc) return FB_ERR_CUDA;
+    if (launch_step_any(B, DT)) return FB_ERR_CUDA;
   }
   return FB_OK;
 }
@@ -415,7 +187,7 @@ int fb_batch_profile_step(fb_batch *B, double DT, float *ms, const char **names,
   Prof P;
   P.n = 0;
   g_prof = &P;
-  int rc = B->precision == FB_FP64 ? launch_step<double>(B, DT) : launch_step<float>(B, DT);
+  int rc = launch_step_any(B, DT);
   g_prof = nullptr;
   if (rc) return FB_ERR_CUDA;
   cudaEventSynchronize(P.ev[P.n - 1]);

@@ -597,7 +597,9 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int n
   // density interface values (VanLeer*_a/_b on Density -> DensStar)
   col_sweep_q<T, DIR, NS>(cg, c0, r, vel, rs, dt, rs);
   T *qo[6] = {q_out0, q_out1, q_out2, q_out3, q_out4, q_out5};
-  for (int q = 0; q < nq; q++) {
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    if (q >= nq) break;
     T qv[NS + 4];
 #pragma unroll
     for (int w = 0; w < NS + 4; w++) {
@@ -626,7 +628,7 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int n
   }
 }
 template <typename T, int DIR, int NS>
-__global__ void __launch_bounds__(128) k_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int nq, int clo, int chi,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int nq, int clo, int chi,
                                                    int t2lo, T *__restrict__ rho_out, T *q_out0, T *q_out1,
                                                    T *q_out2, T *q_out3, T *q_out4, T *q_out5,
                                                    const fb_scalars *__restrict__ scp) {
@@ -1091,6 +1093,205 @@ __global__ void __launch_bounds__(TX *TY) k_sources_sph(Dims m, Geo<T> g, Geo<do
     const T *__restrict__ vz, T *__restrict__ vxt, T *__restrict__ vyt, T *__restrict__ vzt,
     const fb_scalars *__restrict__ scp, int dust, int viscous) {
   b_sources_sph<T, TX, TY>(m, g, gd, rho, cs, vx, vy, vz, vxt, vyt, vzt, scp, dust, viscous, blockIdx);
+}
+
+}  // namespace fb
+
+namespace fb {
+
+// ---------------------------------------------------------------------------
+// Azimuthal sweep, chunked: each thread owns C consecutive cells of a ring
+// and keeps them, with a halo of 3 cells each side, in registers; NT threads
+// hold NT / (nx / C) whole rings.  A pass (van Leer on the residual velocity,
+// or PPA on the uniform fractional velocity) reads the ring from shared
+// memory once, updates every quantity in registers and writes it back, so a
+// ring costs four barriers instead of one per sub-stage.  Per-cell
+// arithmetic is that of vanleer_x_a/_b, fargo_ppa_a..d and update_x as in
+// ring_vl_iface / ring_ppa_iface / upd_x above.
+template <typename T>
+__device__ __forceinline__ T vl_slope(T am, T a0, T ap, T zc, T zp) {
+  const T dqm = (a0 - am) / zc;
+  const T dqp = (ap - a0) / zp;
+  if (dqp * dqm <= (T)0.0) return (T)0.0;
+  return ((T)2. * dqp * dqm) / (dqm + dqp);
+}
+template <typename T>
+__device__ __forceinline__ T mc_slope(T am, T a0, T ap) {
+  const T dqm = (a0 - am), dqp = (ap - a0);
+  if (dqp * dqm <= (T)0.0) return (T)0.0;
+  T sl = (T)0.5 * (ap - am);
+  T work = fabs(sl);
+  if ((T)2.0 * fabs(dqm) < work) work = (T)2.0 * fabs(dqm);
+  if ((T)2.0 * fabs(dqp) < work) work = (T)2.0 * fabs(dqp);
+  return sl < 0 ? -work : work;
+}
+template <typename T>
+__device__ __forceinline__ void ppa_lr(T am, T a0, T ap, T sm, T s0, T sp, T &L, T &R) {
+  R = a0 + (T)0.5 * (ap - a0) - (T)(1.0 / 6.0) * (sp - s0);
+  L = am + (T)0.5 * (a0 - am) - (T)(1.0 / 6.0) * (s0 - sm);
+  if ((R - a0) * (a0 - L) < (T)0.0) { L = a0; R = a0; }
+  const T diff = R - L;
+  const T cord = a0 - (T)0.5 * (L + R);
+  if ((T)6.0 * diff * cord > diff * diff) L = (T)3.0 * a0 - (T)2.0 * R;
+  if (-diff * diff > (T)6.0 * diff * cord) R = (T)3.0 * a0 - (T)2.0 * L;
+}
+
+// Interface values qs(f) at the C+1 faces f = c0 .. c0+C of a window
+// w[0..C+5] holding cells c0-3 .. c0+C+2.  zone(u) is zone_size_x of cell
+// c0-2+u.
+template <typename T, int C, typename Z>
+__device__ __forceinline__ void chunk_iface(const T *w, const T *v, const Z &zone, T dt, bool ppa, T *qs) {
+  if (!ppa) {
+    T sl[C + 2];  // cells c0-1 .. c0+C
+#pragma unroll
+    for (int u = 0; u < C + 2; u++) sl[u] = vl_slope(w[u + 1], w[u + 2], w[u + 3], zone(u + 1), zone(u + 2));
+#pragma unroll
+    for (int f = 0; f <= C; f++) {  // face c0+f: upwind cell c0+f-1 (sl[f]) or c0+f (sl[f+1])
+      if (v[f] > (T)0.0) qs[f] = w[f + 2] + (T)0.5 * (zone(f + 1) - v[f] * dt) * sl[f];
+      else qs[f] = w[f + 3] - (T)0.5 * (zone(f + 2) + v[f] * dt) * sl[f + 1];
+    }
+  } else {
+    T sl[C + 4];  // cells c0-2 .. c0+C+1
+#pragma unroll
+    for (int u = 0; u < C + 4; u++) sl[u] = mc_slope(w[u], w[u + 1], w[u + 2]);
+#pragma unroll
+    for (int f = 0; f <= C; f++) {
+      T L, R, ksi, s;
+      if (v[f] > (T)0.0) {  // upwind cell c0+f-1: window index f+2, slopes sl[f..f+2]
+        ppa_lr(w[f + 1], w[f + 2], w[f + 3], sl[f], sl[f + 1], sl[f + 2], L, R);
+        ksi = v[f] * dt / zone(f + 2);
+        s = R + ksi * (w[f + 2] - R);
+        s += ksi * ((T)1.0 - ksi) * ((T)2.0 * w[f + 2] - R - L);
+      } else {              // cell c0+f: window index f+3, slopes sl[f+1..f+3]
+        ppa_lr(w[f + 2], w[f + 3], w[f + 4], sl[f + 1], sl[f + 2], sl[f + 3], L, R);
+        ksi = -v[f] * dt / zone(f + 2);
+        s = L + ksi * (w[f + 3] - L);
+        s += ksi * ((T)1.0 - ksi) * ((T)2.0 * w[f + 3] - R - L);
+      }
+      qs[f] = s;
+    }
+  }
+}
+
+template <typename T, int C, int NT>
+__device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const Geo<double> &gd, int nq, int jlo,
+                                           int klo, int nj, int nrings, T *rho, T *q0, T *q1, T *q2, T *q3, T *q4,
+                                           T *q5, const T *__restrict__ vxt, const double *__restrict__ vxmed_t,
+                                           int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp,
+                                           uint3 bid) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  const int nx = m.nx, tpr = nx / C, rpc = NT / tpr, nf = 1 + nq;
+  const int slot = threadIdx.x / tpr, lt = threadIdx.x - slot * tpr, c0 = lt * C;
+  const int r = bid.x * rpc + slot;
+  const bool active = slot < rpc && r < nrings;
+  const int j = jlo + (active ? r % nj : 0), k = m.is3d ? klo + (active ? r / nj : 0) : 0;
+  T *qg[6] = {q0, q1, q2, q3, q4, q5};
+  const double dtd = scp->dt;
+  const T dt = (T)dtd;
+  // shared layout: buffers A and B of [slot][field][nx] (field 0 rho, 1.. the
+  // momenta), then the residual-velocity source vxt [slot][nx]
+  const size_t bufsz = (size_t)rpc * nf * nx;
+  T *bufA = sm, *bufB = sm + bufsz, *svx = sm + 2 * bufsz;
+  for (int e = threadIdx.x; e < rpc * nx; e += NT) {
+    const int s = e / nx, i = e - s * nx, rr = bid.x * rpc + s;
+    if (rr < nrings) {
+      const int jj = jlo + rr % nj, kk = m.is3d ? klo + rr / nj : 0;
+      const long long l = m.l(i, jj, kk);
+      T *b = bufA + (size_t)s * nf * nx;
+      b[i] = rho[l];
+      for (int q = 0; q < nq; q++) b[(1 + q) * nx + i] = qg[q][l];
+      svx[s * nx + i] = vxt[l];
+    }
+  }
+  __syncthreads();
+  const int sl0 = slot < rpc ? slot : 0;
+  const double vm = active ? vxmed_t[j + k * m.sy] : 0.0;
+  auto wrap = [&](int i) { i += (i < 0) ? nx : 0; i -= (i >= nx) ? nx : 0; return i; };
+  auto zone = [&](int u) -> T { return zsx(m, g, wrap(c0 - 2 + u), j, k); };
+  const T sxj = ld(g.sxj + j), sxk = ld(g.sxk + k), ivj = ld(g.invvj + j), syk = ld(g.syk + k);
+  for (int pass = 0; pass < 2; pass++) {
+    const T *src = (pass == 0 ? bufA : bufB) + (size_t)sl0 * nf * nx;
+    T *dst = (pass == 0 ? bufB : bufA) + (size_t)sl0 * nf * nx;
+    if (active) {
+      T v[C + 1];
+      if (pass == 0) {
+#pragma unroll
+        for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nx + wrap(c0 + f)] - vm);  // residual
+      } else {
+#pragma unroll
+        for (int f = 0; f <= C; f++) {  // uniform fractional velocity (compute_residual.c:68-73), FP64
+          const double zx = (double)zsx(m, gd, wrap(c0 + f), j, k);
+          const double ntilde = vm * dtd / zx;
+          const double nround = floor(ntilde + 0.5);
+          v[f] = (T)((ntilde - nround) * zx / dtd);
+        }
+      }
+      T wr[C + 6], rs[C + 1];
+#pragma unroll
+      for (int u = 0; u < C + 6; u++) wr[u] = src[wrap(c0 - 3 + u)];
+      chunk_iface<T, C>(wr, v, zone, dt, pass == 1, rs);
+      for (int q = 0; q < nq; q++) {
+        const T *sq = src + (1 + q) * nx;
+        T wq[C + 6], qs[C + 1];
+#pragma unroll
+        for (int u = 0; u < C + 6; u++) wq[u] = sq[wrap(c0 - 3 + u)] / wr[u];  // DivideByRho
+        chunk_iface<T, C>(wq, v, zone, dt, pass == 1, qs);
+#pragma unroll
+        for (int u = 0; u < C; u++) {
+          const T fl = v[u] * qs[u] * rs[u] - v[u + 1] * qs[u + 1] * rs[u + 1];
+          dst[(1 + q) * nx + c0 + u] = sq[c0 + u] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < C; u++) {
+        const T fl = v[u] * rs[u] - v[u + 1] * rs[u + 1];
+        dst[c0 + u] = wr[u + 3] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+      }
+    }
+    __syncthreads();
+  }
+  // AdvectSHIFT (advect_shift.c:49-54): integer shift nround of cell 0
+  for (int e = threadIdx.x; e < rpc * nx; e += NT) {
+    const int s = e / nx, i = e - s * nx, rr = bid.x * rpc + s;
+    if (rr >= nrings) continue;
+    const int jj = jlo + rr % nj, kk = m.is3d ? klo + rr / nj : 0;
+    const double vms = vxmed_t[jj + kk * m.sy];
+    const double ntilde0 = vms * dtd / (double)zsx(m, gd, 0, jj, kk);
+    const int nsh = (int)floor(ntilde0 + 0.5);
+    if (i == 0 && nshift_out) nshift_out[jj + kk * m.sy] = nsh;
+    int it = (i - nsh) % nx;
+    if (it < 0) it += nx;
+    const T *b = bufA + (size_t)s * nf * nx;
+    const long long l = m.l(i, jj, kk);
+    rho[l] = b[it];
+    for (int q = 0; q < nq; q++) qg[q][l] = b[(1 + q) * nx + it];
+  }
+}
+
+// shared memory of b_sweep_x2 for a ring of nx cells (rpc rings per CTA)
+__host__ __device__ inline size_t sweep_x2_smem(int nx, int C, int nt, int nq, size_t esz) {
+  const int rpc = nt / (nx / C);
+  return (size_t)rpc * nx * (2 * (1 + nq) + 1) * esz;
+}
+
+// the chunk width a ring of nx cells uses with NT threads per CTA (0: none fits)
+__host__ __device__ inline int sweep_x_chunk(int nx, int nt) {
+  // the smallest of 4, 8, 16 that fits a ring into nt threads; odd rings 2, 1
+  const int cs[5] = {4, 8, 16, 2, 1};
+  for (int t = 0; t < 5; t++)
+    if (nx % cs[t] == 0 && nx / cs[t] <= nt) return cs[t];
+  return 0;
+}
+
+template <typename T, int C>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_sweep_x2(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
+                                                  int nj, int nrings, T *rho, T *q0, T *q1, T *q2, T *q3, T *q4,
+                                                  T *q5, const T *__restrict__ vxt,
+                                                  const double *__restrict__ vxmed_t, int *__restrict__ nshift_out,
+                                                  const fb_scalars *__restrict__ scp) {
+  b_sweep_x2<T, C, 256>(m, g, gd, nq, jlo, klo, nj, nrings, rho, q0, q1, q2, q3, q4, q5, vxt, vxmed_t, nshift_out,
+                        scp, blockIdx);
 }
 
 }  // namespace fb

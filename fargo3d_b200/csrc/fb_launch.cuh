@@ -140,18 +140,33 @@ static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
   T *rho_out = (T *)(b ? F.rho_b : F.rho_a);
   T *q[6] = {(T *)(b ? F.mpx_b : F.mpx), (T *)(b ? F.mmx_b : F.mmx), (T *)(b ? F.mpy_b : F.mpy),
              (T *)(b ? F.mmy_b : F.mmy), (T *)(b ? F.mpz_b : F.mpz), (T *)(b ? F.mmz_b : F.mmz)};
-  // azimuthal sweep, one CTA per ring
-  const size_t smem = (size_t)(8 + nq) * m.nx * sizeof(T);
-  static size_t configured = 0;
-  if (smem > configured) {
-    cudaFuncSetAttribute(k_sweep_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = smem;
-  }
+  // azimuthal sweep: C cells per thread, whole rings per CTA of 256 threads
+  const int C = sweep_x_chunk(m.nx, 256);
+  if (C == 0) return (int)cudaErrorInvalidValue;
+  const int nj = yhi - ylo + 1, nrings = nj * (m.is3d ? m.nz + 1 : 1);
+  const int rpc = 256 / (m.nx / C);
+  const size_t smem = sweep_x2_smem(m.nx, C, 256, nq, sizeof(T));
   const int klo = m.is3d ? FB_NGH - 1 : 0;
-  dim3 gx(yhi - ylo + 1, m.is3d ? m.nz + 1 : 1);
-  const int threads = m.nx >= 512 ? 512 : 256;
-  k_sweep_x<T><<<gx, threads, smem, st>>>(m, g, gd, nq, ylo, klo, rho_out, q[0], q[1], q[2], q[3], q[4], q[5],
-                                           (const T *)F.vxt, F.vxmed_t, F.nshift, d->scal_dev);
+  dim3 gx((nrings + rpc - 1) / rpc);
+#define FB_SX(CC)                                                                                          \
+  {                                                                                                        \
+    static size_t conf = 0;                                                                                \
+    if (smem > conf) {                                                                                     \
+      cudaFuncSetAttribute(k_sweep_x2<T, CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+      conf = smem;                                                                                         \
+    }                                                                                                      \
+    k_sweep_x2<T, CC><<<gx, 256, smem, st>>>(m, g, gd, nq, ylo, klo, nj, nrings, rho_out, q[0], q[1], q[2], \
+                                             q[3], q[4], q[5], (const T *)F.vxt, F.vxmed_t, F.nshift,      \
+                                             d->scal_dev);                                                 \
+  }
+  switch (C) {
+    case 16: FB_SX(16) break;
+    case 8: FB_SX(8) break;
+    case 4: FB_SX(4) break;
+    case 2: FB_SX(2) break;
+    default: FB_SX(1) break;
+  }
+#undef FB_SX
   return (int)cudaGetLastError();
 }
 
