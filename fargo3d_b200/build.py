@@ -57,7 +57,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     objs = []
-    fast32 = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+    fast32 = [] if os.environ.get("FB_FP32_IEEE") else ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
     cu_flags = {"fb_kernels_f64.cu": ["--fmad=false"], "fb_kernels_f32.cu": fast32, "fb_noalloc.cu": ["--fmad=false"],
                 "fb_batch_f64.cu": ["--fmad=false"], "fb_batch_f32.cu": fast32}
     for f in sorted(os.listdir(CSRC)):

@@ -92,11 +92,11 @@ int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_ba
       cudaMemcpy(B->items[s], v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice);
     }
   }
-  const size_t esz = precision == FB_FP64 ? 8 : 4;
   B->smem_x = 0;
   (void)maxnx;
   for (int i = 0; i < n; i++) {
-    size_t s = sweep_x2_smem(hd[i].nx, B->cx, 256, B->is3d ? 6 : 4, esz);
+    /* the sweep keeps its rings in the compute precision (double for both) */
+    size_t s = sweep_x2_smem(hd[i].nx, B->cx, 256, B->is3d ? 6 : 4, sizeof(double));
     if (s > B->smem_x) B->smem_x = s;
   }
   *out = B;

@@ -30,97 +30,97 @@ constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_NS = 8, 
   const fb_fluid_dev &F = D.fl[f];                     \
   (void)F;
 
-template <typename T, bool ORDERED>
+template <typename T, bool ORDERED, typename S>
 __global__ void __launch_bounds__(256) kb_rowsum(const fb_disk_dev *ds, const int4 *items, int f, int which) {
   FB_TILE
-  b_rowsum<T, ORDERED>(dims_of(D), geo_of<double>(D.geomd), (const T *)(which == 0 ? F.vx : F.vxt),
+  b_rowsum<T, ORDERED, S>(dims_of(D), geo_of<double>(D.geomd), (const S *)(which == 0 ? F.vx : F.vxt),
                        which == 0 ? F.vxmed : F.vxmed_t, D.xlen, bid);
 }
 
-template <typename T>
+template <typename T, typename S>
 __global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
-  b_cfl<T>(dims_of(D), geo_of<T>(D.geom), (const T *)F.rho, (const T *)F.cs, (const T *)F.vx, (const T *)F.vy,
-           (const T *)F.vz, F.vxmed, scp, D.cfl, D.mindx, (unsigned long long *)D.dtmin, bid);
+  b_cfl<T, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), (const S *)F.rho, (const S *)F.cs, (const S *)F.vx, (const S *)F.vy,
+           (const S *)F.vz, F.vxmed, scp, D.cfl, D.mindx, (unsigned long long *)D.dtmin, bid);
 }
 
-template <typename T>
+template <typename T, typename S>
 __global__ void __launch_bounds__(SRC2_TX *SRC2_TY) kb_sources_cyl(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
-  b_sources_cyl<T, SRC2_TX, SRC2_TY>(dims_of(D), geo_of<T>(D.geom), geo_of<double>(D.geomd), (const T *)F.rho,
-                                     (const T *)F.cs, (const T *)F.vx, (const T *)F.vy, (T *)F.vxt, (T *)F.vyt, scp,
+  b_sources_cyl<T, SRC2_TX, SRC2_TY, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), (const S *)F.rho,
+                                     (const S *)F.cs, (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, scp,
                                      F.dust, !F.dust, bid);
 }
 
-template <typename T>
+template <typename T, typename S>
 __global__ void __launch_bounds__(SRC3_TX *SRC3_TY) kb_sources_sph(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
-  b_sources_sph<T, SRC3_TX, SRC3_TY>(dims_of(D), geo_of<T>(D.geom), geo_of<double>(D.geomd), (const T *)F.rho,
-                                     (const T *)F.cs, (const T *)F.vx, (const T *)F.vy, (const T *)F.vz, (T *)F.vxt,
-                                     (T *)F.vyt, (T *)F.vzt, scp, F.dust, !F.dust, bid);
+  b_sources_sph<T, SRC3_TX, SRC3_TY, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), (const S *)F.rho,
+                                     (const S *)F.cs, (const S *)F.vx, (const S *)F.vy, (const S *)F.vz, (S *)F.vxt,
+                                     (S *)F.vyt, (S *)F.vzt, scp, F.dust, !F.dust, bid);
 }
 
-template <typename T>
+template <typename T, typename S>
 __global__ void kb_bnd(const fb_disk_dev *ds, const int4 *items, int f, int vtemp, int zside) {
   FB_TILE
   Dims m = dims_of(D);
   BndTab tb{D.bnd_tab, m.sy, m.sz};
-  T *vx = (T *)(vtemp ? F.vxt : F.vx), *vy = (T *)(vtemp ? F.vyt : F.vy), *vz = (T *)(vtemp ? F.vzt : F.vz);
-  if (zside) b_bnd_z<T>(m, geo_of<T>(D.geom), tb, (T *)F.rho, vx, vy, vz, scp, !vtemp, bid);
-  else b_bnd_y<T>(m, geo_of<T>(D.geom), tb, (T *)F.rho, vx, vy, vz, scp, !vtemp, bid);
+  S *vx = (S *)(vtemp ? F.vxt : F.vx), *vy = (S *)(vtemp ? F.vyt : F.vy), *vz = (S *)(vtemp ? F.vzt : F.vz);
+  if (zside) b_bnd_z<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, bid);
+  else b_bnd_y<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, bid);
 }
 
-template <typename T, int DIR>
+template <typename T, int DIR, typename S>
 __global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? 4 : 1) kb_sweep_col(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   Dims m = dims_of(D);
   const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;
-  QSrc<T> src;
-  src.vxt = (const T *)F.vxt; src.vyt = (const T *)F.vyt; src.vzt = (const T *)F.vzt; src.of = (T)0;
+  QSrc<T, S> src;
+  src.vxt = (const S *)F.vxt; src.vyt = (const S *)F.vyt; src.vzt = (const S *)F.vzt; src.of = (T)0;
   if (!m.is3d || DIR == 1) {
-    src.rho = (const T *)F.rho;
+    src.rho = (const S *)F.rho;
     for (int q = 0; q < 6; q++) src.q[q] = nullptr;
     src.from_v = 1;
   } else {
-    src.rho = (const T *)F.rho_a;
-    src.q[0] = (const T *)F.mpx; src.q[1] = (const T *)F.mmx; src.q[2] = (const T *)F.mpy;
-    src.q[3] = (const T *)F.mmy; src.q[4] = (const T *)F.mpz; src.q[5] = (const T *)F.mmz;
+    src.rho = (const S *)F.rho_a;
+    src.q[0] = (const S *)F.mpx; src.q[1] = (const S *)F.mmx; src.q[2] = (const S *)F.mpy;
+    src.q[3] = (const S *)F.mmy; src.q[4] = (const S *)F.mpz; src.q[5] = (const S *)F.mmz;
     src.from_v = 0;
   }
   if (!m.is3d) {
-    b_sweep_col<T, 0, COL_NS>(m, geo_of<T>(D.geom), src, 4, ylo, yhi, 0, (T *)F.rho_a, (T *)F.mpx, (T *)F.mmx,
-                              (T *)F.mpy, (T *)F.mmy, nullptr, nullptr, scp, bid);
+    b_sweep_col<T, 0, COL_NS, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), src, 4, ylo, yhi, 0, (S *)F.rho_a, (S *)F.mpx, (S *)F.mmx,
+                              (S *)F.mpy, (S *)F.mmy, nullptr, nullptr, scp, bid);
   } else if (DIR == 1) {
-    b_sweep_col<T, 1, COL_NS>(m, geo_of<T>(D.geom), src, 6, FB_NGH - 1, m.nz + FB_NGH - 1, 0, (T *)F.rho_a,
-                              (T *)F.mpx, (T *)F.mmx, (T *)F.mpy, (T *)F.mmy, (T *)F.mpz, (T *)F.mmz, scp, bid);
+    b_sweep_col<T, 1, COL_NS, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), src, 6, FB_NGH - 1, m.nz + FB_NGH - 1, 0, (S *)F.rho_a,
+                              (S *)F.mpx, (S *)F.mmx, (S *)F.mpy, (S *)F.mmy, (S *)F.mpz, (S *)F.mmz, scp, bid);
   } else {
-    b_sweep_col<T, 0, COL_NS>(m, geo_of<T>(D.geom), src, 6, ylo, yhi, FB_NGH - 1, (T *)F.rho_b, (T *)F.mpx_b,
-                              (T *)F.mmx_b, (T *)F.mpy_b, (T *)F.mmy_b, (T *)F.mpz_b, (T *)F.mmz_b, scp, bid);
+    b_sweep_col<T, 0, COL_NS, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), src, 6, ylo, yhi, FB_NGH - 1, (S *)F.rho_b, (S *)F.mpx_b,
+                              (S *)F.mmx_b, (S *)F.mpy_b, (S *)F.mmy_b, (S *)F.mpz_b, (S *)F.mmz_b, scp, bid);
   }
 }
 
-template <typename T, int C>
+template <typename T, int C, typename S>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) kb_sweep_x(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   Dims m = dims_of(D);
   const bool b = m.is3d;
   const int nj = m.ny + 1, nrings = nj * (b ? m.nz + 1 : 1);
-  b_sweep_x2<T, C, 256>(m, geo_of<T>(D.geom), geo_of<double>(D.geomd), b ? 6 : 4, FB_NGH - 1, b ? FB_NGH - 1 : 0,
-                        nj, nrings, (T *)(b ? F.rho_b : F.rho_a), (T *)(b ? F.mpx_b : F.mpx),
-                        (T *)(b ? F.mmx_b : F.mmx), (T *)(b ? F.mpy_b : F.mpy), (T *)(b ? F.mmy_b : F.mmy),
-                        (T *)(b ? F.mpz_b : F.mpz), (T *)(b ? F.mmz_b : F.mmz), (const T *)F.vxt, F.vxmed_t, F.nshift,
+  b_sweep_x2<T, C, 256, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), b ? 6 : 4, FB_NGH - 1, b ? FB_NGH - 1 : 0,
+                        nj, nrings, (S *)(b ? F.rho_b : F.rho_a), (S *)(b ? F.mpx_b : F.mpx),
+                        (S *)(b ? F.mmx_b : F.mmx), (S *)(b ? F.mpy_b : F.mpy), (S *)(b ? F.mmy_b : F.mmy),
+                        (S *)(b ? F.mpz_b : F.mpz), (S *)(b ? F.mmz_b : F.mmz), (const S *)F.vxt, F.vxmed_t, F.nshift,
                         scp, bid);
 }
 
-template <typename T>
+template <typename T, typename S>
 __global__ void __launch_bounds__(NV_BX) kb_newvel(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   Dims m = dims_of(D);
   const bool b = m.is3d;
-  b_newvel<T>(m, geo_of<T>(D.geom), (const T *)(b ? F.rho_b : F.rho_a), (const T *)(b ? F.mpx_b : F.mpx),
-              (const T *)(b ? F.mmx_b : F.mmx), (const T *)(b ? F.mpy_b : F.mpy), (const T *)(b ? F.mmy_b : F.mmy),
-              (const T *)(b ? F.mpz_b : F.mpz), (const T *)(b ? F.mmz_b : F.mmz), (T *)F.rho, (T *)F.vx,
-              (T *)F.vy, (T *)F.vz, (const T *)F.rho0, (const T *)F.vx0, (const T *)F.vy0, (const T *)F.vz0,
+  b_newvel<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), (const S *)(b ? F.rho_b : F.rho_a), (const S *)(b ? F.mpx_b : F.mpx),
+              (const S *)(b ? F.mmx_b : F.mmx), (const S *)(b ? F.mpy_b : F.mpy), (const S *)(b ? F.mmy_b : F.mmy),
+              (const S *)(b ? F.mpz_b : F.mpz), (const S *)(b ? F.mmz_b : F.mmz), (S *)F.rho, (S *)F.vx,
+              (S *)F.vy, (S *)F.vz, (const S *)F.rho0, (const S *)F.vx0, (const S *)F.vy0, (const S *)F.vz0,
               D.ramps, D.stockholm, scp, bid);
 }
 
@@ -201,17 +201,17 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
   return (int)v.size();
 }
 
-template <typename T>
+template <typename T, typename S>
 static void configure_sweep_x(fb_batch *B) {
   static size_t done[17];
   if (done[B->cx] >= B->smem_x) return;
   done[B->cx] = B->smem_x;
   switch (B->cx) {
-    case 16: cudaFuncSetAttribute(kb_sweep_x<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
-    case 8: cudaFuncSetAttribute(kb_sweep_x<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
-    case 4: cudaFuncSetAttribute(kb_sweep_x<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
-    case 2: cudaFuncSetAttribute(kb_sweep_x<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
-    default: cudaFuncSetAttribute(kb_sweep_x<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
+    case 16: cudaFuncSetAttribute(kb_sweep_x<T, 16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
+    case 8: cudaFuncSetAttribute(kb_sweep_x<T, 8, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
+    case 4: cudaFuncSetAttribute(kb_sweep_x<T, 4, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
+    case 2: cudaFuncSetAttribute(kb_sweep_x<T, 2, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
+    default: cudaFuncSetAttribute(kb_sweep_x<T, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
   }
 }
 
@@ -229,52 +229,52 @@ static void pmark(cudaStream_t st, const char *name) {
   g_prof->name[g_prof->n++] = name;
 }
 
-template <typename T>
+template <typename T, typename S>
 static int launch_step(fb_batch *B, double DT) {
-  configure_sweep_x<T>(B);
+  configure_sweep_x<T, S>(B);
   cudaStream_t st = B->stream;
   pmark(st, "start");
   const fb_disk_dev *ds = B->d_disks;
   const int nf = B->nfluids;
   auto grid = [&](int s) { return dim3((unsigned)B->nitems[s]); };
   for (int f = 0; f < nf; f++) {
-    if (B->precision == FB_FP64) kb_rowsum<T, true><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
-    else kb_rowsum<T, false><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
+    if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
+    else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
   }
   pmark(st, "rowsum");
-  for (int f = 0; f < nf; f++) kb_cfl<T><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
+  for (int f = 0; f < nf; f++) kb_cfl<T, S><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
   pmark(st, "cfl");
   kb_scalars<<<(B->n + 63) / 64, 64, 0, st>>>(ds, B->d_psys, B->n, DT);
   pmark(st, "scalars");
   for (int f = 0; f < nf; f++) {
-    if (B->is3d) kb_sources_sph<T><<<grid(ST_SOURCES), dim3(SRC3_TX, SRC3_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
-    else kb_sources_cyl<T><<<grid(ST_SOURCES), dim3(SRC2_TX, SRC2_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
+    if (B->is3d) kb_sources_sph<T, S><<<grid(ST_SOURCES), dim3(SRC3_TX, SRC3_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
+    else kb_sources_cyl<T, S><<<grid(ST_SOURCES), dim3(SRC2_TX, SRC2_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
     pmark(st, "sources");
-    if (B->is3d) kb_bnd<T><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 1, 1);
-    kb_bnd<T><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 1, 0);
+    if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 1, 1);
+    kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 1, 0);
     pmark(st, "bnd_vtemp");
   }
   for (int f = 0; f < nf; f++) {
-    if (B->precision == FB_FP64) kb_rowsum<T, true><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
-    else kb_rowsum<T, false><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
+    if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
+    else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
     pmark(st, "rowsum_vtemp");
-    if (B->is3d) kb_sweep_col<T, 1><<<grid(ST_SWEEP_Z), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Z], f);
-    kb_sweep_col<T, 0><<<grid(ST_SWEEP_Y), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Y], f);
+    if (B->is3d) kb_sweep_col<T, 1, S><<<grid(ST_SWEEP_Z), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Z], f);
+    kb_sweep_col<T, 0, S><<<grid(ST_SWEEP_Y), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Y], f);
     pmark(st, "sweep_cols");
     switch (B->cx) {
-      case 16: kb_sweep_x<T, 16><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 8: kb_sweep_x<T, 8><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 4: kb_sweep_x<T, 4><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 2: kb_sweep_x<T, 2><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      default: kb_sweep_x<T, 1><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      case 16: kb_sweep_x<T, 16, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      case 8: kb_sweep_x<T, 8, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      case 4: kb_sweep_x<T, 4, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      case 2: kb_sweep_x<T, 2, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      default: kb_sweep_x<T, 1, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
     }
     pmark(st, "sweep_x");
   }
   for (int f = 0; f < nf; f++) {
-    kb_newvel<T><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
+    kb_newvel<T, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
     pmark(st, "newvel");
-    if (B->is3d) kb_bnd<T><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 0, 1);
-    kb_bnd<T><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 0, 0);
+    if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 0, 1);
+    kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 0, 0);
     pmark(st, "bnd");
   }
   return (int)cudaGetLastError();

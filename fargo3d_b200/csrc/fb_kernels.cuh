@@ -79,8 +79,8 @@ __device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i
 // (XMAX - XMIN), accumulated sequentially in i as the reference does, one
 // lane per ring; the rings' rows are staged through shared memory so that
 // global loads stay coalesced.  32 rings per CTA of 256 threads.
-template <typename T, bool ORDERED>
-__device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const T *__restrict__ v,
+template <typename T, bool ORDERED, typename S = T>
+__device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const S *__restrict__ v,
                                                  double *__restrict__ out, double xlen, uint3 bid) {
   constexpr int R = 32, CH = 128;
   __shared__ double buf[R][CH + 1];
@@ -125,10 +125,10 @@ __device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const T *__rest
     out[myring] = tot / xlen;
   }
 }
-template <typename T, bool ORDERED>
-__global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const T *__restrict__ v,
+template <typename T, bool ORDERED, typename S = T>
+__global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const S *__restrict__ v,
                                                  double *__restrict__ out, double xlen) {
-  b_rowsum<T, ORDERED>(m, gd, v, out, xlen, blockIdx);
+  b_rowsum<T, ORDERED, S>(m, gd, v, out, xlen, blockIdx);
 }
 
 // ---------------------------------------------------------------------------
@@ -160,10 +160,10 @@ __device__ __forceinline__ T zsz(const Dims &m, const Geo<T> &g, int j, int k) {
   return (ld(g.zmin + k + 1) - ld(g.zmin + k));
 }
 
-template <typename T>
-__device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const T *__restrict__ rho, const T *__restrict__ cs,
-                                             const T *__restrict__ vx, const T *__restrict__ vy,
-                                             const T *__restrict__ vz, const double *__restrict__ vxmed,
+template <typename T, typename S = T>
+__device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const S *__restrict__ rho, const S *__restrict__ cs,
+                                             const S *__restrict__ vx, const S *__restrict__ vy,
+                                             const S *__restrict__ vz, const double *__restrict__ vxmed,
                                              const fb_scalars *__restrict__ sc, double cfl_num,
                                              double mindx, unsigned long long *__restrict__ dtmin, uint3 bid) {
   const int j = FB_NGH + bid.x;
@@ -222,13 +222,13 @@ __device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const T *__restrict__ rh
     if (threadIdx.x == 0 && v > 0.0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
   }
 }
-template <typename T>
-__global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const T *__restrict__ rho, const T *__restrict__ cs,
-                                             const T *__restrict__ vx, const T *__restrict__ vy,
-                                             const T *__restrict__ vz, const double *__restrict__ vxmed,
+template <typename T, typename S = T>
+__global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const S *__restrict__ rho, const S *__restrict__ cs,
+                                             const S *__restrict__ vx, const S *__restrict__ vy,
+                                             const S *__restrict__ vz, const double *__restrict__ vxmed,
                                              const fb_scalars *__restrict__ sc, double cfl_num,
                                              double mindx, unsigned long long *__restrict__ dtmin) {
-  b_cfl<T>(m, g, rho, cs, vx, vy, vz, vxmed, sc, cfl_num, mindx, dtmin, blockIdx);
+  b_cfl<T, S>(m, g, rho, cs, vx, vy, vz, vxmed, sc, cfl_num, mindx, dtmin, blockIdx);
 }
 
 // ---------------------------------------------------------------------------
@@ -268,10 +268,10 @@ namespace fb {
 // addviscosity_cyl, SubStep2_a/b, fused over a TX x TY tile of active cells.
 // Inputs (rho, cs, v, P, Pot) are staged with a one-cell halo; the stress
 // tensor is computed once per point into shared memory.
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, typename S = T>
 __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
-    const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx,
-    const T *__restrict__ vy, T *__restrict__ vxt, T *__restrict__ vyt,
+    const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx,
+    const S *__restrict__ vy, S *__restrict__ vxt, S *__restrict__ vyt,
     const fb_scalars *__restrict__ scp, int dust, int viscous, uint3 bid) {
   constexpr int W = TX + 2, H = TY + 2;
   __shared__ T s_rho[H][W], s_cs[H][W], s_vx[H][W], s_vy[H][W], s_p[H][W];
@@ -382,12 +382,12 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   vxt[l] = ax;
   vyt[l] = ay;
 }
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, typename S = T>
 __global__ void __launch_bounds__(TX *TY) k_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
-    const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx,
-    const T *__restrict__ vy, T *__restrict__ vxt, T *__restrict__ vyt,
+    const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx,
+    const S *__restrict__ vy, S *__restrict__ vxt, S *__restrict__ vyt,
     const fb_scalars *__restrict__ scp, int dust, int viscous) {
-  b_sources_cyl<T, TX, TY>(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, blockIdx);
+  b_sources_cyl<T, TX, TY, S>(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, blockIdx);
 }
 
 }  // namespace fb
@@ -414,9 +414,9 @@ struct BndTab {
 };
 
 // Radial sides: one thread per (i, ghost row jj, side s, layer k).
-template <typename T>
-__device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
-                        T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
+template <typename T, typename S = T>
+__device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
+                        S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
                         int do_rho, uint3 bid) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   const int jj = bid.y % 3, s = bid.y / 3, k = bid.z;
@@ -443,17 +443,17 @@ __device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, T *__restri
   // Vz: SYMMETRIC, centred in y
   if (m.is3d) vz[lgh] = vz[lact];
 }
-template <typename T>
-__global__ void k_bnd_y(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
-                        T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
+template <typename T, typename S = T>
+__global__ void k_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
+                        S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
                         int do_rho) {
-  b_bnd_y<T>(m, g, tb, rho, vx, vy, vz, scp, do_rho, blockIdx);
+  b_bnd_y<T, S>(m, g, tb, rho, vx, vy, vz, scp, do_rho, blockIdx);
 }
 
 // Colatitude sides (3D): one thread per (i, j, ghost layer kk, side s).
-template <typename T>
-__device__ __forceinline__ void b_bnd_z(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
-                        T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
+template <typename T, typename S = T>
+__device__ __forceinline__ void b_bnd_z(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
+                        S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
                         int do_rho, uint3 bid) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   const int j = bid.y, kk = bid.z % 3, s = bid.z / 3;
@@ -472,11 +472,11 @@ __device__ __forceinline__ void b_bnd_z(Dims m, Geo<T> g, BndTab tb, T *__restri
   else if (kk < nghz - 1) vz[m.l(i, j, nz + nghz + 1 + kk)] = -vz[m.l(i, j, klacts)];
   vz[m.l(i, j, knull)] = 0;
 }
-template <typename T>
-__global__ void k_bnd_z(Dims m, Geo<T> g, BndTab tb, T *__restrict__ rho, T *__restrict__ vx,
-                        T *__restrict__ vy, T *__restrict__ vz, const fb_scalars *__restrict__ scp,
+template <typename T, typename S = T>
+__global__ void k_bnd_z(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
+                        S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
                         int do_rho) {
-  b_bnd_z<T>(m, g, tb, rho, vx, vy, vz, scp, do_rho, blockIdx);
+  b_bnd_z<T, S>(m, g, tb, rho, vx, vy, vz, scp, do_rho, blockIdx);
 }
 
 // ---------------------------------------------------------------------------
@@ -531,16 +531,16 @@ __device__ __forceinline__ void col_sweep_q(const ColGeo<T, DIR> &cg, int c0, co
 // Quantity sources: 2D Y sweep and 3D Z sweep build the momenta from rho and
 // V_temp (momenta_x.c:76-85, momenta_y.c:65-66, momenta_z.c:61-66); the 3D
 // Y sweep reads them from the Z sweep's output buffers.
-template <typename T>
+template <typename T, typename S = T>
 struct QSrc {
-  const T *rho, *vxt, *vyt, *vzt;
-  const T *q[6];   // when from buffers: mpx, mmx, mpy, mmy, mpz, mmz
+  const S *rho, *vxt, *vyt, *vzt;
+  const S *q[6];   // when from buffers: mpx, mmx, mpy, mmy, mpz, mmz
   int from_v;
   T of;
 };
 
-template <typename T>
-__device__ __forceinline__ T momentum(const Dims &m, const Geo<T> &g, const QSrc<T> &src, int q, int i, int j,
+template <typename T, typename S>
+__device__ __forceinline__ T momentum(const Dims &m, const Geo<T> &g, const QSrc<T, S> &src, int q, int i, int j,
                                       int k, long long l, T r) {
   if (!src.from_v) return src.q[q][l];
   switch (q) {
@@ -571,10 +571,10 @@ __device__ __forceinline__ T momentum(const Dims &m, const Geo<T> &g, const QSrc
 // One launch covers cells [clo, chi] along DIR for every column in range.
 // grid.x: columns along x (blockDim.x threads), grid.y: the other transverse
 // index (row j for Z sweeps, layer k for Y sweeps), grid.z: segments along DIR.
-template <typename T, int DIR, int NS>
-__device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int nq, int clo, int chi,
-                                                   int t2lo, T *__restrict__ rho_out, T *q_out0, T *q_out1,
-                                                   T *q_out2, T *q_out3, T *q_out4, T *q_out5,
+template <typename T, int DIR, int NS, typename S = T>
+__device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, int nq, int clo, int chi,
+                                                   int t2lo, S *__restrict__ rho_out, S *q_out0, S *q_out1,
+                                                   S *q_out2, S *q_out3, S *q_out4, S *q_out5,
                                                    const fb_scalars *__restrict__ scp, uint3 bid) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   if (i >= m.nx) return;
@@ -589,14 +589,31 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int n
   // cells beyond chi + 2 (faces beyond chi + 1) never reach an output: clamp
   const int cmax = chi + 2;
   T r[NS + 4], vel[NS + 1], rs[NS + 1], a[NS + 4], qs[NS + 1];
-  const T *vface = (DIR == 0) ? src.vyt : src.vzt;
+  const S *vface = (DIR == 0) ? src.vyt : src.vzt;
 #pragma unroll
   for (int w = 0; w < NS + 4; w++) r[w] = src.rho[cidx(min(c0 - 2 + w, cmax))];
 #pragma unroll
   for (int f = 0; f < NS + 1; f++) vel[f] = vface[cidx(min(c0 + f, cmax - 1))];
   // density interface values (VanLeer*_a/_b on Density -> DensStar)
   col_sweep_q<T, DIR, NS>(cg, c0, r, vel, rs, dt, rs);
-  T *qo[6] = {q_out0, q_out1, q_out2, q_out3, q_out4, q_out5};
+  // With reduced-precision storage (S narrower than T) the azimuthal
+  // momenta live in the buffers relative to the frame's rotation,
+  // Mrel = M - OMEGAFRAME * R^2 * rho (R the cylindrical radius): the stored
+  // numbers are then of the size of the residual velocity, so their rounding
+  // is too.  The sweep itself runs on M = Mrel + OMEGAFRAME R^2 rho in T.
+  constexpr bool REL = sizeof(S) < sizeof(T);
+  T rnew[NS];
+#pragma unroll
+  for (int u = 0; u < NS; u++) {
+    const int c = c0 + u;
+    const T flux = cg.surf(vel[u] * rs[u], c) - cg.surf(vel[u + 1] * rs[u + 1], c + 1);
+    rnew[u] = r[u + 2] + cg.finish(flux, dt, c);
+  }
+  auto rc2 = [&](int jj, int kk) -> T {  // cylindrical radius squared times OMEGAFRAME
+    const T rr = m.sph ? ld(g.ymed + jj) * ld(g.sin_zmed + kk) : ld(g.ymed + jj);
+    return src.of * rr * rr;
+  };
+  S *qo[6] = {q_out0, q_out1, q_out2, q_out3, q_out4, q_out5};
 #pragma unroll
   for (int q = 0; q < 6; q++) {
     if (q >= nq) break;
@@ -606,6 +623,7 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int n
       const int c = min(c0 - 2 + w, cmax);
       const int jj = (DIR == 0) ? c : j, kk = (DIR == 0) ? k : c;
       qv[w] = momentum(m, g, src, q, i, jj, kk, cidx(c), r[w]);
+      if (REL && q < 2 && !src.from_v) qv[w] += rc2(jj, kk) * r[w];
       a[w] = qv[w] / r[w];
     }
     col_sweep_q<T, DIR, NS>(cg, c0, a, vel, rs, dt, qs);
@@ -614,25 +632,28 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int n
       const int c = c0 + u;
       if (c <= chi) {
         const T flux = cg.surf(vel[u] * qs[u] * rs[u], c) - cg.surf(vel[u + 1] * qs[u + 1] * rs[u + 1], c + 1);
-        qo[q][cidx(c)] = qv[u + 2] + cg.finish(flux, dt, c);
+        T out = qv[u + 2] + cg.finish(flux, dt, c);
+        if (REL && q < 2) {
+          const int jj = (DIR == 0) ? c : j, kk = (DIR == 0) ? k : c;
+          out -= rc2(jj, kk) * rnew[u];
+        }
+        qo[q][cidx(c)] = out;
       }
     }
   }
 #pragma unroll
   for (int u = 0; u < NS; u++) {
     const int c = c0 + u;
-    if (c <= chi) {
-      const T flux = cg.surf(vel[u] * rs[u], c) - cg.surf(vel[u + 1] * rs[u + 1], c + 1);
-      rho_out[cidx(c)] = r[u + 2] + cg.finish(flux, dt, c);
-    }
+    if (c <= chi) rho_out[cidx(c)] = rnew[u];
   }
 }
-template <typename T, int DIR, int NS>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_sweep_col(Dims m, Geo<T> g, QSrc<T> src, int nq, int clo, int chi,
-                                                   int t2lo, T *__restrict__ rho_out, T *q_out0, T *q_out1,
-                                                   T *q_out2, T *q_out3, T *q_out4, T *q_out5,
+
+template <typename T, int DIR, int NS, typename S = T>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, int nq, int clo, int chi,
+                                                   int t2lo, S *__restrict__ rho_out, S *q_out0, S *q_out1,
+                                                   S *q_out2, S *q_out3, S *q_out4, S *q_out5,
                                                    const fb_scalars *__restrict__ scp) {
-  b_sweep_col<T, DIR, NS>(m, g, src, nq, clo, chi, t2lo, rho_out, q_out0, q_out1, q_out2, q_out3, q_out4, q_out5, scp, blockIdx);
+  b_sweep_col<T, DIR, NS, S>(m, g, src, nq, clo, chi, t2lo, rho_out, q_out0, q_out1, q_out2, q_out3, q_out4, q_out5, scp, blockIdx);
 }
 
 }  // namespace fb
@@ -640,194 +661,17 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_sweep_col(Dims 
 namespace fb {
 
 // ---------------------------------------------------------------------------
-// Azimuthal sweep, one CTA per ring (transport.c:129-158): ComputeResidual,
-// X_advection with van Leer on the residual velocity, X_advection with PPA on
-// the uniform fractional velocity, then AdvectSHIFT by the integer shift.
-// The ring of the density and of every momentum stays in shared memory
-// across the three passes; only the final shifted values are written.
-// Dynamic shared memory: (8 + nq) * nx elements of T.
-template <typename T>
-struct RingSmem {
-  T *rho, *v, *rs, *a, *slope, *qs, *ql, *qr, *q[6];
-};
-
-template <typename T>
-__device__ __forceinline__ void ring_vl_iface(const Dims &m, const Geo<T> &g, int j, int k, const T *q,
-                                              const T *v, T dt, T *slope, T *qs) {
-  const int nx = m.nx;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // VanLeerX_a (vanleer_x_a.c:58-70)
-    const int im = i > 0 ? i - 1 : nx - 1, ip = i < nx - 1 ? i + 1 : 0;
-    const T dqm = (q[i] - q[im]) / zsx(m, g, i, j, k);
-    const T dqp = (q[ip] - q[i]) / zsx(m, g, ip, j, k);
-    if (dqp * dqm <= (T)0.0) slope[i] = (T)0.0;
-    else slope[i] = ((T)2. * dqp * dqm) / (dqm + dqp);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // VanLeerX_b (vanleer_x_b.c:59-66)
-    const int im = i > 0 ? i - 1 : nx - 1;
-    if (v[i] > (T)0.0) qs[i] = q[im] + (T)0.5 * (zsx(m, g, im, j, k) - v[i] * dt) * slope[im];
-    else qs[i] = q[i] - (T)0.5 * (zsx(m, g, i, j, k) + v[i] * dt) * slope[i];
-  }
-  __syncthreads();
-}
-
-template <typename T>
-__device__ __forceinline__ void ring_ppa_iface(const Dims &m, const Geo<T> &g, int j, int k, const T *q,
-                                               const T *v, T dt, T *slope, T *ql, T *qr, T *qs) {
-  const int nx = m.nx;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // VanLeerX_PPA_a (fargo_ppa_a.c:58-72)
-    const int im = i > 0 ? i - 1 : nx - 1, ip = i < nx - 1 ? i + 1 : 0;
-    const T dqm = (q[i] - q[im]), dqp = (q[ip] - q[i]);
-    T sl;
-    if (dqp * dqm <= (T)0.0) sl = (T)0.0;
-    else {
-      sl = (T)0.5 * (q[ip] - q[im]);
-      T work = fabs(sl);
-      if ((T)2.0 * fabs(dqm) < work) work = (T)2.0 * fabs(dqm);
-      if ((T)2.0 * fabs(dqp) < work) work = (T)2.0 * fabs(dqp);
-      if (sl < 0) sl = -work;
-      else sl = work;
-    }
-    slope[i] = sl;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // _b (fargo_ppa_b.c:55-62) and _c (fargo_ppa_c.c:53-67)
-    const int im = i > 0 ? i - 1 : nx - 1, ip = i < nx - 1 ? i + 1 : 0;
-    const T qrr = q[i] + (T)0.5 * (q[ip] - q[i]) - (T)(1.0 / 6.0) * (slope[ip] - slope[i]);
-    const T qll = q[im] + (T)0.5 * (q[i] - q[im]) - (T)(1.0 / 6.0) * (slope[i] - slope[im]);
-    T L = qll, R = qrr;
-    const T qq = q[i];
-    if ((R - qq) * (qq - L) < (T)0.0) { L = qq; R = qq; }
-    const T diff = R - L;
-    const T cord = qq - (T)0.5 * (L + R);
-    if ((T)6.0 * diff * cord > diff * diff) L = (T)3.0 * qq - (T)2.0 * R;
-    if (-diff * diff > (T)6.0 * diff * cord) R = (T)3.0 * qq - (T)2.0 * L;
-    ql[i] = L;
-    qr[i] = R;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {  // VanLeerX_PPA_d (fargo_ppa_d.c:58-75)
-    const int im = i > 0 ? i - 1 : nx - 1;
-    T ksi, s;
-    if (v[i] > (T)0.0) {
-      ksi = v[i] * dt / zsx(m, g, i, j, k);
-      s = qr[im] + ksi * (q[im] - qr[im]);
-      s += ksi * ((T)1.0 - ksi) * ((T)2.0 * q[im] - qr[im] - ql[im]);
-    } else {
-      ksi = -v[i] * dt / zsx(m, g, i, j, k);
-      s = ql[i] + ksi * (q[i] - ql[i]);
-      s += ksi * ((T)1.0 - ksi) * ((T)2.0 * q[i] - qr[i] - ql[i]);
-    }
-    qs[i] = s;
-  }
-  __syncthreads();
-}
-
-// UpdateX / UpdateDensityX (update_x.c:68-70, update_density_x.c:66-68)
-template <typename T>
-__device__ __forceinline__ T upd_x(const Geo<T> &g, int i, int ip, int j, int k, T v, T qs, T rs, T vp, T qsp,
-                                   T rsp, T dt, bool dens) {
-  const T fl = dens ? (v * rs - vp * rsp) : (v * qs * rs - vp * qsp * rsp);
-  return fl * ld(g.sxj + j) * ld(g.sxk + k) * dt * ld(g.invvj + j) / (ld(g.syk + k) * ld(g.sxi + i));
-}
-
-template <typename T>
-__device__ void ring_pass(const Dims &m, const Geo<T> &g, int j, int k, RingSmem<T> &S, int nq, T dt, bool ppa) {
-  const int nx = m.nx;
-  // density interface values
-  if (!ppa) ring_vl_iface(m, g, j, k, S.rho, S.v, dt, S.slope, S.rs);
-  else ring_ppa_iface(m, g, j, k, S.rho, S.v, dt, S.slope, S.ql, S.qr, S.rs);
-  for (int q = 0; q < nq; q++) {
-    T *Q = S.q[q];
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) S.a[i] = Q[i] / S.rho[i];  // DivideByRho
-    __syncthreads();
-    if (!ppa) ring_vl_iface(m, g, j, k, S.a, S.v, dt, S.slope, S.qs);
-    else ring_ppa_iface(m, g, j, k, S.a, S.v, dt, S.slope, S.ql, S.qr, S.qs);
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-      const int ip = i < nx - 1 ? i + 1 : 0;
-      Q[i] = Q[i] + upd_x(g, i, ip, j, k, S.v[i], S.qs[i], S.rs[i], S.v[ip], S.qs[ip], S.rs[ip], dt, false);
-    }
-    __syncthreads();
-  }
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    const int ip = i < nx - 1 ? i + 1 : 0;
-    S.a[i] = S.rho[i] + upd_x(g, i, ip, j, k, S.v[i], (T)0, S.rs[i], S.v[ip], (T)0, S.rs[ip], dt, true);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) S.rho[i] = S.a[i];
-  __syncthreads();
-}
-
-template <typename T>
-__device__ __forceinline__ void b_sweep_x(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
-                                                 T *rho, T *q0, T *q1, T *q2, T *q3, T *q4, T *q5,
-                                                 const T *__restrict__ vxt, const double *__restrict__ vxmed_t,
-                                                 int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp, uint3 bid) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *sm = reinterpret_cast<T *>(smem_raw);
-  const int nx = m.nx;
-  const int j = jlo + bid.x, k = m.is3d ? klo + bid.y : 0;
-  RingSmem<T> S;
-  S.rho = sm; S.v = sm + nx; S.rs = sm + 2 * nx; S.a = sm + 3 * nx; S.slope = sm + 4 * nx;
-  S.qs = sm + 5 * nx; S.ql = sm + 6 * nx; S.qr = sm + 7 * nx;
-  for (int q = 0; q < nq; q++) S.q[q] = sm + (8 + q) * nx;
-  T *qg[6] = {q0, q1, q2, q3, q4, q5};
-  const double dtd = scp->dt;
-  const T dt = (T)dtd;
-  const double vm = vxmed_t[j + k * m.sy];
-  const long long lr = m.l(0, j, k);
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    S.rho[i] = rho[lr + i];
-    for (int q = 0; q < nq; q++) S.q[q][i] = qg[q][lr + i];
-    // ComputeResidual (compute_residual.c:68-73): residual velocity
-    S.v[i] = (T)((double)vxt[lr + i] - vm);
-  }
-  __syncthreads();
-  ring_pass(m, g, j, k, S, nq, dt, false);
-  // uniform fractional velocity (ntilde - nround) * dx / dt, in FP64
-  __shared__ int s_nsh;
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    const double zx = (double)zsx(m, gd, i, j, k);
-    const double ntilde = vm * dtd / zx;
-    const double nround = floor(ntilde + 0.5);
-    S.v[i] = (T)((ntilde - nround) * zx / dtd);
-    if (i == 0) {
-      s_nsh = (int)nround;
-      if (nshift_out) nshift_out[j + k * m.sy] = (int)nround;
-    }
-  }
-  __syncthreads();
-  const int nsh = s_nsh;
-  ring_pass(m, g, j, k, S, nq, dt, true);
-  // AdvectSHIFT (advect_shift.c:49-54)
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    int it = i - nsh;
-    it %= nx;
-    if (it < 0) it += nx;
-    rho[lr + i] = S.rho[it];
-    for (int q = 0; q < nq; q++) qg[q][lr + i] = S.q[q][it];
-  }
-}
-template <typename T>
-__global__ void __launch_bounds__(512) k_sweep_x(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
-                                                 T *rho, T *q0, T *q1, T *q2, T *q3, T *q4, T *q5,
-                                                 const T *__restrict__ vxt, const double *__restrict__ vxmed_t,
-                                                 int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp) {
-  b_sweep_x<T>(m, g, gd, nq, jlo, klo, rho, q0, q1, q2, q3, q4, q5, vxt, vxmed_t, nshift_out, scp, blockIdx);
-}
-
-// ---------------------------------------------------------------------------
 // NewVelocity_x/y/z (newvel_x.c:81, newvel_y.c:70, newvel_z.c:66-69) and
 // StockholmBoundary (stockholm.c:129-185) on the active cells; writes the
 // new state (rho, vx, vy, vz).
-template <typename T>
-__device__ __forceinline__ void b_newvel(Dims m, Geo<T> g, const T *__restrict__ rt, const T *__restrict__ mpx,
-                                                const T *__restrict__ mmx, const T *__restrict__ mpy,
-                                                const T *__restrict__ mmy, const T *__restrict__ mpz,
-                                                const T *__restrict__ mmz, T *__restrict__ rho, T *__restrict__ vx,
-                                                T *__restrict__ vy, T *__restrict__ vz, const T *__restrict__ rho0,
-                                                const T *__restrict__ vx0, const T *__restrict__ vy0,
-                                                const T *__restrict__ vz0, const double *__restrict__ ramps,
+template <typename T, typename S = T>
+__device__ __forceinline__ void b_newvel(Dims m, Geo<T> g, const S *__restrict__ rt, const S *__restrict__ mpx,
+                                                const S *__restrict__ mmx, const S *__restrict__ mpy,
+                                                const S *__restrict__ mmy, const S *__restrict__ mpz,
+                                                const S *__restrict__ mmz, S *__restrict__ rho, S *__restrict__ vx,
+                                                S *__restrict__ vy, S *__restrict__ vz, const S *__restrict__ rho0,
+                                                const S *__restrict__ vx0, const S *__restrict__ vy0,
+                                                const S *__restrict__ vz0, const double *__restrict__ ramps,
                                                 int stockholm, const fb_scalars *__restrict__ scp, uint3 bid) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   const int j = FB_NGH + bid.y;
@@ -843,7 +687,9 @@ __device__ __forceinline__ void b_newvel(Dims m, Geo<T> g, const T *__restrict__
   {
     const T rc = m.sph ? ld(g.ymed + j) * ld(g.sin_zmed + k) : ld(g.ymed + j);
     nvx = (mmx[l] * syk * sxi / ivj + mpx[lxm] * syk * sxim / ivj) /
-              ((r * syk * sxi / ivj + rt[lxm] * syk * sxim / ivj) * rc) - of * rc;
+          ((r * syk * sxi / ivj + rt[lxm] * syk * sxim / ivj) * rc);
+    // relative momenta (reduced-precision storage) carry no frame rotation
+    if (!(sizeof(S) < sizeof(T))) nvx -= of * rc;
   }
   {
     const T ivjm = ld(g.invvj + j - 1);
@@ -884,16 +730,16 @@ __device__ __forceinline__ void b_newvel(Dims m, Geo<T> g, const T *__restrict__
   vy[l] = nvy;
   if (m.is3d) vz[l] = nvz;
 }
-template <typename T>
-__global__ void __launch_bounds__(256) k_newvel(Dims m, Geo<T> g, const T *__restrict__ rt, const T *__restrict__ mpx,
-                                                const T *__restrict__ mmx, const T *__restrict__ mpy,
-                                                const T *__restrict__ mmy, const T *__restrict__ mpz,
-                                                const T *__restrict__ mmz, T *__restrict__ rho, T *__restrict__ vx,
-                                                T *__restrict__ vy, T *__restrict__ vz, const T *__restrict__ rho0,
-                                                const T *__restrict__ vx0, const T *__restrict__ vy0,
-                                                const T *__restrict__ vz0, const double *__restrict__ ramps,
+template <typename T, typename S = T>
+__global__ void __launch_bounds__(256) k_newvel(Dims m, Geo<T> g, const S *__restrict__ rt, const S *__restrict__ mpx,
+                                                const S *__restrict__ mmx, const S *__restrict__ mpy,
+                                                const S *__restrict__ mmy, const S *__restrict__ mpz,
+                                                const S *__restrict__ mmz, S *__restrict__ rho, S *__restrict__ vx,
+                                                S *__restrict__ vy, S *__restrict__ vz, const S *__restrict__ rho0,
+                                                const S *__restrict__ vx0, const S *__restrict__ vy0,
+                                                const S *__restrict__ vz0, const double *__restrict__ ramps,
                                                 int stockholm, const fb_scalars *__restrict__ scp) {
-  b_newvel<T>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, rho, vx, vy, vz, rho0, vx0, vy0, vz0, ramps, stockholm, scp, blockIdx);
+  b_newvel<T, S>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, rho, vx, vy, vz, rho0, vx0, vy0, vz0, ramps, stockholm, scp, blockIdx);
 }
 
 }  // namespace fb
@@ -905,10 +751,10 @@ namespace fb {
 // of one colatitude layer, with the inputs of layers k-1..k+1 staged and the
 // six stress components of visctensor_sph (visctensor_sph.c:141-213) computed
 // where addviscosity_sph (addviscosity_sph.c:74-126) reads them.
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, typename S = T>
 __device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
-    const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx, const T *__restrict__ vy,
-    const T *__restrict__ vz, T *__restrict__ vxt, T *__restrict__ vyt, T *__restrict__ vzt,
+    const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx, const S *__restrict__ vy,
+    const S *__restrict__ vz, S *__restrict__ vxt, S *__restrict__ vyt, S *__restrict__ vzt,
     const fb_scalars *__restrict__ scp, int dust, int viscous, uint3 bid) {
   constexpr int W = TX + 2, H = TY + 2;
   __shared__ T s_rho[3][H][W], s_cs[3][H][W], s_vx[3][H][W], s_vy[3][H][W], s_vz[3][H][W];
@@ -1087,12 +933,12 @@ __device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
   vyt[l] = ay;
   vzt[l] = az;
 }
-template <typename T, int TX, int TY>
+template <typename T, int TX, int TY, typename S = T>
 __global__ void __launch_bounds__(TX *TY) k_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
-    const T *__restrict__ rho, const T *__restrict__ cs, const T *__restrict__ vx, const T *__restrict__ vy,
-    const T *__restrict__ vz, T *__restrict__ vxt, T *__restrict__ vyt, T *__restrict__ vzt,
+    const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx, const S *__restrict__ vy,
+    const S *__restrict__ vz, S *__restrict__ vxt, S *__restrict__ vyt, S *__restrict__ vzt,
     const fb_scalars *__restrict__ scp, int dust, int viscous) {
-  b_sources_sph<T, TX, TY>(m, g, gd, rho, cs, vx, vy, vz, vxt, vyt, vzt, scp, dust, viscous, blockIdx);
+  b_sources_sph<T, TX, TY, S>(m, g, gd, rho, cs, vx, vy, vz, vxt, vyt, vzt, scp, dust, viscous, blockIdx);
 }
 
 }  // namespace fb
@@ -1173,10 +1019,10 @@ __device__ __forceinline__ void chunk_iface(const T *w, const T *v, const Z &zon
   }
 }
 
-template <typename T, int C, int NT>
+template <typename T, int C, int NT, typename S = T>
 __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const Geo<double> &gd, int nq, int jlo,
-                                           int klo, int nj, int nrings, T *rho, T *q0, T *q1, T *q2, T *q3, T *q4,
-                                           T *q5, const T *__restrict__ vxt, const double *__restrict__ vxmed_t,
+                                           int klo, int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,
+                                           S *q5, const S *__restrict__ vxt, const double *__restrict__ vxmed_t,
                                            int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp,
                                            uint3 bid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1186,7 +1032,7 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
   const int r = bid.x * rpc + slot;
   const bool active = slot < rpc && r < nrings;
   const int j = jlo + (active ? r % nj : 0), k = m.is3d ? klo + (active ? r / nj : 0) : 0;
-  T *qg[6] = {q0, q1, q2, q3, q4, q5};
+  S *qg[6] = {q0, q1, q2, q3, q4, q5};
   const double dtd = scp->dt;
   const T dt = (T)dtd;
   // shared layout: buffers A and B of [slot][field][nx] (field 0 rho, 1.. the
@@ -1284,13 +1130,13 @@ __host__ __device__ inline int sweep_x_chunk(int nx, int nt) {
   return 0;
 }
 
-template <typename T, int C>
+template <typename T, int C, typename S = T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_sweep_x2(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
-                                                  int nj, int nrings, T *rho, T *q0, T *q1, T *q2, T *q3, T *q4,
-                                                  T *q5, const T *__restrict__ vxt,
+                                                  int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,
+                                                  S *q5, const S *__restrict__ vxt,
                                                   const double *__restrict__ vxmed_t, int *__restrict__ nshift_out,
                                                   const fb_scalars *__restrict__ scp) {
-  b_sweep_x2<T, C, 256>(m, g, gd, nq, jlo, klo, nj, nrings, rho, q0, q1, q2, q3, q4, q5, vxt, vxmed_t, nshift_out,
+  b_sweep_x2<T, C, 256, S>(m, g, gd, nq, jlo, klo, nj, nrings, rho, q0, q1, q2, q3, q4, q5, vxt, vxmed_t, nshift_out,
                         scp, blockIdx);
 }
 

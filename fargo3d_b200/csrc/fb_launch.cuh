@@ -5,141 +5,141 @@
 
 namespace fb {
 
-template <typename T>
-static inline QSrc<T> qsrc_from_v(const fb_fluid_dev &F, T of) {
-  QSrc<T> s;
-  s.rho = (const T *)F.rho; s.vxt = (const T *)F.vxt; s.vyt = (const T *)F.vyt; s.vzt = (const T *)F.vzt;
+template <typename T, typename S>
+static inline QSrc<T, S> qsrc_from_v(const fb_fluid_dev &F, T of) {
+  QSrc<T, S> s;
+  s.rho = (const S *)F.rho; s.vxt = (const S *)F.vxt; s.vyt = (const S *)F.vyt; s.vzt = (const S *)F.vzt;
   for (int q = 0; q < 6; q++) s.q[q] = nullptr;
   s.from_v = 1;
   s.of = of;
   return s;
 }
 
-template <typename T>
+template <typename T, typename S>
 static int launch_rowsum(const fb_disk_dev *d, int f, int which, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
   Geo<double> gd = geo_of<double>(d->geomd);
   const int nring = m.sy * m.sz;
-  const T *v = (const T *)(which == 0 ? F.vx : F.vxt);
+  const S *v = (const S *)(which == 0 ? F.vx : F.vxt);
   double *out = which == 0 ? F.vxmed : F.vxmed_t;
   dim3 grid((nring + 31) / 32);
   if (d->precision == FB_FP64)
-    k_rowsum<T, true><<<grid, 256, 0, st>>>(m, gd, v, out, d->xlen);
+    k_rowsum<T, true, S><<<grid, 256, 0, st>>>(m, gd, v, out, d->xlen);
   else
-    k_rowsum<T, false><<<grid, 256, 0, st>>>(m, gd, v, out, d->xlen);
+    k_rowsum<T, false, S><<<grid, 256, 0, st>>>(m, gd, v, out, d->xlen);
   return (int)cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, typename S>
 static int launch_cfl(const fb_disk_dev *d, int f, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
-  Geo<T> g = geo_of<T>(d->geom);
+  Geo<T> g = geo_of<T>(sizeof(T) == 8 ? d->geomd : d->geom);
   dim3 grid(m.ny, m.is3d ? m.nz : 1);
-  k_cfl<T><<<grid, 256, 0, st>>>(m, g, (const T *)F.rho, (const T *)F.cs, (const T *)F.vx, (const T *)F.vy,
-                                  (const T *)F.vz, F.vxmed, d->scal_dev, d->cfl, d->mindx,
+  k_cfl<T, S><<<grid, 256, 0, st>>>(m, g, (const S *)F.rho, (const S *)F.cs, (const S *)F.vx, (const S *)F.vy,
+                                  (const S *)F.vz, F.vxmed, d->scal_dev, d->cfl, d->mindx,
                                   (unsigned long long *)d->dtmin);
   return (int)cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, typename S>
 static int launch_sources(const fb_disk_dev *d, int f, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
-  Geo<T> g = geo_of<T>(d->geom);
+  Geo<T> g = geo_of<T>(sizeof(T) == 8 ? d->geomd : d->geom);
   Geo<double> gd = geo_of<double>(d->geomd);
   const int viscous = !F.dust;
   if (!m.is3d) {
     constexpr int TX = 32, TY = 8;
     dim3 grid((m.nx + TX - 1) / TX, (m.ny + TY - 1) / TY);
-    k_sources_cyl<T, TX, TY><<<grid, dim3(TX, TY), 0, st>>>(m, g, gd, (const T *)F.rho, (const T *)F.cs,
-        (const T *)F.vx, (const T *)F.vy, (T *)F.vxt, (T *)F.vyt, d->scal_dev, F.dust, viscous);
+    k_sources_cyl<T, TX, TY, S><<<grid, dim3(TX, TY), 0, st>>>(m, g, gd, (const S *)F.rho, (const S *)F.cs,
+        (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, d->scal_dev, F.dust, viscous);
   } else {
     constexpr int TX = 32, TY = 4;
     dim3 grid((m.nx + TX - 1) / TX, (m.ny + TY - 1) / TY, m.nz);
-    k_sources_sph<T, TX, TY><<<grid, dim3(TX, TY), 0, st>>>(m, g, gd, (const T *)F.rho, (const T *)F.cs,
-        (const T *)F.vx, (const T *)F.vy, (const T *)F.vz, (T *)F.vxt, (T *)F.vyt, (T *)F.vzt, d->scal_dev,
+    k_sources_sph<T, TX, TY, S><<<grid, dim3(TX, TY), 0, st>>>(m, g, gd, (const S *)F.rho, (const S *)F.cs,
+        (const S *)F.vx, (const S *)F.vy, (const S *)F.vz, (S *)F.vxt, (S *)F.vyt, (S *)F.vzt, d->scal_dev,
         F.dust, viscous);
   }
   return (int)cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, typename S>
 static int launch_bnd(const fb_disk_dev *d, int f, int vtemp, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
-  Geo<T> g = geo_of<T>(d->geom);
+  Geo<T> g = geo_of<T>(sizeof(T) == 8 ? d->geomd : d->geom);
   BndTab tb{d->bnd_tab, m.sy, m.sz};
-  T *rho = (T *)F.rho;
-  T *vx = (T *)(vtemp ? F.vxt : F.vx), *vy = (T *)(vtemp ? F.vyt : F.vy), *vz = (T *)(vtemp ? F.vzt : F.vz);
+  S *rho = (S *)F.rho;
+  S *vx = (S *)(vtemp ? F.vxt : F.vx), *vy = (S *)(vtemp ? F.vyt : F.vy), *vz = (S *)(vtemp ? F.vzt : F.vz);
   const int bx = 128;
   if (m.is3d) {
     dim3 gz((m.nx + bx - 1) / bx, m.sy, 6);
-    k_bnd_z<T><<<gz, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp);
+    k_bnd_z<T, S><<<gz, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp);
   }
   dim3 gy((m.nx + bx - 1) / bx, 6, m.sz);
-  k_bnd_y<T><<<gy, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp);
+  k_bnd_y<T, S><<<gy, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp);
   return (int)cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, typename S>
 static int launch_sweep_cols(const fb_disk_dev *d, int f, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
-  Geo<T> g = geo_of<T>(d->geom);
+  Geo<T> g = geo_of<T>(sizeof(T) == 8 ? d->geomd : d->geom);
   Geo<double> gd = geo_of<double>(d->geomd);
   constexpr int NS = 8;
   const int bx = 128;
   const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;  // rows 2 .. Ny+2
-  T *rho_out;
-  T *q[6];
+  S *rho_out;
+  S *q[6];
   int nq;
   (void)gd;
   if (!m.is3d) {
     nq = 4;
-    QSrc<T> src = qsrc_from_v<T>(F, (T)0);
-    rho_out = (T *)F.rho_a;
-    q[0] = (T *)F.mpx; q[1] = (T *)F.mmx; q[2] = (T *)F.mpy; q[3] = (T *)F.mmy; q[4] = q[5] = nullptr;
+    QSrc<T, S> src = qsrc_from_v<T, S>(F, (T)0);
+    rho_out = (S *)F.rho_a;
+    q[0] = (S *)F.mpx; q[1] = (S *)F.mmx; q[2] = (S *)F.mpy; q[3] = (S *)F.mmy; q[4] = q[5] = nullptr;
     dim3 grid((m.nx + bx - 1) / bx, 1, (yhi - ylo + NS) / NS);
-    k_sweep_col<T, 0, NS><<<grid, bx, 0, st>>>(m, g, src, nq, ylo, yhi, 0, rho_out, q[0], q[1], q[2], q[3], q[4],
+    k_sweep_col<T, 0, NS, S><<<grid, bx, 0, st>>>(m, g, src, nq, ylo, yhi, 0, rho_out, q[0], q[1], q[2], q[3], q[4],
                                                q[5], d->scal_dev);
   } else {
     nq = 6;
     const int zlo = FB_NGH - 1, zhi = m.nz + FB_NGH - 1;
     // Z sweep from V_temp into set A, rows 0 .. sy-2
-    QSrc<T> src = qsrc_from_v<T>(F, (T)0);
+    QSrc<T, S> src = qsrc_from_v<T, S>(F, (T)0);
     dim3 gz((m.nx + bx - 1) / bx, m.sy - 1, (zhi - zlo + NS) / NS);
-    k_sweep_col<T, 1, NS><<<gz, bx, 0, st>>>(m, g, src, nq, zlo, zhi, 0, (T *)F.rho_a, (T *)F.mpx, (T *)F.mmx,
-                                             (T *)F.mpy, (T *)F.mmy, (T *)F.mpz, (T *)F.mmz, d->scal_dev);
+    k_sweep_col<T, 1, NS, S><<<gz, bx, 0, st>>>(m, g, src, nq, zlo, zhi, 0, (S *)F.rho_a, (S *)F.mpx, (S *)F.mmx,
+                                             (S *)F.mpy, (S *)F.mmy, (S *)F.mpz, (S *)F.mmz, d->scal_dev);
     // Y sweep from set A into set B, layers 2 .. Nz+2
-    QSrc<T> sa;
-    sa.rho = (const T *)F.rho_a; sa.vxt = (const T *)F.vxt; sa.vyt = (const T *)F.vyt; sa.vzt = (const T *)F.vzt;
-    sa.q[0] = (const T *)F.mpx; sa.q[1] = (const T *)F.mmx; sa.q[2] = (const T *)F.mpy;
-    sa.q[3] = (const T *)F.mmy; sa.q[4] = (const T *)F.mpz; sa.q[5] = (const T *)F.mmz;
+    QSrc<T, S> sa;
+    sa.rho = (const S *)F.rho_a; sa.vxt = (const S *)F.vxt; sa.vyt = (const S *)F.vyt; sa.vzt = (const S *)F.vzt;
+    sa.q[0] = (const S *)F.mpx; sa.q[1] = (const S *)F.mmx; sa.q[2] = (const S *)F.mpy;
+    sa.q[3] = (const S *)F.mmy; sa.q[4] = (const S *)F.mpz; sa.q[5] = (const S *)F.mmz;
     sa.from_v = 0; sa.of = (T)0;
     dim3 gy((m.nx + bx - 1) / bx, zhi - zlo + 1, (yhi - ylo + NS) / NS);
-    rho_out = (T *)F.rho_b;
-    q[0] = (T *)F.mpx_b; q[1] = (T *)F.mmx_b; q[2] = (T *)F.mpy_b; q[3] = (T *)F.mmy_b; q[4] = (T *)F.mpz_b;
-    q[5] = (T *)F.mmz_b;
-    k_sweep_col<T, 0, NS><<<gy, bx, 0, st>>>(m, g, sa, nq, ylo, yhi, zlo, rho_out, q[0], q[1], q[2], q[3], q[4],
+    rho_out = (S *)F.rho_b;
+    q[0] = (S *)F.mpx_b; q[1] = (S *)F.mmx_b; q[2] = (S *)F.mpy_b; q[3] = (S *)F.mmy_b; q[4] = (S *)F.mpz_b;
+    q[5] = (S *)F.mmz_b;
+    k_sweep_col<T, 0, NS, S><<<gy, bx, 0, st>>>(m, g, sa, nq, ylo, yhi, zlo, rho_out, q[0], q[1], q[2], q[3], q[4],
                                              q[5], d->scal_dev);
   }
   return (int)cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, typename S>
 static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
-  Geo<T> g = geo_of<T>(d->geom);
+  Geo<T> g = geo_of<T>(sizeof(T) == 8 ? d->geomd : d->geom);
   Geo<double> gd = geo_of<double>(d->geomd);
   const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;
   const bool b = m.is3d;
   const int nq = b ? 6 : 4;
-  T *rho_out = (T *)(b ? F.rho_b : F.rho_a);
-  T *q[6] = {(T *)(b ? F.mpx_b : F.mpx), (T *)(b ? F.mmx_b : F.mmx), (T *)(b ? F.mpy_b : F.mpy),
-             (T *)(b ? F.mmy_b : F.mmy), (T *)(b ? F.mpz_b : F.mpz), (T *)(b ? F.mmz_b : F.mmz)};
+  S *rho_out = (S *)(b ? F.rho_b : F.rho_a);
+  S *q[6] = {(S *)(b ? F.mpx_b : F.mpx), (S *)(b ? F.mmx_b : F.mmx), (S *)(b ? F.mpy_b : F.mpy),
+             (S *)(b ? F.mmy_b : F.mmy), (S *)(b ? F.mpz_b : F.mpz), (S *)(b ? F.mmz_b : F.mmz)};
   // azimuthal sweep: C cells per thread, whole rings per CTA of 256 threads
   const int C = sweep_x_chunk(m.nx, 256);
   if (C == 0) return (int)cudaErrorInvalidValue;
@@ -152,11 +152,11 @@ static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
   {                                                                                                        \
     static size_t conf = 0;                                                                                \
     if (smem > conf) {                                                                                     \
-      cudaFuncSetAttribute(k_sweep_x2<T, CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
+      cudaFuncSetAttribute(k_sweep_x2<T, CC, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
       conf = smem;                                                                                         \
     }                                                                                                      \
-    k_sweep_x2<T, CC><<<gx, 256, smem, st>>>(m, g, gd, nq, ylo, klo, nj, nrings, rho_out, q[0], q[1], q[2], \
-                                             q[3], q[4], q[5], (const T *)F.vxt, F.vxmed_t, F.nshift,      \
+    k_sweep_x2<T, CC, S><<<gx, 256, smem, st>>>(m, g, gd, nq, ylo, klo, nj, nrings, rho_out, q[0], q[1], q[2], \
+                                             q[3], q[4], q[5], (const S *)F.vxt, F.vxmed_t, F.nshift,      \
                                              d->scal_dev);                                                 \
   }
   switch (C) {
@@ -170,21 +170,21 @@ static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, typename S>
 static int launch_newvel(const fb_disk_dev *d, int f, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
-  Geo<T> g = geo_of<T>(d->geom);
+  Geo<T> g = geo_of<T>(sizeof(T) == 8 ? d->geomd : d->geom);
   const bool b = m.is3d;
-  const T *rt = (const T *)(b ? F.rho_b : F.rho_a);
-  const T *mpx = (const T *)(b ? F.mpx_b : F.mpx), *mmx = (const T *)(b ? F.mmx_b : F.mmx);
-  const T *mpy = (const T *)(b ? F.mpy_b : F.mpy), *mmy = (const T *)(b ? F.mmy_b : F.mmy);
-  const T *mpz = (const T *)(b ? F.mpz_b : F.mpz), *mmz = (const T *)(b ? F.mmz_b : F.mmz);
+  const S *rt = (const S *)(b ? F.rho_b : F.rho_a);
+  const S *mpx = (const S *)(b ? F.mpx_b : F.mpx), *mmx = (const S *)(b ? F.mmx_b : F.mmx);
+  const S *mpy = (const S *)(b ? F.mpy_b : F.mpy), *mmy = (const S *)(b ? F.mmy_b : F.mmy);
+  const S *mpz = (const S *)(b ? F.mpz_b : F.mpz), *mmz = (const S *)(b ? F.mmz_b : F.mmz);
   const int bx = 128;
   dim3 grid((m.nx + bx - 1) / bx, m.ny, m.is3d ? m.nz : 1);
-  k_newvel<T><<<grid, bx, 0, st>>>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, (T *)F.rho, (T *)F.vx, (T *)F.vy,
-                                   (T *)F.vz, (const T *)F.rho0, (const T *)F.vx0, (const T *)F.vy0,
-                                   (const T *)F.vz0, d->ramps, d->stockholm, d->scal_dev);
+  k_newvel<T, S><<<grid, bx, 0, st>>>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, (S *)F.rho, (S *)F.vx, (S *)F.vy,
+                                   (S *)F.vz, (const S *)F.rho0, (const S *)F.vx0, (const S *)F.vy0,
+                                   (const S *)F.vz0, d->ramps, d->stockholm, d->scal_dev);
   return (int)cudaGetLastError();
 }
 
@@ -195,24 +195,24 @@ static int launch_newvel(const fb_disk_dev *d, int f, cudaStream_t st) {
 
 extern "C" {
 int FB_CAT(fb_launch_rowsum, FB_SUF)(const fb_disk_dev *d, int fluid, int which, void *s) {
-  return fb::launch_rowsum<FB_REAL>(d, fluid, which, (cudaStream_t)s);
+  return fb::launch_rowsum<FB_REAL, FB_STORE>(d, fluid, which, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_cfl, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_cfl<FB_REAL>(d, fluid, (cudaStream_t)s);
+  return fb::launch_cfl<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_sources, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_sources<FB_REAL>(d, fluid, (cudaStream_t)s);
+  return fb::launch_sources<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_bnd, FB_SUF)(const fb_disk_dev *d, int fluid, int vtemp, void *s) {
-  return fb::launch_bnd<FB_REAL>(d, fluid, vtemp, (cudaStream_t)s);
+  return fb::launch_bnd<FB_REAL, FB_STORE>(d, fluid, vtemp, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_sweep_cols, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_sweep_cols<FB_REAL>(d, fluid, (cudaStream_t)s);
+  return fb::launch_sweep_cols<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_sweep_x, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_sweep_x<FB_REAL>(d, fluid, (cudaStream_t)s);
+  return fb::launch_sweep_x<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_newvel, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_newvel<FB_REAL>(d, fluid, (cudaStream_t)s);
+  return fb::launch_newvel<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 }

@@ -113,3 +113,23 @@ def test_batch_failing_member_is_frozen_others_continue():
         assert np.array_equal(solo.state(0)["rho"], b.state(i)["rho"])
         solo.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_fp32_accuracy_after_1000_steps():
+    """North-star accuracy bar of the FP32 path: relative L1 density error
+    against the FP64 oracle after 1000 hydro steps <= 1e-5 (batched FP32 with
+    fast single-precision division, FP64 shift / means / planets)."""
+    from fargo3d_b200 import Batch, config_fargo2d, Planet
+    cfgs = [config_fargo2d(128, 64, seed=41),
+            config_fargo2d(128, 64, seed=42).replace(alpha_visc=True, alpha=1e-3, nu=0.0,
+                                                     planets=[Planet(1.0, 1e-3)])]
+    b = Batch(cfgs, "fp32")
+    b.load_initial_states()
+    b.run(1000)
+    for i, c in enumerate(cfgs):
+        ref, _ = oracle_run(c, 1000)
+        st = b.state(i)
+        l1 = np.sum(np.abs(st["rho"] - ref["rho"])) / np.sum(np.abs(ref["rho"]))
+        assert l1 <= 1e-5, (i, l1)
+    b.close()
