@@ -16,6 +16,7 @@ Prof *g_prof = nullptr;
 
 extern "C" int fb_batch_launch_step_f64(fb_batch *B, double DT);
 extern "C" int fb_batch_launch_step_f32(fb_batch *B, double DT);
+extern "C" size_t fb_batch_sweep_x_esz_f32(void);
 
 static int launch_step_any(fb_batch *B, double DT) {
   return B->precision == FB_FP64 ? fb_batch_launch_step_f64(B, DT) : fb_batch_launch_step_f32(B, DT);
@@ -95,8 +96,8 @@ int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_ba
   B->smem_x = 0;
   (void)maxnx;
   for (int i = 0; i < n; i++) {
-    /* the sweep keeps its rings in the compute precision (double for both) */
-    size_t s = sweep_x2_smem(hd[i].nx, B->cx, 256, B->is3d ? 6 : 4, sizeof(double));
+    /* the sweep keeps its rings in its compute precision */
+    size_t s = sweep_x2_smem(hd[i].nx, B->cx, 256, B->is3d ? 6 : 4, precision == FB_FP64 ? 8 : fb_batch_sweep_x_esz_f32());
     if (s > B->smem_x) B->smem_x = s;
   }
   *out = B;

@@ -229,9 +229,11 @@ static void pmark(cudaStream_t st, const char *name) {
   g_prof->name[g_prof->n++] = name;
 }
 
-template <typename T, typename S>
+// T: compute type of the CFL and source stages; TC, TX, TN: of the column
+// sweeps, the azimuthal sweep and NewVelocity; S: storage type.
+template <typename T, typename S, typename TC = T, typename TX = T, typename TN = T>
 static int launch_step(fb_batch *B, double DT) {
-  configure_sweep_x<T, S>(B);
+  configure_sweep_x<TX, S>(B);
   cudaStream_t st = B->stream;
   pmark(st, "start");
   const fb_disk_dev *ds = B->d_disks;
@@ -258,20 +260,20 @@ static int launch_step(fb_batch *B, double DT) {
     if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
     else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
     pmark(st, "rowsum_vtemp");
-    if (B->is3d) kb_sweep_col<T, 1, S><<<grid(ST_SWEEP_Z), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Z], f);
-    kb_sweep_col<T, 0, S><<<grid(ST_SWEEP_Y), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Y], f);
+    if (B->is3d) kb_sweep_col<TC, 1, S><<<grid(ST_SWEEP_Z), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Z], f);
+    kb_sweep_col<TC, 0, S><<<grid(ST_SWEEP_Y), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Y], f);
     pmark(st, "sweep_cols");
     switch (B->cx) {
-      case 16: kb_sweep_x<T, 16, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 8: kb_sweep_x<T, 8, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 4: kb_sweep_x<T, 4, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 2: kb_sweep_x<T, 2, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      default: kb_sweep_x<T, 1, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      case 16: kb_sweep_x<TX, 16, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      case 8: kb_sweep_x<TX, 8, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      case 4: kb_sweep_x<TX, 4, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      case 2: kb_sweep_x<TX, 2, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+      default: kb_sweep_x<TX, 1, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
     }
     pmark(st, "sweep_x");
   }
   for (int f = 0; f < nf; f++) {
-    kb_newvel<T, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
+    kb_newvel<TN, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
     pmark(st, "newvel");
     if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 0, 1);
     kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 0, 0);

@@ -19,6 +19,9 @@ typedef struct {
   const void *sin_zmed, *cos_zmed, *sin_zmin, *cos_zmin;
   const void *cos_xmed, *sin_xmed;
   const void *visc_j, *viscm_j, *tau_j;
+  /* frame-rotation radius tables (FP32 path): ymed^2, its row differences,
+     sin^2(zmed) and its layer differences, differenced in double */
+  const void *r2_j, *dr2_j, *s2_k, *ds2_k;
 } fb_geom_dev;
 
 typedef struct {

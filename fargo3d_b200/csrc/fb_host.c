@@ -182,6 +182,8 @@ static int upload_geometry(fb_disk *D) {
   double *t_szmin = malloc(sizeof(double) * (sz + 1)), *t_czmin = malloc(sizeof(double) * (sz + 1));
   double *t_cx = malloc(sizeof(double) * sx), *t_sx = malloc(sizeof(double) * sx);
   double *t_visc = malloc(sizeof(double) * sy), *t_viscm = malloc(sizeof(double) * sy), *t_tau = malloc(sizeof(double) * sy);
+  double *t_r2 = malloc(sizeof(double) * sy), *t_dr2 = malloc(sizeof(double) * sy);
+  double *t_s2 = malloc(sizeof(double) * (sz + 1)), *t_ds2 = malloc(sizeof(double) * (sz + 1));
   for (k = 0; k < sz; k++) { t_szmed[k] = sin(D->zmed[k]); t_czmed[k] = cos(D->zmed[k]); }
   for (k = 0; k < sz + 1; k++) { t_szmin[k] = sin(D->zmin[k]); t_czmin[k] = cos(D->zmin[k]); }
   t_szmed[sz] = t_czmed[sz] = 0.0;
@@ -191,6 +193,15 @@ static int upload_geometry(fb_disk *D) {
     t_viscm[j] = sqrt(D->ymin[j] * D->ymin[j] * D->ymin[j] / (G * MSTAR));
     t_tau[j] = p->tau_damp * sqrt(D->ymed[j] * D->ymed[j] * D->ymed[j] / G / MSTAR); /* stockholm.c:134 */
   }
+  /* R^2 = (r sin(theta))^2 factors of the frame rotation and their
+     neighbour differences, each difference taken in double so that the
+     FP32 sweeps never subtract two large R^2 values themselves */
+  for (j = 0; j < sy; j++) {
+    t_r2[j] = D->ymed[j] * D->ymed[j];
+    t_dr2[j] = j > 0 ? D->ymed[j] * D->ymed[j] - D->ymed[j - 1] * D->ymed[j - 1] : 0.0;
+  }
+  for (k = 0; k < sz + 1; k++) t_s2[k] = t_szmed[k] * t_szmed[k];
+  for (k = 0; k < sz + 1; k++) t_ds2[k] = k > 0 && k < sz ? t_s2[k] - t_s2[k - 1] : 0.0;
   for (pass = 0; pass < 2; pass++) {
     /* pass 0: double tables; pass 1: the disk's precision (skipped in FP64) */
     fb_geom_dev *g = pass == 0 ? &D->d.geomd : &D->d.geom;
@@ -206,12 +217,14 @@ static int upload_geometry(fb_disk *D) {
     UP(sin_zmin, t_szmin, sz + 1); UP(cos_zmin, t_czmin, sz + 1);
     UP(cos_xmed, t_cx, sx); UP(sin_xmed, t_sx, sx);
     UP(visc_j, t_visc, sy); UP(viscm_j, t_viscm, sy); UP(tau_j, t_tau, sy);
+    UP(r2_j, t_r2, sy); UP(dr2_j, t_dr2, sy); UP(s2_k, t_s2, sz + 1); UP(ds2_k, t_ds2, sz + 1);
 #undef UP
   }
   rc = FB_OK;
 out:
   free(t_szmed); free(t_czmed); free(t_szmin); free(t_czmin); free(t_cx); free(t_sx);
   free(t_visc); free(t_viscm); free(t_tau);
+  free(t_r2); free(t_dr2); free(t_s2); free(t_ds2);
   return rc;
 }
 

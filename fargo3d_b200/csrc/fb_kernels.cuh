@@ -34,6 +34,7 @@ struct Geo {
   const T *sin_zmed, *cos_zmed, *sin_zmin, *cos_zmin;
   const T *cos_xmed, *sin_xmed;
   const T *visc_j, *viscm_j, *tau_j;
+  const T *r2_j, *dr2_j, *s2_k, *ds2_k;
 };
 
 template <typename T>
@@ -49,6 +50,7 @@ __host__ __device__ inline Geo<T> geo_of(const fb_geom_dev &g) {
   o.sin_zmin = (const T *)g.sin_zmin; o.cos_zmin = (const T *)g.cos_zmin;
   o.cos_xmed = (const T *)g.cos_xmed; o.sin_xmed = (const T *)g.sin_xmed;
   o.visc_j = (const T *)g.visc_j; o.viscm_j = (const T *)g.viscm_j; o.tau_j = (const T *)g.tau_j;
+  o.r2_j = (const T *)g.r2_j; o.dr2_j = (const T *)g.dr2_j; o.s2_k = (const T *)g.s2_k; o.ds2_k = (const T *)g.ds2_k;
   return o;
 }
 
@@ -503,16 +505,22 @@ struct ColGeo {
   }
 };
 
-template <typename T, int DIR, int NS>
+template <typename T, int DIR, int NS, bool OFF = false>
 __device__ __forceinline__ void col_sweep_q(const ColGeo<T, DIR> &cg, int c0, const T *a, const T *vel,
-                                            const T *rs, T dt, T *qs) {
-  // a: NS+4 cell values (c0-2 .. c0+NS+1); vel: NS+1 faces (c0 .. c0+NS)
+                                            const T *off, T dt, T *qs) {
+  // a: NS+4 cell values (c0-2 .. c0+NS+1); vel: NS+1 faces (c0 .. c0+NS).
+  // OFF: a holds the quantity less a cell-dependent offset whose neighbour
+  // differences are off[w] = offset(a[w+1]) - offset(a[w]); the limiter sees
+  // the differences of the full quantity and qs[] comes back less the offset
+  // of its upwind cell.
   T slope[NS + 2];
 #pragma unroll
   for (int s = 0; s < NS + 2; s++) {
     const int c = c0 - 1 + s;
-    const T dqm = (a[s + 1] - a[s]) / cg.zone(c);
-    const T dqp = (a[s + 2] - a[s + 1]) / cg.zone(c + 1);
+    T dqm = a[s + 1] - a[s], dqp = a[s + 2] - a[s + 1];
+    if (OFF) { dqm += off[s]; dqp += off[s + 1]; }
+    dqm /= cg.zone(c);
+    dqp /= cg.zone(c + 1);
     if (dqp * dqm <= 0) slope[s] = 0;
     else slope[s] = (T)2. * dqp * dqm / (dqm + dqp);
   }
@@ -525,7 +533,7 @@ __device__ __forceinline__ void col_sweep_q(const ColGeo<T, DIR> &cg, int c0, co
     else
       qs[f] = a[f + 2] - (T)0.5 * (cg.zone(c) + v * dt) * slope[f + 1];
   }
-  (void)rs;
+  (void)off;
 }
 
 // Quantity sources: 2D Y sweep and 3D Z sweep build the momenta from rho and
@@ -539,7 +547,9 @@ struct QSrc {
   T of;
 };
 
-template <typename T, typename S>
+// REL: the azimuthal momenta relative to the frame's rotation (the
+// OMEGAFRAME * R term of momenta_x.c:77-78 left out).
+template <typename T, typename S, bool REL = false>
 __device__ __forceinline__ T momentum(const Dims &m, const Geo<T> &g, const QSrc<T, S> &src, int q, int i, int j,
                                       int k, long long l, T r) {
   if (!src.from_v) return src.q[q][l];
@@ -548,9 +558,11 @@ __device__ __forceinline__ T momentum(const Dims &m, const Geo<T> &g, const QSrc
       const long long lx = (q == 0) ? ((i < m.nx - 1) ? l + 1 : l - (m.nx - 1)) : l;
       if (!m.sph) {
         const T y = ld(g.ymed + j);
+        if (REL) return src.vxt[lx] * y * r;
         return (src.vxt[lx] + y * src.of) * y * r;
       }
       const T rc = ld(g.ymed + j) * ld(g.sin_zmed + k);
+      if (REL) return src.vxt[lx] * rc * r;
       return (src.vxt[lx] + rc * src.of) * rc * r;
     }
     case 2: return src.vyt[l + m.pitch] * r;  // Mpy
@@ -595,13 +607,18 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, in
 #pragma unroll
   for (int f = 0; f < NS + 1; f++) vel[f] = vface[cidx(min(c0 + f, cmax - 1))];
   // density interface values (VanLeer*_a/_b on Density -> DensStar)
-  col_sweep_q<T, DIR, NS>(cg, c0, r, vel, rs, dt, rs);
-  // With reduced-precision storage (S narrower than T) the azimuthal
-  // momenta live in the buffers relative to the frame's rotation,
-  // Mrel = M - OMEGAFRAME * R^2 * rho (R the cylindrical radius): the stored
-  // numbers are then of the size of the residual velocity, so their rounding
-  // is too.  The sweep itself runs on M = Mrel + OMEGAFRAME R^2 rho in T.
-  constexpr bool REL = sizeof(S) < sizeof(T);
+  col_sweep_q<T, DIR, NS>(cg, c0, r, vel, nullptr, dt, rs);
+  // With FP32 storage the azimuthal momenta live in the buffers relative to
+  // the frame's rotation, Mrel = M - OMEGAFRAME * R^2 * rho (R the
+  // cylindrical radius), so that the stored numbers and their rounding are of
+  // the size of the residual velocity.  The sweep then transports Mrel
+  // directly: the limiter sees the differences of the full specific momentum
+  // (a_rel differences plus OMEGAFRAME times the tabulated R^2 differences),
+  // and a face flux carries OMEGAFRAME (R^2_upwind - R^2_cell) times the
+  // density flux, which is M's flux less OMEGAFRAME R^2_cell times rho's.
+  // No large momentum is formed and then cancelled, so the update loses no
+  // digits in FP32 arithmetic.
+  constexpr bool REL = sizeof(S) == 4;
   T rnew[NS];
 #pragma unroll
   for (int u = 0; u < NS; u++) {
@@ -609,9 +626,11 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, in
     const T flux = cg.surf(vel[u] * rs[u], c) - cg.surf(vel[u + 1] * rs[u + 1], c + 1);
     rnew[u] = r[u + 2] + cg.finish(flux, dt, c);
   }
-  auto rc2 = [&](int jj, int kk) -> T {  // cylindrical radius squared times OMEGAFRAME
-    const T rr = m.sph ? ld(g.ymed + jj) * ld(g.sin_zmed + kk) : ld(g.ymed + jj);
-    return src.of * rr * rr;
+  // OMEGAFRAME * (R^2(c) - R^2(c-1))
+  auto dr2 = [&](int c) -> T {
+    if (!m.sph) return src.of * ld(g.dr2_j + c);
+    if (DIR == 0) return src.of * (ld(g.dr2_j + c) * ld(g.s2_k + k));
+    return src.of * (ld(g.r2_j + j) * ld(g.ds2_k + c));
   };
   S *qo[6] = {q_out0, q_out1, q_out2, q_out3, q_out4, q_out5};
 #pragma unroll
@@ -622,22 +641,31 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, in
     for (int w = 0; w < NS + 4; w++) {
       const int c = min(c0 - 2 + w, cmax);
       const int jj = (DIR == 0) ? c : j, kk = (DIR == 0) ? k : c;
-      qv[w] = momentum(m, g, src, q, i, jj, kk, cidx(c), r[w]);
-      if (REL && q < 2 && !src.from_v) qv[w] += rc2(jj, kk) * r[w];
+      qv[w] = momentum<T, S, REL>(m, g, src, q, i, jj, kk, cidx(c), r[w]);
       a[w] = qv[w] / r[w];
     }
-    col_sweep_q<T, DIR, NS>(cg, c0, a, vel, rs, dt, qs);
+    if (REL && q < 2) {
+      T off[NS + 3];
+#pragma unroll
+      for (int w = 0; w < NS + 3; w++) {
+        const int c = c0 - 1 + w;   // the cell of a[w + 1]
+        off[w] = c <= cmax ? dr2(c) : (T)0;
+      }
+      col_sweep_q<T, DIR, NS, true>(cg, c0, a, vel, off, dt, qs);
+    } else {
+      col_sweep_q<T, DIR, NS>(cg, c0, a, vel, nullptr, dt, qs);
+    }
 #pragma unroll
     for (int u = 0; u < NS; u++) {
       const int c = c0 + u;
       if (c <= chi) {
-        const T flux = cg.surf(vel[u] * qs[u] * rs[u], c) - cg.surf(vel[u + 1] * qs[u + 1] * rs[u + 1], c + 1);
-        T out = qv[u + 2] + cg.finish(flux, dt, c);
+        T qin = qs[u], qout = qs[u + 1];
         if (REL && q < 2) {
-          const int jj = (DIR == 0) ? c : j, kk = (DIR == 0) ? k : c;
-          out -= rc2(jj, kk) * rnew[u];
+          if (vel[u] > (T)0.) qin -= dr2(c);              // upwind cell c-1
+          if (!(vel[u + 1] > (T)0.)) qout += dr2(c + 1);  // upwind cell c+1
         }
-        qo[q][cidx(c)] = out;
+        const T flux = cg.surf(vel[u] * qin * rs[u], c) - cg.surf(vel[u + 1] * qout * rs[u + 1], c + 1);
+        qo[q][cidx(c)] = qv[u + 2] + cg.finish(flux, dt, c);
       }
     }
   }
@@ -664,6 +692,17 @@ namespace fb {
 // NewVelocity_x/y/z (newvel_x.c:81, newvel_y.c:70, newvel_z.c:66-69) and
 // StockholmBoundary (stockholm.c:129-185) on the active cells; writes the
 // new state (rho, vx, vy, vz).
+// Correctly rounded division in either precision (IEEE division even where
+// the FP32 build approximates '/').
+__device__ __forceinline__ float div_rn(float a, float b) {
+#ifdef FB_NV_FASTDIV
+  return a / b;
+#else
+  return __fdiv_rn(a, b);
+#endif
+}
+__device__ __forceinline__ double div_rn(double a, double b) { return a / b; }
+
 template <typename T, typename S = T>
 __device__ __forceinline__ void b_newvel(Dims m, Geo<T> g, const S *__restrict__ rt, const S *__restrict__ mpx,
                                                 const S *__restrict__ mmx, const S *__restrict__ mpy,
@@ -684,23 +723,41 @@ __device__ __forceinline__ void b_newvel(Dims m, Geo<T> g, const S *__restrict__
   const T syk = ld(g.syk + k), sxi = ld(g.sxi + i), sxim = ld(g.sxi + im), ivj = ld(g.invvj + j);
   const T r = rt[l];
   T nvx, nvy, nvz = 0;
-  {
+  if (sizeof(S) == 4) {
+    // FP32 storage: the same averages with the factors common to numerator
+    // and denominator (Syk, InvVj) cancelled, one correctly rounded division
+    // per component (a biased division would add the same error to a cell
+    // step after step); the azimuthal momenta are frame-relative, so the
+    // OMEGAFRAME * R term is not subtracted.
     const T rc = m.sph ? ld(g.ymed + j) * ld(g.sin_zmed + k) : ld(g.ymed + j);
-    nvx = (mmx[l] * syk * sxi / ivj + mpx[lxm] * syk * sxim / ivj) /
-          ((r * syk * sxi / ivj + rt[lxm] * syk * sxim / ivj) * rc);
-    // relative momenta (reduced-precision storage) carry no frame rotation
-    if (!(sizeof(S) < sizeof(T))) nvx -= of * rc;
-  }
-  {
+    nvx = div_rn((T)mmx[l] * sxi + (T)mpx[lxm] * sxim, (r * sxi + (T)rt[lxm] * sxim) * rc);
     const T ivjm = ld(g.invvj + j - 1);
     const long long lym = l - m.pitch;
-    nvy = (mmy[l] * syk * sxi / ivj + mpy[lym] * syk * sxi / ivjm) / (r * syk * sxi / ivj + rt[lym] * syk * sxi / ivjm);
-  }
-  if (m.is3d) {
-    const T sykm = ld(g.syk + k - 1);
-    const long long lzm = l - m.stride;
-    nvz = (mmz[l] * syk * sxi / ivj + mpz[lzm] * sykm * sxi / ivj) / (r * syk * sxi / ivj + rt[lzm] * sykm * sxi / ivj);
-    if (m.sph) nvz /= ld(g.ymed + j);
+    nvy = div_rn((T)mmy[l] * ivjm + (T)mpy[lym] * ivj, r * ivjm + (T)rt[lym] * ivj);
+    if (m.is3d) {
+      const T sykm = ld(g.syk + k - 1);
+      const long long lzm = l - m.stride;
+      nvz = div_rn((T)mmz[l] * syk + (T)mpz[lzm] * sykm, r * syk + (T)rt[lzm] * sykm);
+      if (m.sph) nvz = div_rn(nvz, ld(g.ymed + j));
+    }
+  } else {
+    {
+      const T rc = m.sph ? ld(g.ymed + j) * ld(g.sin_zmed + k) : ld(g.ymed + j);
+      nvx = (mmx[l] * syk * sxi / ivj + mpx[lxm] * syk * sxim / ivj) /
+            ((r * syk * sxi / ivj + rt[lxm] * syk * sxim / ivj) * rc);
+      nvx -= of * rc;
+    }
+    {
+      const T ivjm = ld(g.invvj + j - 1);
+      const long long lym = l - m.pitch;
+      nvy = (mmy[l] * syk * sxi / ivj + mpy[lym] * syk * sxi / ivjm) / (r * syk * sxi / ivj + rt[lym] * syk * sxi / ivjm);
+    }
+    if (m.is3d) {
+      const T sykm = ld(g.syk + k - 1);
+      const long long lzm = l - m.stride;
+      nvz = (mmz[l] * syk * sxi / ivj + mpz[lzm] * sykm * sxi / ivj) / (r * syk * sxi / ivj + rt[lzm] * sykm * sxi / ivj);
+      if (m.sph) nvz /= ld(g.ymed + j);
+    }
   }
   T nr = r;
   if (stockholm) {

@@ -207,12 +207,12 @@ int FB_CAT(fb_launch_bnd, FB_SUF)(const fb_disk_dev *d, int fluid, int vtemp, vo
   return fb::launch_bnd<FB_REAL, FB_STORE>(d, fluid, vtemp, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_sweep_cols, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_sweep_cols<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
+  return fb::launch_sweep_cols<FB_REAL_TR, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_sweep_x, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_sweep_x<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
+  return fb::launch_sweep_x<FB_REAL_TR, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_newvel, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_newvel<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
+  return fb::launch_newvel<FB_REAL_TR, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 }
