@@ -8,7 +8,8 @@ from .setups import (DiskConfig, Planet, config_batched, config_fargo2d, config_
                      initial_state)
 from .disk import Disk
 from .batch import Batch
+from .serving import Server, serving_requests
 from ._abi import FargoError
 
 __all__ = ["DiskConfig", "Planet", "config_batched", "config_fargo2d", "config_p3disof", "initial_state",
-           "geometry", "Disk", "Batch", "FargoError"]
+           "geometry", "Disk", "Batch", "Server", "serving_requests", "FargoError"]

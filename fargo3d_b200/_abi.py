@@ -13,6 +13,8 @@ FB_FP64, FB_FP32 = 0, 1
 FB_OK = 0
 ERRORS = {-1: "FB_ERR_ARG", -2: "FB_ERR_CUDA", -3: "FB_ERR_NULL_DT", -4: "FB_ERR_NONFINITE",
           -5: "FB_ERR_NOMEM", -6: "FB_ERR_TOO_LARGE"}
+FB_DONE, FB_SLOT_EMPTY, FB_SLOT_RESERVED = 1, 2, 3
+FB_REQ_QUEUED, FB_REQ_RUNNING, FB_REQ_DONE, FB_REQ_FAILED = 0, 1, 2, 3
 
 
 class FbParams(C.Structure):
@@ -87,6 +89,8 @@ def lib():
     L.fb_disk_device_fields.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]
     L.fb_disk_stream.restype = C.c_void_p
     L.fb_disk_stream.argtypes = [C.c_void_p]
+    L.fb_params_bytes.argtypes = [C.POINTER(FbParams), C.c_int, C.POINTER(C.c_size_t)]
+    L.fb_disk_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
     _lib = L
     return L
 
@@ -116,5 +120,37 @@ def bind_batch(L):
     L.fb_batch_stream.restype = C.c_void_p
     L.fb_batch_stream.argtypes = [C.c_void_p]
     L.fb_batch_profile_step.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.c_int]
+    L.fb_batch_create_slots.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    L.fb_batch_add.argtypes = [C.c_void_p, C.POINTER(FbParams), C.c_double, C.POINTER(C.c_int)]
+    L.fb_batch_activate.argtypes = [C.c_void_p, C.c_int]
+    L.fb_batch_remove.argtypes = [C.c_void_p, C.c_int]
+    L.fb_batch_capacity.argtypes = [C.c_void_p]
+    L.fb_batch_poll.argtypes = [C.c_void_p, C.POINTER(C.c_int), _D, C.POINTER(C.c_longlong)]
     L._batch_bound = True
     return L
+
+
+def bind_server(L):
+    if getattr(L, "_server_bound", False):
+        return L
+    bind_batch(L)
+    L.fb_server_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    L.fb_server_submit.argtypes = [C.c_void_p, C.POINTER(FbParams), _D, _D, _D, _D, _D, C.c_double,
+                                   C.POINTER(C.c_longlong)]
+    L.fb_server_status.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(C.c_int)]
+    L.fb_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double, C.POINTER(C.c_int)]
+    L.fb_server_fetch.argtypes = [C.c_void_p, C.c_longlong, _D, _D, _D, _D, _D]
+    L.fb_server_stats.argtypes = [C.c_void_p, _D]
+    L.fb_server_clock.argtypes = [C.c_void_p]
+    L.fb_server_clock.restype = C.c_double
+    L.fb_server_destroy.argtypes = [C.c_void_p]
+    L._server_bound = True
+    return L
+
+
+def params_bytes(cfg, precision: str) -> int:
+    """Upper bound of the device bytes one disk of this configuration takes."""
+    out = C.c_size_t()
+    p = params_of(cfg)
+    check(lib().fb_params_bytes(C.byref(p), FB_FP64 if precision == "fp64" else FB_FP32, C.byref(out)))
+    return out.value

@@ -75,7 +75,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             sys.stdout.write(out)
         objs.append(obj)
-    _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lm"])
+    _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lm", "-lpthread"])
     return LIB
 
 

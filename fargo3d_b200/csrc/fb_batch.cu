@@ -10,7 +10,15 @@
 // A disk whose state goes non-finite or whose time step collapses is frozen
 // (its tiles return immediately) while the others continue.  The stage
 // kernels are compiled per precision (fb_batch_f64.cu, fb_batch_f32.cu).
+//
+// Membership is by slots: a disk is added to a free slot, activated (state
+// uploaded, initialised), and removed when its caller is done with it.  The
+// device descriptor array and the per-disk planet systems are indexed by slot;
+// the work lists (the azimuthal sweep has one per chunk width) and the graph
+// depend on the active set and are rebuilt lazily at the next run.
 #include "fb_batch.cuh"
+
+#include <stdio.h>
 
 Prof *g_prof = nullptr;
 
@@ -20,6 +28,45 @@ extern "C" size_t fb_batch_sweep_x_esz_f32(void);
 
 static int launch_step_any(fb_batch *B, double DT) {
   return B->precision == FB_FP64 ? fb_batch_launch_step_f64(B, DT) : fb_batch_launch_step_f32(B, DT);
+}
+
+// Work lists, chunk width and shared-memory size for the active set; drops
+// the captured graph.
+static int rebuild(fb_batch *B) {
+  if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
+  B->graph_steps = 0;
+  for (int s = 0; s < ST_N; s++) {
+    if (B->items[s]) cudaFree(B->items[s]);
+    B->items[s] = nullptr;
+    B->nitems[s] = 0;
+  }
+  std::vector<const fb_disk_dev *> act;
+  for (int i = 0; i < B->n; i++)
+    if (B->state[i] == 2) act.push_back(fb_disk_internal_dev(B->disks[i]));
+  B->dirty = 0;
+  if (act.empty()) return FB_OK;
+  // per chunk-width class: the largest shared-memory need of its disks
+  for (int k = 0; k < NXC; k++) B->smem_x[k] = 0;
+  for (const fb_disk_dev *d : act) {
+    const int c = sweep_x_chunk(d->nx, 256);
+    if (c < 1) return FB_ERR_ARG;
+    int k = 0;
+    while ((1 << k) < c) k++;
+    // the sweep keeps its rings in its compute precision
+    size_t s = sweep_x2_smem(d->nx, c, 256, B->is3d ? 6 : 4,
+                             B->precision == FB_FP64 ? 8 : fb_batch_sweep_x_esz_f32());
+    if (s > B->smem_x[k]) B->smem_x[k] = s;
+  }
+  for (int s = 0; s < ST_N; s++) {
+    std::vector<int4> v;
+    B->nitems[s] = tiles(B, s, v);
+    if (B->nitems[s] > 0) {
+      if (cudaMalloc(&B->items[s], sizeof(int4) * v.size()) != cudaSuccess) return FB_ERR_NOMEM;
+      if (cudaMemcpy(B->items[s], v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return FB_ERR_CUDA;
+    }
+  }
+  return FB_OK;
 }
 
 extern "C" {
@@ -33,104 +80,142 @@ int fb_batch_destroy(fb_batch *B) {
     if (B->items[s]) cudaFree(B->items[s]);
   if (B->d_disks) cudaFree(B->d_disks);
   if (B->d_psys) cudaFree(B->d_psys);
-  for (fb_disk *d : B->disks) fb_disk_destroy(d);
+  for (fb_disk *d : B->disks)
+    if (d) fb_disk_destroy(d);
   if (B->stream) cudaStreamDestroy(B->stream);
   delete B;
   return FB_OK;
 }
 
-int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_batch **out) {
+int fb_batch_create_slots(int capacity, int precision, int device, int is3d, int nfluids, fb_batch **out) {
+  if (!out) return FB_ERR_ARG;
   *out = nullptr;
-  if (!ps || n < 1) return FB_ERR_ARG;
+  if (capacity < 1 || nfluids < 1 || nfluids > FB_MAXFLUIDS || (precision != FB_FP64 && precision != FB_FP32))
+    return FB_ERR_ARG;
   fb_batch *B = new fb_batch();
-  B->n = n; B->precision = precision; B->device = device;
-  B->is3d = ps[0].nz > 1;
-  B->nfluids = ps[0].nfluids;
-  for (int i = 0; i < n; i++) {
-    if ((ps[i].nz > 1) != B->is3d || ps[i].nfluids != B->nfluids) { fb_batch_destroy(B); return FB_ERR_ARG; }
-    fb_disk *d = nullptr;
-    int rc = fb_disk_create(&ps[i], precision, device, &d);
-    if (rc) { fb_batch_destroy(B); return rc; }
-    B->disks.push_back(d);
-  }
+  B->n = capacity; B->precision = precision; B->device = device;
+  B->is3d = is3d ? 1 : 0;
+  B->nfluids = nfluids;
+  B->state.assign(capacity, 0);
+  B->t_end.assign(capacity, 0.0);
+  B->disks.assign(capacity, nullptr);
   if (cudaSetDevice(device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess) {
     fb_batch_destroy(B);
     return FB_ERR_CUDA;
   }
-  std::vector<fb_disk_dev> hd(n);
-  std::vector<fb_psys> hp(n);
-  int maxnx = 0;
-  for (int i = 0; i < n; i++) {
-    hd[i] = *fb_disk_internal_dev(B->disks[i]);
-    hp[i] = *fb_disk_internal_psys(B->disks[i]);
-    if (hd[i].nx > maxnx) maxnx = hd[i].nx;
-  }
-  if (cudaMalloc(&B->d_disks, sizeof(fb_disk_dev) * n) != cudaSuccess ||
-      cudaMalloc(&B->d_psys, sizeof(fb_psys) * n) != cudaSuccess) {
+  if (cudaMalloc(&B->d_disks, sizeof(fb_disk_dev) * capacity) != cudaSuccess ||
+      cudaMalloc(&B->d_psys, sizeof(fb_psys) * capacity) != cudaSuccess) {
     fb_batch_destroy(B);
     return FB_ERR_NOMEM;
   }
-  cudaMemcpy(B->d_disks, hd.data(), sizeof(fb_disk_dev) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(B->d_psys, hp.data(), sizeof(fb_psys) * n, cudaMemcpyHostToDevice);
-  // one chunk width for the whole batch: the first of 4, 8, 16, 2, 1 that
-  // every ring fits
-  {
-    const int cs[5] = {4, 8, 16, 2, 1};
-    B->cx = 0;
-    for (int t = 0; t < 5 && !B->cx; t++) {
-      bool ok = true;
-      for (int i = 0; i < n; i++) ok = ok && hd[i].nx % cs[t] == 0 && hd[i].nx / cs[t] <= 256;
-      if (ok) B->cx = cs[t];
-    }
-    if (!B->cx) { fb_batch_destroy(B); return FB_ERR_ARG; }
-  }
-  for (int s = 0; s < ST_N; s++) {
-    std::vector<int4> v;
-    B->nitems[s] = tiles(B, s, v);
-    if (B->nitems[s] > 0) {
-      if (cudaMalloc(&B->items[s], sizeof(int4) * v.size()) != cudaSuccess) { fb_batch_destroy(B); return FB_ERR_NOMEM; }
-      cudaMemcpy(B->items[s], v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice);
-    }
-  }
-  B->smem_x = 0;
-  (void)maxnx;
+  // zeroed descriptors mark empty slots for the scalar kernel
+  cudaMemset(B->d_disks, 0, sizeof(fb_disk_dev) * capacity);
+  cudaMemset(B->d_psys, 0, sizeof(fb_psys) * capacity);
+  *out = B;
+  return FB_OK;
+}
+
+int fb_batch_add(fb_batch *B, const fb_params *p, double t_end, int *slot) {
+  if (!B || !p || !slot) return FB_ERR_ARG;
+  if ((p->nz > 1) != (B->is3d != 0) || p->nfluids != B->nfluids) return FB_ERR_ARG;
+  int s = -1;
+  for (int i = 0; i < B->n && s < 0; i++)
+    if (B->state[i] == 0) s = i;
+  if (s < 0) return FB_ERR_TOO_LARGE;
+  fb_disk *d = nullptr;
+  int rc = fb_disk_create(p, B->precision, B->device, &d);
+  if (rc) return rc;
+  B->disks[s] = d;
+  B->state[s] = 1;
+  B->t_end[s] = t_end > 0.0 ? t_end : 0.0;
+  *slot = s;
+  return FB_OK;
+}
+
+int fb_batch_activate(fb_batch *B, int s) {
+  if (!B || s < 0 || s >= B->n || B->state[s] != 1) return FB_ERR_ARG;
+  fb_disk *d = B->disks[s];
+  int rc = fb_disk_initialize(d);
+  if (rc) return rc;
+  if (cudaSetDevice(B->device) != cudaSuccess) return FB_ERR_CUDA;
+  // CFL minimum start and flag word; the scalars were uploaded by
+  // fb_disk_initialize
+  unsigned long long init[2] = {0x4415AF1D78B58C40ULL, 0ull};
+  fb_psys ps = *fb_disk_internal_psys(d);
+  ps.t_end = B->t_end[s];
+  const fb_disk_dev *dd = fb_disk_internal_dev(d);
+  // the batch's stream may still be running other members: order the
+  // uploads on it
+  if (cudaMemcpyAsync(dd->dtmin, init, sizeof init, cudaMemcpyHostToDevice, B->stream) != cudaSuccess ||
+      cudaMemcpyAsync(B->d_psys + s, &ps, sizeof ps, cudaMemcpyHostToDevice, B->stream) != cudaSuccess ||
+      cudaMemcpyAsync(B->d_disks + s, dd, sizeof(fb_disk_dev), cudaMemcpyHostToDevice, B->stream) != cudaSuccess ||
+      cudaStreamSynchronize(B->stream) != cudaSuccess)
+    return FB_ERR_CUDA;
+  B->state[s] = 2;
+  B->dirty = 1;
+  return FB_OK;
+}
+
+int fb_batch_remove(fb_batch *B, int s) {
+  if (!B || s < 0 || s >= B->n || B->state[s] == 0) return FB_ERR_ARG;
+  cudaSetDevice(B->device);
+  if (cudaStreamSynchronize(B->stream) != cudaSuccess) return FB_ERR_CUDA;
+  if (cudaMemset(B->d_disks + s, 0, sizeof(fb_disk_dev)) != cudaSuccess) return FB_ERR_CUDA;
+  if (B->state[s] == 2) B->dirty = 1;
+  fb_disk_destroy(B->disks[s]);
+  B->disks[s] = nullptr;
+  B->state[s] = 0;
+  B->t_end[s] = 0.0;
+  return FB_OK;
+}
+
+int fb_batch_capacity(fb_batch *B) { return B ? B->n : 0; }
+
+// All members at once (the original interface): slots 0..n-1 in order.
+int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_batch **out) {
+  if (!out) return FB_ERR_ARG;
+  *out = nullptr;
+  if (!ps || n < 1) return FB_ERR_ARG;
+  fb_batch *B = nullptr;
+  int rc = fb_batch_create_slots(n, precision, device, ps[0].nz > 1, ps[0].nfluids, &B);
+  if (rc) return rc;
   for (int i = 0; i < n; i++) {
-    /* the sweep keeps its rings in its compute precision */
-    size_t s = sweep_x2_smem(hd[i].nx, B->cx, 256, B->is3d ? 6 : 4, precision == FB_FP64 ? 8 : fb_batch_sweep_x_esz_f32());
-    if (s > B->smem_x) B->smem_x = s;
+    int s;
+    rc = fb_batch_add(B, &ps[i], 0.0, &s);
+    if (rc) { fb_batch_destroy(B); return rc; }
   }
   *out = B;
   return FB_OK;
 }
 
 int fb_batch_disk(fb_batch *B, int i, fb_disk **d) {
-  if (!B || i < 0 || i >= B->n) return FB_ERR_ARG;
+  if (!B || !d || i < 0 || i >= B->n || !B->disks[i]) return FB_ERR_ARG;
   *d = B->disks[i];
   return FB_OK;
 }
 
+// Activate every reserved slot (the members' states set beforehand).
 int fb_batch_initialize(fb_batch *B) {
   if (!B) return FB_ERR_ARG;
-  for (fb_disk *d : B->disks) {
-    int rc = fb_disk_initialize(d);
+  for (int i = 0; i < B->n; i++) {
+    if (B->state[i] != 1) continue;
+    int rc = fb_batch_activate(B, i);
     if (rc) return rc;
-  }
-  // scalars uploaded by fb_disk_initialize; start the CFL minimum and flags
-  cudaSetDevice(B->device);
-  for (fb_disk *d : B->disks) {
-    unsigned long long init[2] = {0x4415AF1D78B58C40ULL, 0ull};
-    if (cudaMemcpy(fb_disk_internal_dev(d)->dtmin, init, sizeof init, cudaMemcpyHostToDevice) != cudaSuccess)
-      return FB_ERR_CUDA;
   }
   return FB_OK;
 }
 
-// Advance every disk by nsteps hydro steps without host round trips.  The
-// steps are issued through one captured CUDA graph of `chunk` steps.
+// Advance every active disk by nsteps hydro steps without host round trips.
+// The steps are issued through one captured CUDA graph of `chunk` steps.
 int fb_batch_run(fb_batch *B, int nsteps, double DT) {
   if (!B || nsteps < 0) return FB_ERR_ARG;
   if (cudaSetDevice(B->device) != cudaSuccess) return FB_ERR_CUDA;
+  if (B->dirty) {
+    int rc = rebuild(B);
+    if (rc) return rc;
+  }
+  if (B->nitems[ST_CFL] == 0) return FB_OK;
   const int chunk = 10;  // steps per captured graph; a remainder runs eagerly
   if (nsteps >= chunk && (!B->exec || B->graph_steps != chunk || B->graph_dt != DT)) {
     if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
@@ -161,10 +246,10 @@ int fb_batch_sync(fb_batch *B) {
 }
 
 // Scalars of disk i ([0] PhysicalTime [1] OMEGAFRAME [2] last dt [3..6]
-// planet 0 x, y, vx, vy [7] Domega) and its status (FB_OK or the error that
-// froze it).
+// planet 0 x, y, vx, vy [7] Domega) and its status (FB_OK, FB_DONE or the
+// error that froze it).
 int fb_batch_get_scalars(fb_batch *B, int i, double *o, int *status) {
-  if (!B || i < 0 || i >= B->n) return FB_ERR_ARG;
+  if (!B || i < 0 || i >= B->n || B->state[i] != 2) return FB_ERR_ARG;
   fb_psys S;
   cudaSetDevice(B->device);
   if (cudaStreamSynchronize(B->stream) != cudaSuccess) return FB_ERR_CUDA;
@@ -178,6 +263,22 @@ int fb_batch_get_scalars(fb_batch *B, int i, double *o, int *status) {
   return FB_OK;
 }
 
+int fb_batch_poll(fb_batch *B, int *status, double *phys_time, long long *steps) {
+  if (!B) return FB_ERR_ARG;
+  cudaSetDevice(B->device);
+  if (cudaStreamSynchronize(B->stream) != cudaSuccess) return FB_ERR_CUDA;
+  std::vector<fb_psys> h(B->n);
+  if (cudaMemcpy(h.data(), B->d_psys, sizeof(fb_psys) * B->n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return FB_ERR_CUDA;
+  for (int i = 0; i < B->n; i++) {
+    const bool act = B->state[i] == 2;
+    if (status) status[i] = act ? h[i].status : (B->state[i] == 1 ? FB_SLOT_RESERVED : FB_SLOT_EMPTY);
+    if (phys_time) phys_time[i] = act ? h[i].phys_time : 0.0;
+    if (steps) steps[i] = act ? h[i].step_count : 0;
+  }
+  return FB_OK;
+}
+
 void *fb_batch_stream(fb_batch *B) { return B ? (void *)B->stream : nullptr; }
 
 // One eager step of every disk with CUDA events between the launch groups;
@@ -185,6 +286,11 @@ void *fb_batch_stream(fb_batch *B) { return B ? (void *)B->stream : nullptr; }
 int fb_batch_profile_step(fb_batch *B, double DT, float *ms, const char **names, int max) {
   if (!B) return FB_ERR_ARG;
   cudaSetDevice(B->device);
+  if (B->dirty) {
+    int rc = rebuild(B);
+    if (rc) return rc;
+  }
+  if (B->nitems[ST_CFL] == 0) return 0;
   Prof P;
   P.n = 0;
   g_prof = &P;

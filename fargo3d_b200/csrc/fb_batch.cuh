@@ -15,7 +15,12 @@
 
 namespace fb {
 
-enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_SWEEP_Z, ST_SWEEP_Y, ST_SWEEP_X, ST_NEWVEL, ST_N };
+// The azimuthal sweep has one work list per chunk width C (cells per thread;
+// ST_X1 + log2 C): each disk uses the width its own ring length picks
+// (sweep_x_chunk), so its arithmetic never depends on the other members.
+enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_SWEEP_Z, ST_SWEEP_Y, ST_X1, ST_X2, ST_X4, ST_X8, ST_X16,
+       ST_NEWVEL, ST_N };
+constexpr int NXC = 5;
 
 // tile shapes shared with the one-disk launchers (fb_launch.cuh)
 constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_NS = 8, COL_BX = 128, BND_BX = 128,
@@ -126,21 +131,29 @@ __global__ void __launch_bounds__(NV_BX) kb_newvel(const fb_disk_dev *ds, const 
 
 // The scalar work of the step for every disk, one thread per disk; then the
 // CFL minimum is reset for the next step.  dtmin[1] carries the kernels'
-// non-finite flag.
+// non-finite flag.  A disk with an end time uses it as its DT interval, so
+// its last step is clipped to land on it; that step still runs in full, and
+// the disk is frozen (FB_DONE) when the next step's scalar work finds it
+// there.  Empty slots (zeroed descriptors) are passed over.
 static __global__ void kb_scalars(const fb_disk_dev *ds, fb_psys *ps, int n, double DT) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const fb_disk_dev &D = ds[i];
+  if (D.nx == 0) return;
   unsigned long long *dm = (unsigned long long *)D.dtmin;
   fb_scalars sc = *D.scal_dev;
   if (!sc.skip) {
     fb_psys S = ps[i];
     const double cflmin = __longlong_as_double((long long)dm[0]);
-    if (dm[1] != 0ull) {
+    if (S.status == FB_DONE) {
+      sc.skip = 1;
+    } else if (dm[1] != 0ull) {
       S.status = FB_ERR_NONFINITE;
       sc.skip = 1;
-    } else if (fb_psys_step(&S, cflmin, DT, &sc) < 0.0) {
+    } else if (fb_psys_step(&S, cflmin, S.t_end > 0.0 ? S.t_end : DT, &sc) < 0.0) {
       sc.skip = 1;
+    } else if (S.t_end > 0.0 && S.dtemp >= S.t_end) {
+      S.status = FB_DONE;
     }
     ps[i] = S;
     *D.scal_dev = sc;
@@ -152,16 +165,20 @@ static __global__ void kb_scalars(const fb_disk_dev *ds, fb_psys *ps, int n, dou
 
 using namespace fb;
 
+// Slots: state[i] 0 empty, 1 reserved (created, not activated), 2 active.
+// n is the capacity; the work lists cover the active slots only.
 struct fb_batch {
   int n, precision, device, is3d, nfluids;
+  std::vector<int> state;
+  std::vector<double> t_end;
+  int dirty;
   cudaStream_t stream;
   std::vector<fb_disk *> disks;
   fb_disk_dev *d_disks;
   fb_psys *d_psys;
   int4 *items[ST_N];
   int nitems[ST_N];
-  size_t smem_x;
-  int cx;  /* cells per thread of the azimuthal sweep, uniform over the batch */
+  size_t smem_x[NXC];  /* shared memory of each chunk-width class of the azimuthal sweep */
   cudaGraphExec_t exec;
   int graph_steps;
   double graph_dt;
@@ -169,6 +186,7 @@ struct fb_batch {
 
 static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
   for (int di = 0; di < B->n; di++) {
+    if (B->state[di] != 2) continue;
     const fb_disk_dev &D = *fb_disk_internal_dev(B->disks[di]);
     const int nx = D.nx, ny = D.ny, nz = D.nz, sy = D.sy, sz = D.sz;
     dim3 g(1, 1, 1);
@@ -187,8 +205,10 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
       case ST_SWEEP_Y:
         g = dim3((nx + COL_BX - 1) / COL_BX, D.is3d ? nz + 1 : 1, (ny + 1 + COL_NS - 1) / COL_NS);
         break;
-      case ST_SWEEP_X: {
-        const int rpc = 256 / (nx / B->cx), nr = (ny + 1) * (D.is3d ? nz + 1 : 1);
+      case ST_X1: case ST_X2: case ST_X4: case ST_X8: case ST_X16: {
+        const int c = 1 << (st - ST_X1);
+        if (sweep_x_chunk(nx, 256) != c) { g = dim3(0); break; }
+        const int rpc = 256 / (nx / c), nr = (ny + 1) * (D.is3d ? nz + 1 : 1);
         g = dim3((nr + rpc - 1) / rpc);
         break;
       }
@@ -203,15 +223,18 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
 
 template <typename T, typename S>
 static void configure_sweep_x(fb_batch *B) {
-  static size_t done[17];
-  if (done[B->cx] >= B->smem_x) return;
-  done[B->cx] = B->smem_x;
-  switch (B->cx) {
-    case 16: cudaFuncSetAttribute(kb_sweep_x<T, 16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
-    case 8: cudaFuncSetAttribute(kb_sweep_x<T, 8, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
-    case 4: cudaFuncSetAttribute(kb_sweep_x<T, 4, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
-    case 2: cudaFuncSetAttribute(kb_sweep_x<T, 2, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
-    default: cudaFuncSetAttribute(kb_sweep_x<T, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B->smem_x); break;
+  static size_t done[NXC];
+  for (int k = 0; k < NXC; k++) {
+    if (done[k] >= B->smem_x[k]) continue;
+    done[k] = B->smem_x[k];
+    const int sm = (int)B->smem_x[k];
+    switch (k) {
+      case 4: cudaFuncSetAttribute(kb_sweep_x<T, 16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+      case 3: cudaFuncSetAttribute(kb_sweep_x<T, 8, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+      case 2: cudaFuncSetAttribute(kb_sweep_x<T, 4, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+      case 1: cudaFuncSetAttribute(kb_sweep_x<T, 2, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+      default: cudaFuncSetAttribute(kb_sweep_x<T, 1, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); break;
+    }
   }
 }
 
@@ -233,6 +256,7 @@ static void pmark(cudaStream_t st, const char *name) {
 // sweeps, the azimuthal sweep and NewVelocity; S: storage type.
 template <typename T, typename S, typename TC = T, typename TX = T, typename TN = T>
 static int launch_step(fb_batch *B, double DT) {
+  if (B->nitems[ST_CFL] == 0) return 0;  // no active disk
   configure_sweep_x<TX, S>(B);
   cudaStream_t st = B->stream;
   pmark(st, "start");
@@ -263,12 +287,18 @@ static int launch_step(fb_batch *B, double DT) {
     if (B->is3d) kb_sweep_col<TC, 1, S><<<grid(ST_SWEEP_Z), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Z], f);
     kb_sweep_col<TC, 0, S><<<grid(ST_SWEEP_Y), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Y], f);
     pmark(st, "sweep_cols");
-    switch (B->cx) {
-      case 16: kb_sweep_x<TX, 16, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 8: kb_sweep_x<TX, 8, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 4: kb_sweep_x<TX, 4, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      case 2: kb_sweep_x<TX, 2, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
-      default: kb_sweep_x<TX, 1, S><<<grid(ST_SWEEP_X), 256, B->smem_x, st>>>(ds, B->items[ST_SWEEP_X], f); break;
+    for (int k = 0; k < NXC; k++) {
+      const int n = B->nitems[ST_X1 + k];
+      if (!n) continue;
+      const int4 *it = B->items[ST_X1 + k];
+      const size_t sm = B->smem_x[k];
+      switch (k) {
+        case 4: kb_sweep_x<TX, 16, S><<<n, 256, sm, st>>>(ds, it, f); break;
+        case 3: kb_sweep_x<TX, 8, S><<<n, 256, sm, st>>>(ds, it, f); break;
+        case 2: kb_sweep_x<TX, 4, S><<<n, 256, sm, st>>>(ds, it, f); break;
+        case 1: kb_sweep_x<TX, 2, S><<<n, 256, sm, st>>>(ds, it, f); break;
+        default: kb_sweep_x<TX, 1, S><<<n, 256, sm, st>>>(ds, it, f); break;
+      }
     }
     pmark(st, "sweep_x");
   }

@@ -72,6 +72,7 @@ struct fb_disk {
   double *h_dtmin;              /* pinned */
   void *allocs[MAXALLOC];
   int nalloc;
+  size_t bytes;                 /* device bytes requested by this disk */
   /* optional per-launch timing (fb_disk_profile) */
   int prof;
   int nev;
@@ -98,6 +99,7 @@ static int dalloc(fb_disk *D, void **p, size_t bytes) {
   e = cudaMalloc(p, bytes ? bytes : 16);
   if (e != cudaSuccess) return fail(FB_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
   D->allocs[D->nalloc++] = *p;
+  D->bytes += bytes ? bytes : 16;
   cudaMemset(*p, 0, bytes ? bytes : 16);
   return FB_OK;
 }
@@ -300,6 +302,33 @@ static int upload_tables(fb_disk *D) {
   rc = upload(D, (const void **)&D->d.ramps, ramps, sy + 2 * sz, 0);
   free(ramps);
   return rc;
+}
+
+/* Upper bound of the device bytes fb_disk_create requests for a mesh: the
+ * fields (exact) plus the per-row / per-layer tables (bounded). */
+int fb_params_bytes(const fb_params *p, int precision, size_t *out) {
+  size_t esz, sy, sz, nc, rings, fields, b;
+  int is3d;
+  if (!p || !out || p->nx < 1 || p->ny < 1 || p->nfluids < 1) return fail(FB_ERR_ARG, "invalid parameters");
+  is3d = p->nz > 1;
+  esz = precision == FB_FP64 ? sizeof(double) : sizeof(float);
+  sy = (size_t)p->ny + 2 * NG;
+  sz = is3d ? (size_t)p->nz + 2 * NG : 1;
+  nc = (size_t)p->nx * sy * sz;
+  rings = sy * sz;
+  fields = is3d ? 15 + 7 : 11;
+  b = (size_t)p->nfluids * (fields * nc * esz + 2 * rings * sizeof(double) + rings * sizeof(int) + 4 * rings * esz);
+  b += 2 * sizeof(double) * (6 * ((size_t)p->nx + 1) + 20 * (sy + 1) + 16 * (sz + 1));
+  b += sizeof(double) * (18 + 6 * sz + 6 * sy + 6) + sizeof(double) * (sy + 2 * sz);
+  b += 64 + sizeof(fb_scalars) + 64 * 16;
+  *out = b;
+  return FB_OK;
+}
+
+int fb_disk_bytes(fb_disk *D, size_t *out) {
+  if (!D || !out) return fail(FB_ERR_ARG, "null argument");
+  *out = D->bytes;
+  return FB_OK;
 }
 
 /* ------------------------------------------------------------------------ */

@@ -38,7 +38,8 @@ typedef struct fb_psys_s {
   double omegaframe, omegaframe0, domega, phys_time, dtemp, last_dt;
   double roche_smoothing, aspectratio, flaringindex, thickness_smoothing;
   long long step_count;
-  int status;     /* 0 ok, FB_ERR_NULL_DT after a null time step */
+  int status;     /* 0 ok, FB_ERR_NULL_DT after a null time step, FB_DONE */
+  double t_end;   /* > 0: the disk stops at this physical time (batches) */
 } fb_psys;
 
 typedef struct { double e, a, M, i, phi; } fb_orbit;
@@ -231,6 +232,7 @@ static FB_HD inline void fb_psys_init(fb_psys *S, int np, const double *dist, co
   S->domega = S->phys_time = S->dtemp = S->last_dt = 0.0;
   S->step_count = 0;
   S->status = 0;
+  S->t_end = 0.0;
   for (n = 0; n < np; n++) {
     double d = dist[n];
     S->pmass[n] = mass[n];

@@ -116,6 +116,62 @@ void *fb_batch_stream(fb_batch *b);
 /* one eager step with per-launch-group device timing (see fb_disk_profile_read) */
 int fb_batch_profile_step(fb_batch *b, double dt_interval, float *ms, const char **names, int max);
 
+/* Batches with changing membership (no counterpart in the reference).  A
+ * batch made with fb_batch_create_slots holds up to `capacity` disks of one
+ * precision, dimensionality and fluid count; members join and leave between
+ * fb_batch_run calls, and the stage work lists and the captured graph are
+ * rebuilt at the next run after a change.  fb_batch_add creates a disk in a
+ * free slot (state still to be set through fb_batch_disk + fb_disk_set_state);
+ * fb_batch_activate initialises it and lets it step.  With t_end > 0 the disk
+ * runs until its physical time reaches t_end (its last step clipped to land
+ * on it, as a DT interval of length t_end clips the reference's last step)
+ * and is then frozen with FB_DONE; with t_end <= 0 it follows the dt_interval
+ * given to fb_batch_run.  fb_batch_remove destroys the slot's disk.
+ * fb_batch_poll reads every slot's status (FB_OK, FB_DONE, FB_SLOT_EMPTY,
+ * FB_SLOT_RESERVED or the error that froze it), physical time and step count
+ * after waiting for the batch's stream; arrays have `capacity` entries. */
+int fb_batch_create_slots(int capacity, int precision, int device, int is3d, int nfluids, fb_batch **out);
+int fb_batch_add(fb_batch *b, const fb_params *p, double t_end, int *slot);
+int fb_batch_activate(fb_batch *b, int slot);
+int fb_batch_remove(fb_batch *b, int slot);
+int fb_batch_capacity(fb_batch *b);
+int fb_batch_poll(fb_batch *b, int *status, double *phys_time, long long *steps);
+
+/* Device bytes: an upper bound of what fb_disk_create requests for these
+ * parameters, and what a disk actually requested. */
+int fb_params_bytes(const fb_params *p, int precision, size_t *out);
+int fb_disk_bytes(fb_disk *d, size_t *out);
+
+/* ---- continuous-batching server (fargo3d_b200/csrc/fb_server.cu; no
+ * counterpart in the reference).  Requests (one disk-planet solve each: its
+ * parameters, its initial state in host memory and an end time) are queued
+ * by fb_server_submit from any thread.  A worker thread admits queued
+ * requests in arrival order while their device bytes fit the HBM budget and
+ * a slot is free, runs every admitted disk together in chunks of
+ * `chunk_steps` steps (one batched launch per stage), and retires each disk
+ * when it reaches its end time, copying its final state to host memory.
+ * Requests arriving while others run join at the next chunk boundary.  All
+ * requests share precision, dimensionality and fluid count (one fluid).
+ * Times in info[] are seconds on the server's monotonic clock:
+ * [0] submitted [1] admitted [2] finished [3] hydro steps [4] physical time
+ * [5] final status [6] device bytes reserved [7] active cells. */
+typedef struct fb_server fb_server;
+int fb_server_create(int precision, int device, int is3d, size_t hbm_budget, int max_disks, int chunk_steps,
+                     fb_server **out);
+int fb_server_submit(fb_server *s, const fb_params *p, const double *rho, const double *vx, const double *vy,
+                     const double *vz, const double *cs, double t_end, long long *id);
+/* request state (FB_REQ_*) */
+int fb_server_status(fb_server *s, long long id, int *state);
+/* wait up to timeout_s seconds for a request to finish; *state as above */
+int fb_server_wait(fb_server *s, long long id, double timeout_s, int *state);
+/* copy a finished request's final state and info[8] out and forget it */
+int fb_server_fetch(fb_server *s, long long id, double *rho, double *vx, double *vy, double *vz, double info[8]);
+/* [0] queued [1] running [2] finished, not fetched [3] device bytes reserved
+ * [4] budget [5] chunks run [6] cell-updates done [7] seconds since create */
+int fb_server_stats(fb_server *s, double out8[8]);
+double fb_server_clock(fb_server *s);
+int fb_server_destroy(fb_server *s);
+
 /* CFL time step without allocating: for callers that own all device memory
  * and cannot let a library call cudaMalloc (FARGO3D's own GPU build, whose
  * Fields CreateField allocates once; applications on a fixed memory pool).

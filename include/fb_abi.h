@@ -25,4 +25,15 @@
 #define FB_ERR_NOMEM -5      /* device allocation failed */
 #define FB_ERR_TOO_LARGE -6  /* request exceeds a fixed capacity */
 
+/* per-member states of a batch (fb_batch_poll) */
+#define FB_DONE 1            /* reached its end time (fb_batch_add) */
+#define FB_SLOT_EMPTY 2      /* no disk in this slot */
+#define FB_SLOT_RESERVED 3   /* disk created, not yet activated */
+
+/* request states of a server (fb_server_status) */
+#define FB_REQ_QUEUED 0
+#define FB_REQ_RUNNING 1
+#define FB_REQ_DONE 2
+#define FB_REQ_FAILED 3
+
 #endif

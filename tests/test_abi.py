@@ -42,6 +42,24 @@ def test_no_cpu_fallback_without_device():
     with pytest.raises(FargoError) as e:
         Disk(config_fargo2d(32, 16))
     assert "FB_ERR_CUDA" in str(e.value)
+    from fargo3d_b200 import Server
+    with pytest.raises(FargoError) as e:
+        Server("fp32")
+    assert "FB_ERR_CUDA" in str(e.value)
+
+
+def test_params_bytes_bound():
+    """fb_params_bytes (host arithmetic only): the fields dominate and the
+    bound scales with cells and element size."""
+    from fargo3d_b200 import config_fargo2d, config_p3disof
+    from fargo3d_b200._abi import params_bytes
+    c = config_fargo2d(384, 128)
+    b64, b32 = params_bytes(c, "fp64"), params_bytes(c, "fp32")
+    cells = 384 * (128 + 6)
+    assert 11 * cells * 8 <= b64 <= 11 * cells * 8 * 1.2
+    assert 11 * cells * 4 <= b32 < b64
+    c3 = config_p3disof(64, 32, 16)
+    assert params_bytes(c3, "fp64") >= 22 * 64 * 38 * 22 * 8
 
 
 def test_params_layout_matches_oracle():
