@@ -14,6 +14,13 @@ dataset is involved):
            is measured beside it ("fp64_plain").
   p3disof  one 3D spherical disk 512 x 256 x 48 (plain path, --precision)
   fargo2d  one 2D cylindrical disk 384 x 128 (plain path, --precision)
+  serving  the continuous-batching server: --requests requests (default
+           100) arriving as a Poisson process (--rate, 20/s), sizes
+           {256x64, 512x128, 1024x256, 2048x512} weighted {.4,.3,.2,.1}, each
+           run for --orbits orbits (default 0.25, a bounded stand-in for the
+           50-orbit requests), FP32; reports p50/p99 request latency beside
+           throughput.  The default (batched) run adds the same measurement
+           as its "serving" object.
 
 value       cell-updates/s of the whole job, device-timed with CUDA events on
             the launching stream, state resident in HBM (max over ranks)
@@ -74,6 +81,10 @@ def workload(name: str, rank: int = 0):
         return [config_fargo2d(384, 128, seed=rank)], "fargo2d 384x128 (2D cylindrical, 1 planet, nu=1e-5)"
     if name == "p3disof":
         return [config_p3disof(512, 256, 48, seed=rank)], "p3disof 512x256x48 (3D spherical, 1 planet, nu=1e-5)"
+    if name == "serving":
+        from fargo3d_b200 import serving_requests
+        return [r.cfg for r in serving_requests(64, seed=rank)], ("serving requests, sizes {256x64, 512x128, "
+                                                                  "1024x256, 2048x512} weighted {.4,.3,.2,.1}")
     return config_batched(64, seed=rank), ("64 independent 2D disks, N_phi x N_r in {128..1024} x {64..512}, "
                                            "alpha viscosity, 1 planet each")
 
@@ -164,6 +175,51 @@ def time_plain_fp64(cfgs, steps, device):
         cells += c.active_cells * steps
         d.close()
     return cells / t
+
+
+def run_serving(n_requests: int, rate: float, orbits: float, device: int, seed: int = 0):
+    """The serving workload through the continuous-batching server: Poisson
+    arrivals submitted in real time by a thread, every request run to its end
+    time; latency = finished - submitted on the server's clock.  The initial
+    states are built before the clock starts."""
+    from fargo3d_b200 import Server, initial_state, serving_requests
+    reqs = serving_requests(n_requests, rate=rate, orbits=orbits, seed=seed)
+    states = [initial_state(r.cfg) for r in reqs]
+    srv = Server("fp32", device=device, max_disks=256, chunk_steps=10)
+    # warm-up: one small request of each size class (kernel loading, graphs)
+    warm = [srv.submit(r.cfg, 0.05, st) for r, st in zip(reqs[:4], states[:4])]
+    for w in warm:
+        srv.wait(w)
+        srv.fetch(w)
+    ids = [None] * len(reqs)
+
+    def submitter():
+        t0 = time.perf_counter()
+        for k, (r, st) in enumerate(zip(reqs, states)):
+            dt = r.arrival - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids[k] = srv.submit(r.cfg, r.t_end, st)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    infos = []
+    for rid in ids:
+        srv.wait(rid)
+        infos.append(srv.fetch(rid)[1])
+    srv.close()
+    lat = np.array([i["finished"] - i["submitted"] for i in infos])
+    work = sum(i["steps"] * i["cells"] for i in infos)
+    span = max(i["finished"] for i in infos) - min(i["submitted"] for i in infos)
+    return {"value": work / span, "unit": "cell-updates/s",
+            "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3), "p99": float(np.percentile(lat, 99) * 1e3),
+                           "max": float(lat.max() * 1e3)},
+            "queue_wait_ms_p50": float(np.percentile([i["admitted"] - i["submitted"] for i in infos], 50) * 1e3),
+            "requests": len(infos), "failed": int(sum(1 for i in infos if i["status"] != 1)),
+            "workload": "%d requests, Poisson %.0f/s, sizes {256x64, 512x128, 1024x256, 2048x512} weighted "
+                        "{.4,.3,.2,.1}, %.2g orbits each, FP32, continuous batching" % (len(infos), rate, orbits),
+            "span_s": span}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -342,7 +398,11 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "p3disof", "fargo2d"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "p3disof", "fargo2d", "serving"])
+    ap.add_argument("--requests", type=int, default=100, help="serving: number of requests")
+    ap.add_argument("--orbits", type=float, default=0.25, help="serving: orbits per request")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg of the default run")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
     ap.add_argument("--cpu-steps", type=int, default=0, help="reference steps per disk (0: auto)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg (profiling runs)")
@@ -354,7 +414,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     cfgs, wname = workload(args.workload, 0)
-    auto = {"batched": 6, "p3disof": 2, "fargo2d": 300}[args.workload]
+    auto = {"batched": 6, "p3disof": 2, "fargo2d": 300, "serving": 6}[args.workload]
     cpu_steps = args.cpu_steps or auto
     if args.impl == "reference":
         if rank != 0:
@@ -370,6 +430,17 @@ def main():
                 "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
+    if args.workload == "serving":
+        if rank != 0:
+            return
+        sv = run_serving(args.requests, args.rate, args.orbits, local_rank)
+        line = {"metric": METRIC, "value": sv["value"], "unit": "cell-updates/s", "n_gpus": 1,
+                "steps": sv["requests"], "warmup": 4, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": sv["workload"], "parallelism": "one GPU"},
+                "latency_ms": sv["latency_ms"], "serving": sv}
+        print(json.dumps(line), flush=True)
+        return
     if world > 1:
         import torch
         import torch.distributed as tdist
@@ -377,6 +448,8 @@ def main():
         torch.cuda.set_device(local_rank)
         tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
     line = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and args.workload == "batched" and not args.no_serving:
+        line["serving"] = run_serving(args.requests, args.rate, args.orbits, local_rank)
     if rank == 0 and not args.no_cpu:
         v, kind, cores, wall = cpu_reference(cfgs, cpu_steps)
         line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": kind,
