@@ -90,6 +90,8 @@ def lib():
     L.fb_disk_stream.restype = C.c_void_p
     L.fb_disk_stream.argtypes = [C.c_void_p]
     L.fb_params_bytes.argtypes = [C.POINTER(FbParams), C.c_int, C.POINTER(C.c_size_t)]
+    L.fb_disk_set_tiles.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.fb_disk_get_tiles.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.fb_disk_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
     _lib = L
     return L
@@ -126,6 +128,9 @@ def bind_batch(L):
     L.fb_batch_remove.argtypes = [C.c_void_p, C.c_int]
     L.fb_batch_capacity.argtypes = [C.c_void_p]
     L.fb_batch_poll.argtypes = [C.c_void_p, C.POINTER(C.c_int), _D, C.POINTER(C.c_longlong)]
+    L.fb_batch_set_tiles.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+    L.fb_disk_set_tiles.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.fb_disk_get_tiles.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L._batch_bound = True
     return L
 
@@ -144,6 +149,7 @@ def bind_server(L):
     L.fb_server_clock.argtypes = [C.c_void_p]
     L.fb_server_clock.restype = C.c_double
     L.fb_server_destroy.argtypes = [C.c_void_p]
+    L.fb_server_set_tiles.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
     L._server_bound = True
     return L
 

@@ -22,7 +22,10 @@ class _Member:
 
 
 class Batch:
-    def __init__(self, cfgs, precision: str = "fp32", device: int = 0):
+    """`tiles`: "table" applies the autotuner's table (fargo3d_b200/autotune.py)
+    to every member whose shape it lists, None keeps the defaults."""
+
+    def __init__(self, cfgs, precision: str = "fp32", device: int = 0, tiles="table"):
         L = _abi.bind_batch(_abi.lib())
         self.cfgs = list(cfgs)
         arr = (_abi.FbParams * len(self.cfgs))(*[_abi.params_of(c) for c in self.cfgs])
@@ -36,6 +39,9 @@ class Batch:
             dh = C.c_void_p()
             _abi.check(L.fb_batch_disk(h, i, C.byref(dh)))
             self._members.append(_Member(dh, c.shape))
+        if tiles == "table":
+            from .autotune import TileTable
+            TileTable.default().apply(self)
 
     def __len__(self):
         return len(self.cfgs)
@@ -76,6 +82,23 @@ class Batch:
         _abi.check(_abi.lib().fb_batch_get_scalars(self._h, i, o.ctypes.data_as(C.POINTER(C.c_double)),
                                                    C.byref(st)))
         return o, st.value
+
+    def set_tiles(self, i, sweep_x_cells: int = 0, col_segment: int = 0):
+        _abi.check(_abi.lib().fb_batch_set_tiles(self._h, i, sweep_x_cells, col_segment))
+
+    def tiles(self, i):
+        cx, ns = C.c_int(), C.c_int()
+        _abi.check(_abi.lib().fb_disk_get_tiles(self._members[i]._h, C.byref(cx), C.byref(ns)))
+        return cx.value, ns.value
+
+    def profile_step(self, dt_interval: float = 1e30) -> dict:
+        """One eager step with per-launch-group device times (ms)."""
+        ms = (C.c_float * 40)()
+        names = (C.c_char_p * 40)()
+        n = _abi.lib().fb_batch_profile_step(self._h, dt_interval, ms, names, 40)
+        if n < 0:
+            _abi.check(n)
+        return {names[i].decode(): float(ms[i]) for i in range(n)}
 
     @property
     def stream(self) -> int:

@@ -48,8 +48,8 @@ static int rebuild(fb_batch *B) {
   // per chunk-width class: the largest shared-memory need of its disks
   for (int k = 0; k < NXC; k++) B->smem_x[k] = 0;
   for (const fb_disk_dev *d : act) {
-    const int c = sweep_x_chunk(d->nx, 256);
-    if (c < 1) return FB_ERR_ARG;
+    const int c = disk_cx(*d);
+    if (!valid_cx(d->nx, c)) return FB_ERR_ARG;
     int k = 0;
     while ((1 << k) < c) k++;
     // the sweep keeps its rings in its compute precision
@@ -62,8 +62,8 @@ static int rebuild(fb_batch *B) {
     B->nitems[s] = tiles(B, s, v);
     if (B->nitems[s] > 0) {
       if (cudaMalloc(&B->items[s], sizeof(int4) * v.size()) != cudaSuccess) return FB_ERR_NOMEM;
-      if (cudaMemcpy(B->items[s], v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-        return FB_ERR_CUDA;
+      cudaError_t e = cudaMemcpy(B->items[s], v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fb_internal_fail(FB_ERR_CUDA, "work list upload", (int)e);
     }
   }
   return FB_OK;
@@ -172,6 +172,14 @@ int fb_batch_remove(fb_batch *B, int s) {
 
 int fb_batch_capacity(fb_batch *B) { return B ? B->n : 0; }
 
+int fb_batch_set_tiles(fb_batch *B, int s, int sweep_x_cells, int col_segment) {
+  if (!B || s < 0 || s >= B->n || !B->disks[s]) return FB_ERR_ARG;
+  int rc = fb_disk_set_tiles(B->disks[s], sweep_x_cells, col_segment);
+  if (rc) return rc;
+  if (B->state[s] == 2) B->dirty = 1;
+  return FB_OK;
+}
+
 // All members at once (the original interface): slots 0..n-1 in order.
 int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_batch **out) {
   if (!out) return FB_ERR_ARG;
@@ -222,7 +230,8 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
     cudaGraph_t g;
     if (cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FB_ERR_CUDA;
     for (int s = 0; s < chunk; s++) launch_step_any(B, DT);
-    if (cudaStreamEndCapture(B->stream, &g) != cudaSuccess) return FB_ERR_CUDA;
+    cudaError_t e = cudaStreamEndCapture(B->stream, &g);
+    if (e != cudaSuccess) return fb_internal_fail(FB_ERR_CUDA, "step graph capture", (int)e);
     if (cudaGraphInstantiate(&B->exec, g, 0) != cudaSuccess) { cudaGraphDestroy(g); return FB_ERR_CUDA; }
     cudaGraphDestroy(g);
     B->graph_steps = chunk;
@@ -230,11 +239,13 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
   }
   int done = 0;
   while (done + chunk <= nsteps) {
-    if (cudaGraphLaunch(B->exec, B->stream) != cudaSuccess) return FB_ERR_CUDA;
+    cudaError_t e = cudaGraphLaunch(B->exec, B->stream);
+    if (e != cudaSuccess) return fb_internal_fail(FB_ERR_CUDA, "cudaGraphLaunch", (int)e);
     done += chunk;
   }
   for (; done < nsteps; done++) {
-    if (launch_step_any(B, DT)) return FB_ERR_CUDA;
+    int e = launch_step_any(B, DT);
+    if (e) return fb_internal_fail(FB_ERR_CUDA, "batched step launch", e);
   }
   return FB_OK;
 }

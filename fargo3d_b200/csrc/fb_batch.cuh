@@ -18,12 +18,15 @@ namespace fb {
 // The azimuthal sweep has one work list per chunk width C (cells per thread;
 // ST_X1 + log2 C): each disk uses the width its own ring length picks
 // (sweep_x_chunk), so its arithmetic never depends on the other members.
-enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_SWEEP_Z, ST_SWEEP_Y, ST_X1, ST_X2, ST_X4, ST_X8, ST_X16,
-       ST_NEWVEL, ST_N };
-constexpr int NXC = 5;
+// Likewise the column sweeps have one per segment length NS (ST_Z4 + k,
+// ST_Y4 + k for NS = 4 << k).  Both are per-disk tile choices (disk_cx,
+// disk_ns; the autotuner sets them).
+enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_Z4, ST_Z8, ST_Z16, ST_Y4, ST_Y8, ST_Y16,
+       ST_X1, ST_X2, ST_X4, ST_X8, ST_X16, ST_NEWVEL, ST_N };
+constexpr int NXC = 5, NNS = 3;
 
 // tile shapes shared with the one-disk launchers (fb_launch.cuh)
-constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_NS = 8, COL_BX = 128, BND_BX = 128,
+constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_BX = 128, BND_BX = 128,
               NV_BX = 128;
 
 #define FB_TILE                                        \
@@ -75,7 +78,7 @@ __global__ void kb_bnd(const fb_disk_dev *ds, const int4 *items, int f, int vtem
   else b_bnd_y<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, bid);
 }
 
-template <typename T, int DIR, typename S>
+template <typename T, int DIR, int COL_NS, typename S>
 __global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? 4 : 1) kb_sweep_col(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   Dims m = dims_of(D);
@@ -199,15 +202,20 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
         break;
       case ST_BND_Z: g = D.is3d ? dim3((nx + BND_BX - 1) / BND_BX, sy, 6) : dim3(0); break;
       case ST_BND_Y: g = dim3((nx + BND_BX - 1) / BND_BX, 6, sz); break;
-      case ST_SWEEP_Z:
-        g = D.is3d ? dim3((nx + COL_BX - 1) / COL_BX, sy - 1, (nz + 1 + COL_NS - 1) / COL_NS) : dim3(0);
+      case ST_Z4: case ST_Z8: case ST_Z16: {
+        const int ns = 4 << (st - ST_Z4);
+        g = D.is3d && disk_ns(D) == ns ? dim3((nx + COL_BX - 1) / COL_BX, sy - 1, (nz + 1 + ns - 1) / ns) : dim3(0);
         break;
-      case ST_SWEEP_Y:
-        g = dim3((nx + COL_BX - 1) / COL_BX, D.is3d ? nz + 1 : 1, (ny + 1 + COL_NS - 1) / COL_NS);
+      }
+      case ST_Y4: case ST_Y8: case ST_Y16: {
+        const int ns = 4 << (st - ST_Y4);
+        g = disk_ns(D) == ns ? dim3((nx + COL_BX - 1) / COL_BX, D.is3d ? nz + 1 : 1, (ny + 1 + ns - 1) / ns)
+                             : dim3(0);
         break;
+      }
       case ST_X1: case ST_X2: case ST_X4: case ST_X8: case ST_X16: {
         const int c = 1 << (st - ST_X1);
-        if (sweep_x_chunk(nx, 256) != c) { g = dim3(0); break; }
+        if (disk_cx(D) != c) { g = dim3(0); break; }
         const int rpc = 256 / (nx / c), nr = (ny + 1) * (D.is3d ? nz + 1 : 1);
         g = dim3((nr + rpc - 1) / rpc);
         break;
@@ -284,8 +292,14 @@ static int launch_step(fb_batch *B, double DT) {
     if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
     else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
     pmark(st, "rowsum_vtemp");
-    if (B->is3d) kb_sweep_col<TC, 1, S><<<grid(ST_SWEEP_Z), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Z], f);
-    kb_sweep_col<TC, 0, S><<<grid(ST_SWEEP_Y), COL_BX, 0, st>>>(ds, B->items[ST_SWEEP_Y], f);
+    if (B->is3d) {
+      if (B->nitems[ST_Z4]) kb_sweep_col<TC, 1, 4, S><<<grid(ST_Z4), COL_BX, 0, st>>>(ds, B->items[ST_Z4], f);
+      if (B->nitems[ST_Z8]) kb_sweep_col<TC, 1, 8, S><<<grid(ST_Z8), COL_BX, 0, st>>>(ds, B->items[ST_Z8], f);
+      if (B->nitems[ST_Z16]) kb_sweep_col<TC, 1, 16, S><<<grid(ST_Z16), COL_BX, 0, st>>>(ds, B->items[ST_Z16], f);
+    }
+    if (B->nitems[ST_Y4]) kb_sweep_col<TC, 0, 4, S><<<grid(ST_Y4), COL_BX, 0, st>>>(ds, B->items[ST_Y4], f);
+    if (B->nitems[ST_Y8]) kb_sweep_col<TC, 0, 8, S><<<grid(ST_Y8), COL_BX, 0, st>>>(ds, B->items[ST_Y8], f);
+    if (B->nitems[ST_Y16]) kb_sweep_col<TC, 0, 16, S><<<grid(ST_Y16), COL_BX, 0, st>>>(ds, B->items[ST_Y16], f);
     pmark(st, "sweep_cols");
     for (int k = 0; k < NXC; k++) {
       const int n = B->nitems[ST_X1 + k];

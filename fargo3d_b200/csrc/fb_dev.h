@@ -70,6 +70,8 @@ typedef struct {
   double *bnd_tab;        /* boundary factor tables (double) */
   int bnd_tab_n;
   double *ramps;          /* Stockholm ramps: [sy] radial, [sz] zmed, [sz] zmin */
+  int tile_cx;            /* azimuthal sweep cells per thread (0: default) */
+  int tile_ns;            /* column sweep segment length (0: default) */
 } fb_disk_dev;
 
 /* Launchers (fb_kernels_f64.cu / fb_kernels_f32.cu). Return cudaError_t. */
@@ -91,6 +93,7 @@ fb_disk_dev *fb_disk_internal_dev(struct fb_disk *d);
 struct fb_psys_s *fb_disk_internal_psys(struct fb_disk *d);
 void *fb_disk_internal_scalars(struct fb_disk *d);
 size_t fb_disk_internal_esz(struct fb_disk *d);
+int fb_internal_fail(int code, const char *what, int cuda_err);
 
 #ifdef __cplusplus
 }

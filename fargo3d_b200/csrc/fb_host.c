@@ -40,6 +40,12 @@ static int fail(int code, const char *fmt, ...) {
   return code;
 }
 
+/* error text for the batch and server translation units */
+int fb_internal_fail(int code, const char *what, int cuda_err) {
+  if (cuda_err) return fail(code, "%s: %s", what, cudaGetErrorString((cudaError_t)cuda_err));
+  return fail(code, "%s", what);
+}
+
 #define CU(call)                                                                 \
   do {                                                                           \
     cudaError_t e_ = (call);                                                     \
@@ -322,6 +328,44 @@ int fb_params_bytes(const fb_params *p, int precision, size_t *out) {
   b += sizeof(double) * (18 + 6 * sz + 6 * sy + 6) + sizeof(double) * (sy + 2 * sz);
   b += 64 + sizeof(fb_scalars) + 64 * 16;
   *out = b;
+  return FB_OK;
+}
+
+/* Tile choices: azimuthal sweep cells per thread (1, 2, 4, 8, 16 dividing
+ * Nx with at most 256 threads per ring; 0 restores the default) and column
+ * sweep segment length (4, 8, 16; 0 restores 8). */
+#define FB_SMEM_MAX (227 * 1024)
+
+static int default_cx(int nx) {
+  const int cs[5] = {4, 8, 16, 2, 1};
+  int t;
+  for (t = 0; t < 5; t++)
+    if (nx % cs[t] == 0 && nx / cs[t] <= 256) return cs[t];
+  return 0;
+}
+
+int fb_disk_set_tiles(fb_disk *D, int cx, int ns) {
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  if (cx != 0 && !((cx == 1 || cx == 2 || cx == 4 || cx == 8 || cx == 16) && D->d.nx % cx == 0 && D->d.nx / cx <= 256))
+    return fail(FB_ERR_ARG, "azimuthal chunk %d does not tile Nx = %d in 256 threads", cx, D->d.nx);
+  if (cx != 0) {
+    /* whole rings per CTA of 256 threads, two buffers of (1 + nq) fields
+     * plus the velocity ring, in the sweep's element size: at most 227 KiB */
+    size_t rpc = 256 / (D->d.nx / cx), nq = D->d.is3d ? 6 : 4;
+    size_t bytes = rpc * (size_t)D->d.nx * (2 * (1 + nq) + 1) * D->esz;
+    if (bytes > FB_SMEM_MAX)
+      return fail(FB_ERR_ARG, "azimuthal chunk %d on Nx = %d needs %zu bytes of shared memory", cx, D->d.nx, bytes);
+  }
+  if (ns != 0 && ns != 4 && ns != 8 && ns != 16) return fail(FB_ERR_ARG, "column segment %d not in {4, 8, 16}", ns);
+  D->d.tile_cx = cx;
+  D->d.tile_ns = ns;
+  return FB_OK;
+}
+
+int fb_disk_get_tiles(fb_disk *D, int *cx, int *ns) {
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  if (cx) *cx = D->d.tile_cx ? D->d.tile_cx : default_cx(D->d.nx);
+  if (ns) *ns = D->d.tile_ns ? D->d.tile_ns : 8;
   return FB_OK;
 }
 

@@ -1187,6 +1187,13 @@ __host__ __device__ inline int sweep_x_chunk(int nx, int nt) {
   return 0;
 }
 
+// Tile choices of a disk: the set value (fb_disk_set_tiles, usually from the
+// autotuner) or the default.
+inline int disk_cx(const fb_disk_dev &d) { return d.tile_cx ? d.tile_cx : sweep_x_chunk(d.nx, 256); }
+inline int disk_ns(const fb_disk_dev &d) { return d.tile_ns ? d.tile_ns : 8; }
+inline bool valid_cx(int nx, int c) { return (c == 1 || c == 2 || c == 4 || c == 8 || c == 16) && nx % c == 0 && nx / c <= 256; }
+inline bool valid_ns(int ns) { return ns == 4 || ns == 8 || ns == 16; }
+
 template <typename T, int C, typename S = T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_sweep_x2(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
                                                   int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,

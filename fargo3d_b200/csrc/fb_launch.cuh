@@ -83,13 +83,12 @@ static int launch_bnd(const fb_disk_dev *d, int f, int vtemp, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
-template <typename T, typename S>
-static int launch_sweep_cols(const fb_disk_dev *d, int f, cudaStream_t st) {
+template <typename T, typename S, int NS>
+static int launch_sweep_cols_n(const fb_disk_dev *d, int f, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
   Dims m = dims_of(*d);
   Geo<T> g = geo_of<T>(sizeof(T) == 8 ? d->geomd : d->geom);
   Geo<double> gd = geo_of<double>(d->geomd);
-  constexpr int NS = 8;
   const int bx = 128;
   const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;  // rows 2 .. Ny+2
   S *rho_out;
@@ -128,6 +127,16 @@ static int launch_sweep_cols(const fb_disk_dev *d, int f, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+// column segment length: the disk's tile choice (4, 8 or 16 cells)
+template <typename T, typename S>
+static int launch_sweep_cols(const fb_disk_dev *d, int f, cudaStream_t st) {
+  switch (disk_ns(*d)) {
+    case 4: return launch_sweep_cols_n<T, S, 4>(d, f, st);
+    case 16: return launch_sweep_cols_n<T, S, 16>(d, f, st);
+    default: return launch_sweep_cols_n<T, S, 8>(d, f, st);
+  }
+}
+
 template <typename T, typename S>
 static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
   const fb_fluid_dev &F = d->fl[f];
@@ -141,8 +150,8 @@ static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
   S *q[6] = {(S *)(b ? F.mpx_b : F.mpx), (S *)(b ? F.mmx_b : F.mmx), (S *)(b ? F.mpy_b : F.mpy),
              (S *)(b ? F.mmy_b : F.mmy), (S *)(b ? F.mpz_b : F.mpz), (S *)(b ? F.mmz_b : F.mmz)};
   // azimuthal sweep: C cells per thread, whole rings per CTA of 256 threads
-  const int C = sweep_x_chunk(m.nx, 256);
-  if (C == 0) return (int)cudaErrorInvalidValue;
+  const int C = disk_cx(*d);
+  if (!valid_cx(m.nx, C)) return (int)cudaErrorInvalidValue;
   const int nj = yhi - ylo + 1, nrings = nj * (m.is3d ? m.nz + 1 : 1);
   const int rpc = 256 / (m.nx / C);
   const size_t smem = sweep_x2_smem(m.nx, C, 256, nq, sizeof(T));

@@ -31,6 +31,8 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+long long shape_key(int nx, int ny, int nz) { return ((long long)nx << 40) | ((long long)ny << 20) | (nz > 1 ? nz : 1); }
+
 struct Req {
   long long id;
   fb_params p;
@@ -57,6 +59,7 @@ struct fb_server {
   std::deque<Req *> queue;
   std::map<long long, Req *> reqs;
   std::vector<Req *> slot_req;
+  std::map<long long, std::pair<int, int>> tiles;  // shape key -> (sweep_x_cells, col_segment)
   size_t reserved = 0;
   int nrunning = 0, nfinished = 0;
   long long next_id = 1;
@@ -115,6 +118,15 @@ void fb_server::run() {
       if (!rc)
         rc = fb_disk_set_state(d, 0, r->in[0].data(), r->in[1].data(), r->in[2].data(),
                                r->in[3].empty() ? nullptr : r->in[3].data(), r->in[4].data());
+      if (!rc) {
+        std::pair<int, int> t(0, 0);
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          auto it = tiles.find(shape_key(r->p.nx, r->p.ny, r->p.nz));
+          if (it != tiles.end()) t = it->second;
+        }
+        if (t.first || t.second) rc = fb_batch_set_tiles(B, slot, t.first, t.second);
+      }
       if (!rc) rc = fb_batch_activate(B, slot);
       std::lock_guard<std::mutex> lk(mu);
       if (rc) {
@@ -280,6 +292,13 @@ int fb_server_stats(fb_server *S, double *o) {
 }
 
 double fb_server_clock(fb_server *S) { return S ? S->now() : 0.0; }
+
+int fb_server_set_tiles(fb_server *S, int nx, int ny, int nz, int sweep_x_cells, int col_segment) {
+  if (!S || nx < 1 || ny < 1) return FB_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->tiles[shape_key(nx, ny, nz)] = std::make_pair(sweep_x_cells, col_segment);
+  return FB_OK;
+}
 
 int fb_server_destroy(fb_server *S) {
   if (!S) return FB_OK;

@@ -19,7 +19,9 @@ def _ptr(a):
 
 
 class Disk:
-    def __init__(self, cfg: DiskConfig, precision: str = "fp64", device: int = 0):
+    def __init__(self, cfg: DiskConfig, precision: str = "fp64", device: int = 0, tiles="table"):
+        """`tiles`: "table" applies the autotuner's choice for this shape
+        (fargo3d_b200/autotune.py), None keeps the defaults."""
         self.cfg = cfg
         self.precision = precision
         L = _abi.lib()
@@ -28,6 +30,11 @@ class Disk:
         prec = _abi.FB_FP64 if precision == "fp64" else _abi.FB_FP32
         _abi.check(L.fb_disk_create(C.byref(self._p), prec, device, C.byref(h)))
         self._h = h
+        if tiles == "table":
+            from .autotune import TileTable, cx_candidates
+            t = TileTable.default().get(cfg, precision)
+            if t and t[0] in cx_candidates(cfg.nx, precision, cfg.is3d):
+                _abi.check(L.fb_disk_set_tiles(h, t[0], t[1]))
         self.shape = cfg.shape
 
     # ------------------------------------------------------------------ state

@@ -33,7 +33,7 @@ def _ptr(a):
 
 class Server:
     def __init__(self, precision: str = "fp32", device: int = 0, is3d: bool = False, hbm_budget: int = 0,
-                 max_disks: int = 64, chunk_steps: int = 10):
+                 max_disks: int = 64, chunk_steps: int = 10, tiles="table"):
         L = _abi.bind_server(_abi.lib())
         h = C.c_void_p()
         prec = _abi.FB_FP64 if precision == "fp64" else _abi.FB_FP32
@@ -42,6 +42,13 @@ class Server:
         self._h = h
         self.precision = precision
         self._shapes = {}
+        if tiles == "table":   # the autotuner's choices for every shape it lists
+            from .autotune import TileTable
+            for key, e in TileTable.default().entries.items():
+                shape, prec = key.split(":")
+                nx, ny, nz = (int(v) for v in shape.split("x"))
+                if prec == precision and (nz > 1) == is3d:
+                    _abi.check(L.fb_server_set_tiles(h, nx, ny, nz, e["sweep_x_cells"], e["col_segment"]))
 
     def submit(self, cfg: DiskConfig, t_end: float, state=None) -> int:
         """Queue one disk; `state` = (rho, vx, vy, vz, cs) or the setup's

@@ -137,6 +137,17 @@ int fb_batch_remove(fb_batch *b, int slot);
 int fb_batch_capacity(fb_batch *b);
 int fb_batch_poll(fb_batch *b, int *status, double *phys_time, long long *steps);
 
+/* Tile shapes (no counterpart in the reference, whose c2cuda build fixes one
+ * block shape per kernel after a sweep, scripts/blocks_function.py):
+ * sweep_x_cells = cells per thread of the azimuthal sweep (1, 2, 4, 8 or 16,
+ * dividing Nx with at most 256 threads per ring), col_segment = cells per
+ * thread of the radial/colatitude sweeps (4, 8 or 16); 0 = the default.  The
+ * autotuner (fargo3d_b200/autotune.py) picks them per (Nx, Ny, Nz,
+ * precision).  A batch member's choice takes effect at the next run. */
+int fb_disk_set_tiles(fb_disk *d, int sweep_x_cells, int col_segment);
+int fb_disk_get_tiles(fb_disk *d, int *sweep_x_cells, int *col_segment);
+int fb_batch_set_tiles(fb_batch *b, int slot, int sweep_x_cells, int col_segment);
+
 /* Device bytes: an upper bound of what fb_disk_create requests for these
  * parameters, and what a disk actually requested. */
 int fb_params_bytes(const fb_params *p, int precision, size_t *out);
@@ -170,6 +181,8 @@ int fb_server_fetch(fb_server *s, long long id, double *rho, double *vx, double 
  * [4] budget [5] chunks run [6] cell-updates done [7] seconds since create */
 int fb_server_stats(fb_server *s, double out8[8]);
 double fb_server_clock(fb_server *s);
+/* tiles (fb_disk_set_tiles) for every later admitted disk of this shape */
+int fb_server_set_tiles(fb_server *s, int nx, int ny, int nz, int sweep_x_cells, int col_segment);
 int fb_server_destroy(fb_server *s);
 
 /* CFL time step without allocating: for callers that own all device memory
