@@ -21,7 +21,7 @@ namespace fb {
 // Likewise the column sweeps have one per segment length NS (ST_Z4 + k,
 // ST_Y4 + k for NS = 4 << k).  Both are per-disk tile choices (disk_cx,
 // disk_ns; the autotuner sets them).
-enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_Z4, ST_Z8, ST_Z16, ST_Y4, ST_Y8, ST_Y16,
+enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_COLL, ST_Z4, ST_Z8, ST_Z16, ST_Y4, ST_Y8, ST_Y16,
        ST_X1, ST_X2, ST_X4, ST_X8, ST_X16, ST_NEWVEL, ST_N };
 constexpr int NXC = 5, NNS = 3;
 
@@ -76,6 +76,14 @@ __global__ void kb_bnd(const fb_disk_dev *ds, const int4 *items, int f, int vtem
   S *vx = (S *)(vtemp ? F.vxt : F.vx), *vy = (S *)(vtemp ? F.vyt : F.vy), *vz = (S *)(vtemp ? F.vzt : F.vz);
   if (zside) b_bnd_z<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, bid);
   else b_bnd_y<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, bid);
+}
+
+template <typename T, int N, typename S>
+__global__ void __launch_bounds__(128) kb_collisions(const fb_disk_dev *ds, const int4 *items) {
+  const int4 w = items[blockIdx.x];
+  const fb_disk_dev &D = ds[w.x];
+  if (D.scal_dev->skip) return;
+  b_collisions<T, N, S>(D, dims_of(D), geo_of<double>(D.geomd), D.scal_dev, make_uint3(w.y, w.z, w.w));
 }
 
 template <typename T, int DIR, int COL_NS, typename S>
@@ -202,6 +210,7 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
         break;
       case ST_BND_Z: g = D.is3d ? dim3((nx + BND_BX - 1) / BND_BX, sy, 6) : dim3(0); break;
       case ST_BND_Y: g = dim3((nx + BND_BX - 1) / BND_BX, 6, sz); break;
+      case ST_COLL: g = D.nfluids > 1 ? dim3((nx + 127) / 128, sy - 1, D.is3d ? sz - 1 : 1) : dim3(0); break;
       case ST_Z4: case ST_Z8: case ST_Z16: {
         const int ns = 4 << (st - ST_Z4);
         g = D.is3d && disk_ns(D) == ns ? dim3((nx + COL_BX - 1) / COL_BX, sy - 1, (nz + 1 + ns - 1) / ns) : dim3(0);
@@ -287,6 +296,19 @@ static int launch_step(fb_batch *B, double DT) {
     if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 1, 1);
     kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 1, 0);
     pmark(st, "bnd_vtemp");
+  }
+  if (nf > 1 && B->nitems[ST_COLL]) {  // implicit drag between the fluids
+    const int4 *it = B->items[ST_COLL];
+    switch (nf) {
+      case 2: kb_collisions<T, 2, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
+      case 3: kb_collisions<T, 3, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
+      case 4: kb_collisions<T, 4, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
+      case 5: kb_collisions<T, 5, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
+      case 6: kb_collisions<T, 6, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
+      case 7: kb_collisions<T, 7, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
+      default: kb_collisions<T, 8, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
+    }
+    pmark(st, "collisions");
   }
   for (int f = 0; f < nf; f++) {
     if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);

@@ -72,6 +72,9 @@ typedef struct {
   double *ramps;          /* Stockholm ramps: [sy] radial, [sz] zmed, [sz] zmin */
   int tile_cx;            /* azimuthal sweep cells per thread (0: default) */
   int tile_ns;            /* column sweep segment length (0: default) */
+  /* collision rates between the fluids, alpha[p + o * nfluids] (ColRate,
+     colrate.c:10-23): alpha[0 + f n] = alpha[f + 0 n] = 1/St of dust fluid f */
+  double alpha[FB_MAXFLUIDS * FB_MAXFLUIDS];
 } fb_disk_dev;
 
 /* Launchers (fb_kernels_f64.cu / fb_kernels_f32.cu). Return cudaError_t. */
@@ -82,7 +85,8 @@ typedef struct {
   int fb_launch_bnd_##SUF(const fb_disk_dev *d, int fluid, int vtemp, void *stream); \
   int fb_launch_sweep_cols_##SUF(const fb_disk_dev *d, int fluid, void *stream);    \
   int fb_launch_sweep_x_##SUF(const fb_disk_dev *d, int fluid, void *stream);       \
-  int fb_launch_newvel_##SUF(const fb_disk_dev *d, int fluid, void *stream);
+  int fb_launch_newvel_##SUF(const fb_disk_dev *d, int fluid, void *stream);        \
+  int fb_launch_collisions_##SUF(const fb_disk_dev *d, void *stream);
 
 FB_DECL_LAUNCHERS(f64)
 FB_DECL_LAUNCHERS(f32)

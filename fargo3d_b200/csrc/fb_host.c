@@ -26,7 +26,7 @@
 #define MSTAR 1.0
 #define R0 1.0
 #define SMALLTIME (1e-10 * sqrt(R0 * R0 * R0 / (G * MSTAR)))
-#define MAXALLOC 96
+#define MAXALLOC 1024  /* device allocations per disk: geometry, tables, 8 fluids x 30 fields */
 
 static __thread char g_err[512];
 
@@ -414,6 +414,11 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
   D->d.cfl = p->cfl;
   D->d.stockholm = p->stockholm;
   D->d.nfluids = p->nfluids;
+  /* collision rates (ColRate with feedback, setups/fargo_multifluid/condinit.c:88-94) */
+  for (f = 1; f < p->nfluids; f++) {
+    D->d.alpha[0 + f * p->nfluids] = p->invstokes[f - 1];
+    D->d.alpha[f + 0 * p->nfluids] = p->invstokes[f - 1];
+  }
   D->d.aspectratio = p->aspectratio; D->d.sigmaslope = p->sigmaslope; D->d.flaringindex = p->flaringindex;
   D->ncell = nc = D->d.stride * D->d.sz;
   D->xmin = calloc(p->nx + 1, 8); D->ymin = calloc(D->d.sy + 1, 8); D->zmin = calloc(D->d.sz + 1, 8);
@@ -603,6 +608,11 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
     mark(D, "sources");
     LCH(LAUNCH(bnd, &D->d, f, 1, D->stream));
     mark(D, "bnd_vtemp");
+  }
+  /* implicit drag between the fluids on V_temp (main.c:412-414) */
+  if (D->p.nfluids > 1) {
+    LCH(LAUNCH(collisions, &D->d, D->stream));
+    mark(D, "collisions");
   }
   /* Transport (algogas.c:135-159) */
   for (f = 0; f < D->p.nfluids; f++) {

@@ -1172,6 +1172,109 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
   }
 }
 
+// ---------------------------------------------------------------------------
+// Implicit drag between the N fluids (Collisions(dt, 1): collisions.c:10-189,
+// collision_kernel.h:11-94, gauss.h:1-45), on V_temp after every fluid's
+// sources.  One thread per cell (i, j >= 1[, k >= 1]) solves, for each
+// direction, the N x N system of the face between the cell and its lower
+// neighbour along that direction:
+//   M[o][p] (o != p) = -dt W a[p][o] rho_p / rho_o  (p > o),  -dt W a[p][o]  (p < o)
+//   M[p][p]          = 1 + dt W sum_{q != p} (q > p ? a[q][p] rho_q / rho_p : a[q][p])
+// with face-averaged densities, W = sqrt(G M / r^3) at Ymed (x, z faces) or
+// Ymin (y faces), by Gaussian elimination with the reference's row pivoting
+// (the search compares |m| with the signed value last kept) and back
+// substitution, in the reference's operation order.  The directions touch
+// different velocity fields, so solving them in one thread per cell gives the
+// reference's direction-by-direction result.
+template <typename T, int N, typename S>
+__device__ __forceinline__ void b_collisions(const fb_disk_dev &D, Dims m, Geo<double> gd, const fb_scalars *scp,
+                                             uint3 bid) {
+  const int i = bid.x * blockDim.x + threadIdx.x;
+  const int j = 1 + bid.y, k = m.is3d ? 1 + bid.z : 0;
+  if (i >= m.nx) return;
+  const T dt = (T)scp->dt;
+  const long long l = m.l(i, j, k);
+  const int ndir = m.is3d ? 3 : 2;
+  for (int dir = 0; dir < ndir; dir++) {
+    const long long lm = dir == 0 ? (i > 0 ? l - 1 : l + (m.nx - 1)) : (dir == 1 ? l - m.pitch : l - m.stride);
+    const T y = (T)(dir == 1 ? ld(gd.ymin + j) : ld(gd.ymed + j));
+    const T w = sqrt((T)1.0 / (y * y * y));  // G = MSTAR = 1 (fondam.h)
+    T rf[N], M[N * N], b[N];
+#pragma unroll
+    for (int f = 0; f < N; f++) {
+      const S *r = (const S *)D.fl[f].rho;
+      rf[f] = (T)0.5 * ((T)r[l] + (T)r[lm]);
+    }
+#pragma unroll
+    for (int o = 0; o < N; o++) {
+#pragma unroll
+      for (int p = 0; p < N; p++) {
+        if (p != o) {
+          if (p > o) M[p + o * N] = -dt * w * (T)D.alpha[p + o * N] * rf[p] / rf[o];
+          else M[p + o * N] = -dt * w * (T)D.alpha[p + o * N];
+        } else {
+          T sum = (T)0.0;
+#pragma unroll
+          for (int q = 0; q < N; q++) {
+            if (q == p) continue;
+            if (q > p) sum += (T)D.alpha[q + p * N] * rf[q] / rf[p];
+            else sum += (T)D.alpha[q + p * N];
+          }
+          M[p + p * N] = (T)1.0 + dt * w * sum;
+        }
+      }
+      const S *v = (const S *)(dir == 0 ? D.fl[o].vxt : (dir == 1 ? D.fl[o].vyt : D.fl[o].vzt));
+      b[o] = (T)v[l];
+    }
+#pragma unroll
+    for (int ir = 0; ir < N - 1; ir++) {
+      T mx = (T)-1;
+      int irm = ir;
+#pragma unroll
+      for (int ir2 = ir; ir2 < N; ir2++)
+        if (fabs(M[ir + ir2 * N]) >= mx) { mx = M[ir + ir2 * N]; irm = ir2; }
+      if (irm != ir) {
+#pragma unroll
+        for (int ic = 0; ic < N; ic++) {
+          // row exchange by predicated copies keeps the matrix in registers
+          T a = M[ic + ir * N];
+#pragma unroll
+          for (int r2 = ir + 1; r2 < N; r2++)
+            if (r2 == irm) { M[ic + ir * N] = M[ic + r2 * N]; M[ic + r2 * N] = a; }
+        }
+        T a = b[ir];
+#pragma unroll
+        for (int r2 = ir + 1; r2 < N; r2++)
+          if (r2 == irm) { b[ir] = b[r2]; b[r2] = a; }
+      }
+#pragma unroll
+      for (int ir2 = ir + 1; ir2 < N; ir2++) {
+        const T factor = M[ir + ir2 * N] / M[ir + ir * N];
+#pragma unroll
+        for (int ic = 0; ic < N; ic++) M[ic + ir2 * N] -= M[ic + ir * N] * factor;
+        b[ir2] -= b[ir] * factor;
+      }
+    }
+#pragma unroll
+    for (int ir = N - 1; ir > -1; ir--) {
+#pragma unroll
+      for (int ic = N - 1; ic > ir; ic--) b[ir] -= M[ic + ir * N] * b[ic];
+      b[ir] /= M[ir + ir * N];
+    }
+#pragma unroll
+    for (int o = 0; o < N; o++) {
+      S *v = (S *)(dir == 0 ? D.fl[o].vxt : (dir == 1 ? D.fl[o].vyt : D.fl[o].vzt));
+      v[l] = (S)b[o];
+    }
+  }
+}
+
+template <typename T, int N, typename S>
+__global__ void __launch_bounds__(128) k_collisions(const fb_disk_dev D, Dims m, Geo<double> gd,
+                                                    const fb_scalars *scp) {
+  b_collisions<T, N, S>(D, m, gd, scp, blockIdx);
+}
+
 // shared memory of b_sweep_x2 for a ring of nx cells (rpc rings per CTA)
 __host__ __device__ inline size_t sweep_x2_smem(int nx, int C, int nt, int nq, size_t esz) {
   const int rpc = nt / (nx / C);

@@ -197,6 +197,25 @@ static int launch_newvel(const fb_disk_dev *d, int f, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+// implicit drag of all fluids (fluid count 2..FB_MAXFLUIDS)
+template <typename T, typename S>
+static int launch_collisions(const fb_disk_dev *d, cudaStream_t st) {
+  Dims m = dims_of(*d);
+  Geo<double> gd = geo_of<double>(d->geomd);
+  dim3 g((m.nx + 127) / 128, m.sy - 1, m.is3d ? m.sz - 1 : 1);
+  switch (d->nfluids) {
+    case 2: k_collisions<T, 2, S><<<g, 128, 0, st>>>(*d, m, gd, d->scal_dev); break;
+    case 3: k_collisions<T, 3, S><<<g, 128, 0, st>>>(*d, m, gd, d->scal_dev); break;
+    case 4: k_collisions<T, 4, S><<<g, 128, 0, st>>>(*d, m, gd, d->scal_dev); break;
+    case 5: k_collisions<T, 5, S><<<g, 128, 0, st>>>(*d, m, gd, d->scal_dev); break;
+    case 6: k_collisions<T, 6, S><<<g, 128, 0, st>>>(*d, m, gd, d->scal_dev); break;
+    case 7: k_collisions<T, 7, S><<<g, 128, 0, st>>>(*d, m, gd, d->scal_dev); break;
+    case 8: k_collisions<T, 8, S><<<g, 128, 0, st>>>(*d, m, gd, d->scal_dev); break;
+    default: return (int)cudaErrorInvalidValue;
+  }
+  return (int)cudaGetLastError();
+}
+
 }  // namespace fb
 
 #define FB_CAT2(a, b) a##_##b
@@ -223,5 +242,8 @@ int FB_CAT(fb_launch_sweep_x, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) 
 }
 int FB_CAT(fb_launch_newvel, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
   return fb::launch_newvel<FB_REAL_TR, FB_STORE>(d, fluid, (cudaStream_t)s);
+}
+int FB_CAT(fb_launch_collisions, FB_SUF)(const fb_disk_dev *d, void *s) {
+  return fb::launch_collisions<FB_REAL, FB_STORE>(d, (cudaStream_t)s);
 }
 }

@@ -93,6 +93,17 @@ def config_fargo2d(nx: int = 384, ny: int = 128, seed: int = 0) -> DiskConfig:
     return DiskConfig(nx=nx, ny=ny, seed=seed)
 
 
+def config_multifluid(nx: int = 768, ny: int = 256, nfluids: int = 5,
+                      invstokes=(1000.0, 100.0, 10.0, 1.0), seed: int = 0) -> DiskConfig:
+    """2D cylindrical gas disk with nfluids - 1 dust species coupled by
+    implicit drag (setups/fargo_multifluid with DRAGFORCE + STOKESNUMBER):
+    1/St per dust species `invstokes`, dust-to-gas ratio 0.01 / (nfluids - 1)
+    per species, fixed frame, no indirect term, constant nu = 1e-5, planet
+    q = 1e-3 at r = 1."""
+    return DiskConfig(nx=nx, ny=ny, sigma0=1e-4, frame="F", omegaframe=0.0, indirect_term=False,
+                      nfluids=nfluids, invstokes=tuple(invstokes[:nfluids - 1]), seed=seed)
+
+
 def config_p3disof(nx: int = 512, ny: int = 256, nz: int = 48, seed: int = 0) -> DiskConfig:
     """3D spherical isothermal disk (setups/p3disof): colatitude pi/2 +- 0.15,
     rho ~ r^-1.5 with a vertical hydrostatic profile, h = 0.05, no flaring,
@@ -135,8 +146,8 @@ def initial_state(cfg: DiskConfig, fluid: int = 0):
     (1 + noise U(-1,1)), v_phi from the pressure-supported rotation curve and
     v_r = 0.  3D: setups/p3disof/condinit.c:21-50 (FlaringIndex = 0 branch),
     with the same multiplicative density noise.  Dust fluids (fluid > 0) get
-    eps = 0.01 / (nfluids - 1) times the gas density, the gas velocity and no
-    pressure (cs = 0)."""
+    eps = 0.01 / (nfluids - 1) times the gas density, the Keplerian velocity
+    without pressure support (2D) and no pressure (cs = 0)."""
     rng = np.random.default_rng(cfg.seed * 1000 + fluid)
     nzs, nys, nxs = cfg.shape
     _, _, _, xmed, ymed, zmed = geometry(cfg)
@@ -165,9 +176,14 @@ def initial_state(cfg: DiskConfig, fluid: int = 0):
         vy = np.zeros(cfg.shape)
         vz = np.zeros(cfg.shape)
     if fluid > 0:
+        # dust (setups/fargo_multifluid/condinit.c:38-44): eps times the gas
+        # density, Keplerian azimuthal velocity without pressure support, no
+        # radial velocity, no sound speed
         eps = 0.01 / max(cfg.nfluids - 1, 1)
         rho = rho * eps
         cs = np.zeros(cfg.shape)
+        if not cfg.is3d:
+            vx = omega * r - omegaframe * r
     return (np.ascontiguousarray(rho), np.ascontiguousarray(vx), np.ascontiguousarray(vy),
             np.ascontiguousarray(vz), np.ascontiguousarray(cs))
 

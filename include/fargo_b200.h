@@ -54,7 +54,7 @@ typedef struct {
   int pl_feeldisk[FB_MAXPLANETS], pl_feelothers[FB_MAXPLANETS];
   double eccentricity, inclination;
   int nfluids;                 /* 1: gas; >1: gas + dust with implicit drag      */
-  double invstokes[FB_MAXFLUIDS];
+  double invstokes[FB_MAXFLUIDS];   /* drag (STOKESNUMBER): [f-1] = 1/St of dust fluid f */
   int stockholm;               /* STOCKHOLM damping                             */
 } fb_params;
 

@@ -1295,8 +1295,7 @@ static void stockholm(fo_disk *d, double dt) {
 }
 
 /* ------------------------------------------------------------------------- */
-/* Multifluid implicit drag: restated in fo_collisions below (filled in with
- * the multifluid configuration). */
+/* Multifluid implicit drag (collisions below). */
 static void collisions(fo_disk *d, double dt);
 
 /* ------------------------------------------------------------------------- */
@@ -1491,4 +1490,82 @@ double fo_mass(const fo_disk *d, int f) {
   return s;
 }
 
-static void collisions(fo_disk *d, double dt) { (void)d; (void)dt; abort(); }
+/* Implicit drag between the fluids, STOKESNUMBER form (collisions.c:10-189,
+ * collision_kernel.h:11-94, gauss.h:1-45), applied to V_temp after the
+ * sources of every fluid.  For each direction in turn (x, then y, then z) and
+ * each face l of the range j >= 1 (k >= 1 in 3D), the velocities b[o] of the
+ * N fluids at that face solve M b_new = b_old with
+ *   M[o][p] (o != p) = -dt W a[p][o] rho_p / rho_o   if p > o
+ *                      -dt W a[p][o]                 otherwise
+ *   M[p][p]          = 1 + dt W sum_{q != p} (q > p ? a[q][p] rho_q / rho_p : a[q][p])
+ * where rho_* are face averages 0.5 (rho[l] + rho[l - 1 cell along the
+ * direction]), W the Keplerian frequency at the face's radius (Ymed for the
+ * x and z faces, Ymin for the y faces: collision_kernel.h:16-18) and
+ * a[p][o] the collision-rate matrix (alpha[p + o N]),
+ * filled as ColRate does (colrate.c:10-23): a[0][f] = a[f][0] = 1/St_f.  The
+ * system is solved by Gaussian elimination with the reference's row pivoting
+ * (the pivot search compares |m| with the signed value last kept, gauss.h:7-13)
+ * and back substitution; the operation order is the reference's, so the
+ * result is bit-identical. */
+static void collisions(fo_disk *d, double dt) {
+  const int N = d->p.nfluids;
+  double alpha[FO_MAXFLUIDS * FO_MAXFLUIDS] = {0};
+  double m[FO_MAXFLUIDS * FO_MAXFLUIDS], b[FO_MAXFLUIDS];
+  double *rho[FO_MAXFLUIDS], *vel[FO_MAXFLUIDS];
+  int dir, f, i, j, k, o, p, q, ir, ir2, ir_max = 0, ic;
+  for (f = 1; f < N; f++) alpha[0 + f * N] = alpha[f + 0 * N] = d->p.invstokes[f - 1];
+  for (f = 0; f < N; f++) rho[f] = d->fl[f].rho;
+  for (dir = 0; dir < (d->is3d ? 3 : 2); dir++) {
+    for (f = 0; f < N; f++) vel[f] = dir == 0 ? d->fl[f].vxt : (dir == 1 ? d->fl[f].vyt : d->fl[f].vzt);
+    for (k = d->is3d ? 1 : 0; k < (d->is3d ? d->sz : 1); k++)
+      for (j = 1; j < d->sy; j++)
+        for (i = 0; i < d->nx; i++) {
+          const long l = L(i, j, k);
+          const long lm = dir == 0 ? lxm_(d, i, l) : (dir == 1 ? l - d->pitch : l - d->stride);
+          const double y = dir == 1 ? Ymin(j) : Ymed(j);
+          const double w = sqrt(G * MSTAR / (y * y * y));
+          double rho_p, rho_o, rho_q, sum, mx, tmp, factor;
+          for (o = 0; o < N; o++) {
+            for (p = 0; p < N; p++) {
+              rho_p = 0.5 * (rho[p][l] + rho[p][lm]);
+              if (p != o) {
+                rho_o = 0.5 * (rho[o][l] + rho[o][lm]);
+                if (p > o) m[p + o * N] = -dt * w * alpha[p + o * N] * rho_p / rho_o;
+                else m[p + o * N] = -dt * w * alpha[p + o * N];
+              } else {
+                sum = 0.0;
+                for (q = 0; q < N; q++) {
+                  if (q == p) continue;
+                  rho_q = 0.5 * (rho[q][l] + rho[q][lm]);
+                  if (q > p) sum += alpha[q + p * N] * rho_q / rho_p;
+                  else sum += alpha[q + p * N];
+                }
+                m[p + p * N] = 1.0 + dt * w * sum;
+              }
+            }
+            b[o] = vel[o][l];
+          }
+          for (ir = 0; ir < N - 1; ir++) {
+            mx = -1;
+            for (ir2 = ir; ir2 < N; ir2++)
+              if (fabs(m[ir + ir2 * N]) >= mx) { mx = m[ir + ir2 * N]; ir_max = ir2; }
+            if (ir_max != ir) {
+              for (ic = 0; ic < N; ic++) {
+                tmp = m[ic + ir * N]; m[ic + ir * N] = m[ic + ir_max * N]; m[ic + ir_max * N] = tmp;
+              }
+              tmp = b[ir]; b[ir] = b[ir_max]; b[ir_max] = tmp;
+            }
+            for (ir2 = ir + 1; ir2 < N; ir2++) {
+              factor = m[ir + ir2 * N] / m[ir + ir * N];
+              for (ic = 0; ic < N; ic++) m[ic + ir2 * N] -= m[ic + ir * N] * factor;
+              b[ir2] -= b[ir] * factor;
+            }
+          }
+          for (ir = N - 1; ir > -1; ir--) {
+            for (ic = N - 1; ic > ir; ic--) b[ir] -= m[ic + ir * N] * b[ic];
+            b[ir] /= m[ir + ir * N];
+          }
+          for (o = 0; o < N; o++) vel[o][l] = b[o];
+        }
+  }
+}

@@ -44,7 +44,7 @@ typedef struct {
   int pl_feeldisk[FO_MAXPLANETS], pl_feelothers[FO_MAXPLANETS];
   double eccentricity, inclination;
   int nfluids;                 /* 1: gas only; >1: gas + dust, implicit drag       */
-  double invstokes[FO_MAXFLUIDS]; /* STOKESNUMBER drag: 1/St per dust fluid          */
+  double invstokes[FO_MAXFLUIDS]; /* STOKESNUMBER drag: [f-1] = 1/St of dust fluid f */
   int stockholm;               /* STOCKHOLM damping on/off                        */
 } fo_params;
 

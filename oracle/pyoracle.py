@@ -73,6 +73,10 @@ def build():
 
 
 def ref_variant(cfg) -> str:
+    if cfg.nfluids > 1:
+        if cfg.nfluids != 5 or cfg.is3d or cfg.alpha_visc:
+            raise ValueError("the compiled reference has one multifluid variant: 2D, 5 fluids, constant nu")
+        return "mf5"
     if cfg.is3d:
         return "sph3d"
     return "cyl2d_alpha" if cfg.alpha_visc else "cyl2d"

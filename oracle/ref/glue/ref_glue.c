@@ -413,6 +413,11 @@ int ref_create(const fo_params *p) {
     boundary_zmax[f] = bnd_zmax;
 #endif
   }
+#ifdef DRAGFORCE
+  /* the collision rates of setups/fargo_multifluid/condinit.c:88-94, one per
+     dust fluid, with feedback on the gas */
+  for (f = 1; f < NFLUIDS; f++) ColRate(p->invstokes[f - 1], 0, f, YES);
+#endif
   SelectFluid(0);
   g_dtemp = 0.0;
   return 0;

@@ -1,7 +1,7 @@
 """Small parity cases shared by the golden-vector generator and the tests."""
 import math
 
-from fargo3d_b200.setups import DiskConfig, Planet, config_fargo2d, config_p3disof
+from fargo3d_b200.setups import DiskConfig, Planet, config_fargo2d, config_multifluid, config_p3disof
 
 
 def cases():
@@ -20,4 +20,31 @@ def cases():
             planets=[Planet(1.0, 1e-3, False, True), Planet(1.6, 5e-4, False, True)]), 15, 1e30),
         # setups/p3disof flags, 3D spherical
         "sph3d": (config_p3disof(16, 12, 6, seed=5), 6, 1e30),
+        # setups/fargo_multifluid flags: gas + 4 dust species, implicit drag
+        "mf5": (config_multifluid(32, 16, seed=6), 12, 1e30),
     }
+
+
+def _key(f, k):
+    return k if f == 0 else "f%d_%s" % (f, k)
+
+
+def golden_init(g, cfg):
+    """Per-fluid initial states (rho, vx, vy, vz, cs) stored in a golden file."""
+    return [tuple(g[_key(f, k)] for k in ("rho0", "vx0", "vy0", "vz0", "cs")) for f in range(cfg.nfluids)]
+
+
+def golden_out(g, f=0):
+    """Fluid f's state after the golden run."""
+    return {k: g[_key(f, k)] for k in ("rho", "vx", "vy", "vz")}
+
+
+def golden_arrays(init, out):
+    """npz arrays of every fluid's initial and final state."""
+    d = {}
+    for f, (st, o) in enumerate(zip(init, out)):
+        for k, v in zip(("rho0", "vx0", "vy0", "vz0", "cs"), st):
+            d[_key(f, k)] = v
+        for k in ("rho", "vx", "vy", "vz"):
+            d[_key(f, k)] = o[k]
+    return d

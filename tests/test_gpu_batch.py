@@ -133,3 +133,28 @@ def test_fp32_accuracy_after_1000_steps():
         l1 = np.sum(np.abs(st["rho"] - ref["rho"])) / np.sum(np.abs(ref["rho"]))
         assert l1 <= 1e-5, (i, l1)
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_multifluid_drag_matches_oracle(precision):
+    """Gas + 4 dust species with implicit drag, two disks in one batch: every
+    fluid of every member against the FP64 oracle."""
+    import pyoracle
+    from fargo3d_b200 import Batch, config_multifluid
+    cfgs = [config_multifluid(64, 32, seed=81), config_multifluid(128, 48, seed=82)]
+    b = Batch(cfgs, precision)
+    b.load_initial_states()
+    b.run(12)
+    pyoracle.build()
+    for i, c in enumerate(cfgs):
+        out, dts, _ = pyoracle.run(c, 12, "oracle")
+        for f in range(c.nfluids):
+            st = b.state(i, fluid=f)
+            if precision == "fp64":
+                for k in ("rho", "vx", "vy"):
+                    assert rel_linf(st[k], out[f][k]) <= 1e-10, (i, f, k, rel_linf(st[k], out[f][k]))
+            else:
+                l1 = np.sum(np.abs(st["rho"] - out[f]["rho"])) / np.sum(np.abs(out[f]["rho"]))
+                assert l1 <= 1e-5, (i, f, l1)
+    b.close()
