@@ -14,6 +14,8 @@ dataset is involved):
            is measured beside it ("fp64_plain").
   p3disof  one 3D spherical disk 512 x 256 x 48 (plain path, --precision)
   fargo2d  one 2D cylindrical disk 384 x 128 (plain path, --precision)
+  multifluid  one 2D disk 768 x 256 with gas + 4 dust species coupled by
+           implicit drag (plain path, --precision)
   serving  the continuous-batching server: --requests requests (default
            100) arriving as a Poisson process (--rate, 20/s), sizes
            {256x64, 512x128, 1024x256, 2048x512} weighted {.4,.3,.2,.1}, each
@@ -81,6 +83,10 @@ def workload(name: str, rank: int = 0):
         return [config_fargo2d(384, 128, seed=rank)], "fargo2d 384x128 (2D cylindrical, 1 planet, nu=1e-5)"
     if name == "p3disof":
         return [config_p3disof(512, 256, 48, seed=rank)], "p3disof 512x256x48 (3D spherical, 1 planet, nu=1e-5)"
+    if name == "multifluid":
+        from fargo3d_b200 import config_multifluid
+        return [config_multifluid(768, 256, seed=rank)], ("multifluid 768x256, gas + 4 dust species (1/St = 1000, "
+                                                          "100, 10, 1), implicit drag, 1 planet")
     if name == "serving":
         from fargo3d_b200 import serving_requests
         return [r.cfg for r in serving_requests(64, seed=rank)], ("serving requests, sizes {256x64, 512x128, "
@@ -146,11 +152,18 @@ class ClockSampler:
 
 
 def read_profile(L, fn, h, *extra):
+    """{launch group: ms summed over its occurrences (one per fluid)}, and the
+    number of occurrences of each group."""
     import ctypes as C
     ms = (C.c_float * 40)()
     names = (C.c_char_p * 40)()
     n = fn(h, *extra, ms, names, 40)
-    return {names[i].decode(): float(ms[i]) for i in range(max(n, 0))}
+    out, count = {}, {}
+    for i in range(max(n, 0)):
+        k = names[i].decode()
+        out[k] = out.get(k, 0.0) + float(ms[i])
+        count[k] = count.get(k, 0) + 1
+    return out, count
 
 
 # --------------------------------------------------------------------------
@@ -234,11 +247,13 @@ def run_ours(args, rank, world, local_rank):
     esz = 8 if precision == "fp64" else 4
     cells = sum(c.active_cells for c in cfgs)
     L = _abi.bind_batch(_abi.lib())
-    inits = [initial_state(c) for c in cfgs]
+    nf = cfgs[0].nfluids
+    inits = [[initial_state(c, f) for f in range(nf)] for c in cfgs]   # [disk][fluid]
     if batched:
         runner = Batch(cfgs, precision, device=local_rank)
-        for i, st in enumerate(inits):
-            runner.set_state(i, *st)
+        for i, sts in enumerate(inits):
+            for f, st in enumerate(sts):
+                runner.set_state(i, *st, fluid=f)
         runner.initialize()
         stream = torch.cuda.ExternalStream(runner.stream)
         runner.run(max(args.warmup, 10))   # includes the graph capture
@@ -246,7 +261,8 @@ def run_ours(args, rank, world, local_rank):
         step_fn = lambda n: runner.run(n)
     else:
         runner = Disk(cfgs[0], precision, device=local_rank)
-        runner.set_state(*inits[0])
+        for f, st in enumerate(inits[0]):
+            runner.set_state(*st, fluid=f)
         runner.initialize()
         stream = torch.cuda.ExternalStream(runner.stream)
         runner.run(args.warmup)
@@ -271,39 +287,44 @@ def run_ours(args, rank, world, local_rank):
     value = cells * args.steps * world / (ms / 1e3)
     # per-launch-group timing of one extra step (dominant kernel, roofline)
     if batched:
-        prof = read_profile(L, L.fb_batch_profile_step, runner._h, 1e30)
+        prof, count = read_profile(L, L.fb_batch_profile_step, runner._h, 1e30)
     else:
         L.fb_disk_profile(runner._h, 1)
         runner.step()
-        prof = read_profile(L, L.fb_disk_profile_read, runner._h)
+        prof, count = read_profile(L, L.fb_disk_profile_read, runner._h)
         L.fb_disk_profile(runner._h, 0)
     prof.pop("host_scalars", None)
-    launches_per_step = sum(KERNELS_PER_GROUP[dim].get(k, 1) for k in prof)
+    count.pop("host_scalars", None)
+    launches_per_step = sum(KERNELS_PER_GROUP[dim].get(k, 1) * count[k] for k in prof)
     dom = max((k for k in prof if LAUNCH_WORDS[dim].get(k, 0) > 0), key=lambda k: prof[k])
     hbm, peak_kind = peaks()
-    dom_bytes = LAUNCH_WORDS[dim][dom] * esz * cells
+    # a group's time covers all its fluids: its words per cell, once per fluid
+    dom_bytes = LAUNCH_WORDS[dim][dom] * esz * cells * (count[dom] if dom not in ("cfl", "rowsum") else nf)
     achieved = dom_bytes / (prof[dom] / 1e3) / 1e9
     runner.close()
     # end-to-end through the public API from pinned host buffers
-    pinned = [[torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in st] for st in inits]
+    pinned = [[[torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in st] for st in sts]
+              for sts in inits]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     if batched:
         r2 = Batch(cfgs, precision, device=local_rank)
-        for i, st in enumerate(pinned):
-            r2.set_state(i, *[p.numpy() for p in st])
+        for i, sts in enumerate(pinned):
+            for f, st in enumerate(sts):
+                r2.set_state(i, *[p.numpy() for p in st], fluid=f)
         r2.initialize()
         r2.run(args.steps)
-        outs = [r2.state(i) for i in range(len(cfgs))]
+        outs = [r2.state(i, fluid=f) for i in range(len(cfgs)) for f in range(nf)]
     else:
         r2 = Disk(cfgs[0], precision, device=local_rank)
-        r2.set_state(*[p.numpy() for p in pinned[0]])
+        for f, st in enumerate(pinned[0]):
+            r2.set_state(*[p.numpy() for p in st], fluid=f)
         r2.initialize()
         r2.run(args.steps)
-        outs = [r2.state()]
+        outs = [r2.state(f) for f in range(nf)]
     t_e2e = time.perf_counter() - t0
     r2.close()
-    nstored = sum(int(np.prod(c.shape)) for c in cfgs)
+    nstored = sum(int(np.prod(c.shape)) for c in cfgs) * nf
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -319,7 +340,8 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
                      "alg_bytes_per_launch": dom_bytes, "launch_ms": prof[dom],
-                     "step_alg_frac": ALG_WORDS[dim] * esz * cells * args.steps / (ms / 1e3) / 1e9 / hbm},
+                     "step_alg_frac": (ALG_WORDS[dim] + (ALG_WORDS[dim] - 1) * (nf - 1)) * esz * cells
+                                      * args.steps / (ms / 1e3) / 1e9 / hbm},
         "launch_ms": prof,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
@@ -346,7 +368,8 @@ def _ref_disk_worker(job):
     except FileNotFoundError:
         d = pyoracle.Disk(cfg, "oracle")
         kind = "port"
-    d.set_state(*initial_state(cfg))
+    for f in range(cfg.nfluids):
+        d.set_state(*initial_state(cfg, f), fluid=f)
     d.initialize()
     t0 = time.time()
     for _ in range(steps):
@@ -398,7 +421,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "p3disof", "fargo2d", "serving"])
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "p3disof", "fargo2d", "multifluid", "serving"])
     ap.add_argument("--requests", type=int, default=100, help="serving: number of requests")
     ap.add_argument("--orbits", type=float, default=0.25, help="serving: orbits per request")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
@@ -414,7 +438,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     cfgs, wname = workload(args.workload, 0)
-    auto = {"batched": 6, "p3disof": 2, "fargo2d": 300, "serving": 6}[args.workload]
+    auto = {"batched": 6, "p3disof": 2, "fargo2d": 300, "multifluid": 20, "serving": 6}[args.workload]
     cpu_steps = args.cpu_steps or auto
     if args.impl == "reference":
         if rank != 0:
