@@ -649,6 +649,46 @@ int fb_disk_get_scalars(fb_disk *D, double *o) {
   return FB_OK;
 }
 
+/* The planetary system (Sys of psys.c): positions, velocities and masses of
+ * the n planets, and the frame rotation.  Setting it replaces the circular
+ * orbits built from pl_dist at creation, e.g. when a running simulation hands
+ * its state over; getting it keeps the caller's copy current for outputs. */
+int fb_disk_set_planets(fb_disk *D, int n, const double *x, const double *y, const double *z, const double *vx,
+                        const double *vy, const double *vz, const double *mass, double omegaframe,
+                        double omegaframe0) {
+  int i;
+  if (!D || n != D->ps.np || (n > 0 && (!x || !y || !z || !vx || !vy || !vz || !mass)))
+    return fail(FB_ERR_ARG, "planet count %d does not match the disk's %d", n, D ? D->ps.np : -1);
+  for (i = 0; i < n; i++) {
+    D->ps.px[i] = x[i]; D->ps.py[i] = y[i]; D->ps.pz[i] = z[i];
+    D->ps.pvx[i] = vx[i]; D->ps.pvy[i] = vy[i]; D->ps.pvz[i] = vz[i];
+    D->ps.pmass[i] = mass[i];
+  }
+  D->ps.omegaframe = omegaframe;
+  D->ps.omegaframe0 = omegaframe0;
+  fb_psys_fill_scalars(&D->ps, &D->sc);
+  D->sc.omegaframe = omegaframe;
+  D->sc.omegaframe0 = omegaframe0;
+  return FB_OK;
+}
+
+int fb_disk_get_planets(fb_disk *D, int n, double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                        double *mass, double *omegaframe) {
+  int i;
+  if (!D || n != D->ps.np) return fail(FB_ERR_ARG, "planet count mismatch");
+  for (i = 0; i < n; i++) {
+    if (x) x[i] = D->ps.px[i];
+    if (y) y[i] = D->ps.py[i];
+    if (z) z[i] = D->ps.pz[i];
+    if (vx) vx[i] = D->ps.pvx[i];
+    if (vy) vy[i] = D->ps.pvy[i];
+    if (vz) vz[i] = D->ps.pvz[i];
+    if (mass) mass[i] = D->ps.pmass[i];
+  }
+  if (omegaframe) *omegaframe = D->ps.omegaframe;
+  return FB_OK;
+}
+
 int fb_disk_device_fields(fb_disk *D, int f, void *ptrs[5], size_t *esz) {
   if (!D || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
   ptrs[0] = D->d.fl[f].rho; ptrs[1] = D->d.fl[f].vx; ptrs[2] = D->d.fl[f].vy;

@@ -81,16 +81,18 @@ __device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i
 // (XMAX - XMIN), accumulated sequentially in i as the reference does, one
 // lane per ring; the rings' rows are staged through shared memory so that
 // global loads stay coalesced.  32 rings per CTA of 256 threads.
-template <typename T, bool ORDERED, typename S = T>
+template <typename T, bool ORDERED, typename S = T, int R = 32>
 __device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const S *__restrict__ v,
                                                  double *__restrict__ out, double xlen, uint3 bid) {
-  constexpr int R = 32, CH = 128;
+  // R rings per CTA of 256 threads: 32 for meshes with many rings, 8 where
+  // the rings are few (2D) and 32 per CTA would leave most SMs idle
+  constexpr int CH = 128;
   __shared__ double buf[R][CH + 1];
   const int nring = m.sy * m.sz;
   const int r0 = bid.x * R;
   const int tid = threadIdx.x;
   double acc = 0.0;
-  const int myring = r0 + (tid & 31);
+  const int myring = r0 + (tid & (R - 1));
   for (int c0 = 0; c0 < m.nx; c0 += CH) {
     const int cw = min(CH, m.nx - c0);
     for (int e = tid; e < R * CH; e += blockDim.x) {
@@ -110,10 +112,10 @@ __device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const S *__rest
         for (int ii = 0; ii < cw; ii++) acc = acc + buf[tid][ii];
       }
     } else {
-      // warp w sums rings 4w..4w+3 with a shuffle tree (order-free path)
+      // warp w sums rings (R/8)w .. (R/8)(w+1)-1 with a shuffle tree (order-free path)
       const int w = tid >> 5, lane = tid & 31;
-      for (int q = 0; q < 4; q++) {
-        const int rr = w * 4 + q;
+      for (int q = 0; q < R / 8; q++) {
+        const int rr = w * (R / 8) + q;
         double s = 0.0;
         for (int ii = lane; ii < cw; ii += 32) s += buf[rr][ii];
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -127,10 +129,10 @@ __device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const S *__rest
     out[myring] = tot / xlen;
   }
 }
-template <typename T, bool ORDERED, typename S = T>
+template <typename T, bool ORDERED, typename S = T, int R = 32>
 __global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const S *__restrict__ v,
                                                  double *__restrict__ out, double xlen) {
-  b_rowsum<T, ORDERED, S>(m, gd, v, out, xlen, blockIdx);
+  b_rowsum<T, ORDERED, S, R>(m, gd, v, out, xlen, blockIdx);
 }
 
 // ---------------------------------------------------------------------------

@@ -80,6 +80,17 @@ int fb_disk_step(fb_disk *d, double dt_interval, double *dt_out);
 /* [0] PhysicalTime [1] OMEGAFRAME [2] last dt [3..6] planet 0 x, y, vx, vy [7] Domega */
 int fb_disk_get_scalars(fb_disk *d, double out8[8]);
 
+/* The planetary system and frame rotation (Sys, OMEGAFRAME and the initial
+ * OMEGAFRAME0 of main.c:242; psys.c): set
+ * replaces the circular orbits built from pl_dist (a running simulation
+ * handing over its state), get reads the current one back.  n must equal
+ * nplanets. */
+int fb_disk_set_planets(fb_disk *d, int n, const double *x, const double *y, const double *z, const double *vx,
+                        const double *vy, const double *vz, const double *mass, double omegaframe,
+                        double omegaframe0);
+int fb_disk_get_planets(fb_disk *d, int n, double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                        double *mass, double *omegaframe);
+
 /* Device pointers of one fluid's state (rho, vx, vy, vz, cs) and the element
  * size, for callers that keep their inputs on the device. */
 int fb_disk_device_fields(fb_disk *d, int fluid, void *ptrs5[5], size_t *elem_size);

@@ -72,6 +72,14 @@ def build():
         subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref], check=True)
 
 
+def build_dropin():
+    """The drop-in variants of the reference build (needs libfargo_b200.so
+    and the reference tree)."""
+    ref = os.environ.get("FARGO_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "src")):
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref, "dropin"], check=True)
+
+
 def ref_variant(cfg) -> str:
     if cfg.nfluids > 1:
         if cfg.nfluids != 5 or cfg.is3d or cfg.alpha_visc:
@@ -90,7 +98,9 @@ def _ptr(a):
 
 
 class Disk:
-    """One disk advanced by the oracle ('oracle') or the reference ('ref')."""
+    """One disk advanced by the oracle ('oracle'), the reference ('ref'), or
+    the reference's step loop handed to the B200 library through the
+    FARGO3D-side drop-in binding ('dropin')."""
 
     _libs = {}
 
@@ -98,11 +108,13 @@ class Disk:
         self.cfg, self.kind = cfg, kind
         if kind == "oracle":
             path = os.path.join(HERE, "_build", "libfargo_oracle.so")
+        elif kind == "dropin":
+            path = os.path.join(HERE, "_ref", "libfargo_ref_dropin_%s.so" % ref_variant(cfg))
         else:
             path = os.path.join(HERE, "_ref", "libfargo_ref_%s.so" % ref_variant(cfg))
         if not os.path.exists(path):
             raise FileNotFoundError(path)
-        if kind == "ref":
+        if kind in ("ref", "dropin"):
             # Each reference library holds one disk in its globals (and in
             # function-level statics such as potential.c's alreadycalculated):
             # load a fresh private copy per Disk.  dlopen identifies a library

@@ -7,6 +7,9 @@
  * ref_step() -- Sources, Transport, ComputeVmed, cfl, CflFluidsMin,
  * compute_potential, the planetary system, StockholmBoundary, FillGhosts,
  * boundaries() and all *_cpu kernels.
+ * With -DFB_DROPIN the step instead runs through the drop-in binding
+ * (fargo3d_b200/integration/b200_hydro.c) on the B200 library, from the same
+ * Fields, .par globals and planetary system.
  * What is written here: what FARGO3D's build generates or its start-up does
  * (main.c, ChangeArch, var.c/param.h, the generated boundary functions from
  * std/boundaries.txt + the setup's .bound file, InitSpace/InitSurfaces,
@@ -460,8 +463,24 @@ void ref_initialize(void) {
 }
 
 /* One pass of the DT loop body of main.c:361-448. */
+#ifdef FB_DROPIN
+/* fargo3d_b200/integration/b200_hydro.c: the FARGO3D-side binding of the
+ * B200 library, compiled into this build in place of the step's body */
+void B200_HydroStep(real DT_interval, real *dt);
+void B200_Sync(void);
+#endif
+
 double ref_step(double DTint) {
   real dt;
+#ifdef FB_DROPIN
+  B200_HydroStep(DTint, &dt);   /* attaches to the Fields on its first call */
+  PhysicalTime += dt;
+  Timestepcount++;
+  B200_Sync();
+  SelectFluid(0);
+  g_last_dt = dt;
+  return dt;
+#endif
   if (g_dtemp >= DTint) g_dtemp = 0.0;
 #ifdef X
   MULTIFLUID(ComputeVmed(Vx));
