@@ -280,9 +280,8 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms = float(t.item())
+        from fargo3d_b200.shard import max_over_ranks
+        ms = max_over_ranks(ms, device="cuda")   # the job's time is its slowest rank's
         tdist.barrier()
     value = cells * args.steps * world / (ms / 1e3)
     # per-launch-group timing of one extra step (dominant kernel, roofline)
