@@ -269,9 +269,10 @@ static void pmark(cudaStream_t st, const char *name) {
   g_prof->name[g_prof->n++] = name;
 }
 
-// T: compute type of the CFL and source stages; TC, TX, TN: of the column
-// sweeps, the azimuthal sweep and NewVelocity; S: storage type.
-template <typename T, typename S, typename TC = T, typename TX = T, typename TN = T>
+// T: compute type of the source stage; TC, TX, TN, TF: of the column sweeps,
+// the azimuthal sweep, NewVelocity and the CFL's per-cell limits (its
+// minimum is always FP64); S: storage type.
+template <typename T, typename S, typename TC = T, typename TX = T, typename TN = T, typename TF = T>
 static int launch_step(fb_batch *B, double DT) {
   if (B->nitems[ST_CFL] == 0) return 0;  // no active disk
   configure_sweep_x<TX, S>(B);
@@ -285,7 +286,7 @@ static int launch_step(fb_batch *B, double DT) {
     else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
   }
   pmark(st, "rowsum");
-  for (int f = 0; f < nf; f++) kb_cfl<T, S><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
+  for (int f = 0; f < nf; f++) kb_cfl<TF, S><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
   pmark(st, "cfl");
   kb_scalars<<<(B->n + 63) / 64, 64, 0, st>>>(ds, B->d_psys, B->n, DT);
   pmark(st, "scalars");

@@ -352,7 +352,8 @@ int fb_disk_set_tiles(fb_disk *D, int cx, int ns) {
     /* whole rings per CTA of 256 threads, two buffers of (1 + nq) fields
      * plus the velocity ring, in the sweep's element size: at most 227 KiB */
     size_t rpc = 256 / (D->d.nx / cx), nq = D->d.is3d ? 6 : 4;
-    size_t bytes = rpc * (size_t)D->d.nx * (2 * (1 + nq) + 1) * D->esz;
+    size_t nxp = (size_t)D->d.nx + (D->d.nx >> (D->esz == 4 ? 5 : 4)) + 1; /* padded ring */
+    size_t bytes = rpc * nxp * (2 * (1 + nq) + 1) * D->esz;
     if (bytes > FB_SMEM_MAX)
       return fail(FB_ERR_ARG, "azimuthal chunk %d on Nx = %d needs %zu bytes of shared memory", cx, D->d.nx, bytes);
   }

@@ -16,6 +16,7 @@
 // (including the order implied by its geometry macros), so the FP64
 // instantiation, compiled without FMA contraction, reproduces the CPU build.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -141,6 +142,10 @@ __global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const S 
 // device-wide minimum held as the bit pattern of a positive double.
 __device__ __forceinline__ double dmax2(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double dmax3(double a, double b, double c) {
+  return (((a) > (b) ? (a) : (b)) > (c) ? ((a) > (b) ? (a) : (b)) : (c));
+}
+__device__ __forceinline__ float dmax2(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float dmax3(float a, float b, float c) {
   return (((a) > (b) ? (a) : (b)) > (c) ? ((a) > (b) ? (a) : (b)) : (c));
 }
 
@@ -280,7 +285,10 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   constexpr int W = TX + 2, H = TY + 2;
   __shared__ T s_rho[H][W], s_cs[H][W], s_vx[H][W], s_vy[H][W], s_p[H][W];
   __shared__ double s_pot[H][W];
-  __shared__ T s_txx[H][W], s_tyy[H][W], s_tyx[H][W];
+  // viscous stresses: FP32 arithmetic for FP32 storage (they enter as small
+  // increments; velocity differences are taken exactly in T first), T else
+  using TV = typename std::conditional<(sizeof(S) < sizeof(T)), float, T>::type;
+  __shared__ TV s_txx[H][W], s_tyy[H][W], s_tyx[H][W];
   __shared__ fb_scalars sc;
   const int i0 = bid.x * TX, j0 = FB_NGH + bid.y * TY;
   const int tid = threadIdx.x + threadIdx.y * TX;
@@ -307,35 +315,38 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   }
   __syncthreads();
   if (viscous) {
-    const T nu = (T)sc.nu, alpha = (T)sc.alpha;
+    const TV nu = (TV)sc.nu, alpha = (TV)sc.alpha;
     for (int e = tid; e < H * W; e += TX * TY) {
       const int lj = e / W, li = e - lj * W;
       const int j = j0 - 1 + lj, i = wrapx(i0 - 1 + li, m.nx);
       if (j >= m.sy - 1 || i0 - 1 + li > m.nx) continue;
       // tau_xx, tau_yy at (li in [0,TX], lj in [0,TY]); tau_yx at (li,lj >= 1)
-      T visc = nu, viscm = nu;
+      TV visc = nu, viscm = nu;
       if (m.alpha && lj >= 1 && li >= 1) {
-        const T e0 = s_cs[lj][li], ex = s_cs[lj][li - 1], ey = s_cs[lj - 1][li], exy = s_cs[lj - 1][li - 1];
-        viscm = alpha * (T)0.0625 * (e0 + ex + ey + exy) * (e0 + ex + ey + exy) * ld(g.viscm_j + j);
+        const TV e0 = (TV)s_cs[lj][li], ex = (TV)s_cs[lj][li - 1], ey = (TV)s_cs[lj - 1][li],
+                 exy = (TV)s_cs[lj - 1][li - 1];
+        viscm = alpha * (TV)0.0625 * (e0 + ex + ey + exy) * (e0 + ex + ey + exy) * (TV)ld(g.viscm_j + j);
       }
-      if (m.alpha) visc = alpha * s_cs[lj][li] * s_cs[lj][li] * ld(g.visc_j + j);
+      if (m.alpha) visc = alpha * (TV)s_cs[lj][li] * (TV)s_cs[lj][li] * (TV)ld(g.visc_j + j);
       if (li <= TX && lj <= TY) {
-        const T r = s_rho[lj][li];
-        const T sxi = ld(g.sxi + i), syk = ld(g.syk + 0), sxk = ld(g.sxk + 0);
-        T div_v = 0.0;
-        div_v += (s_vx[lj][li + 1] - s_vx[lj][li]) * ld(g.sxj + j) * sxk;
-        div_v += (s_vy[lj + 1][li] * ld(g.syj + j + 1) * syk * sxi - s_vy[lj][li] * ld(g.syj + j) * syk * sxi);
-        div_v *= (T)(2.0 / 3.0) * ld(g.invvj + j) / (syk * sxi);
-        T txx = visc * r * ((T)2.0 * (s_vx[lj][li + 1] - s_vx[lj][li]) / zsx(m, g, i, j, 0) - div_v);
-        txx += visc * r * (s_vy[lj + 1][li] + s_vy[lj][li]) / ld(g.ymed + j);
+        const TV r = (TV)s_rho[lj][li];
+        const TV sxi = (TV)ld(g.sxi + i), syk = (TV)ld(g.syk + 0), sxk = (TV)ld(g.sxk + 0);
+        TV div_v = 0.0;
+        div_v += (TV)(s_vx[lj][li + 1] - s_vx[lj][li]) * (TV)ld(g.sxj + j) * sxk;
+        div_v += ((TV)s_vy[lj + 1][li] * (TV)ld(g.syj + j + 1) * syk * sxi - (TV)s_vy[lj][li] * (TV)ld(g.syj + j) * syk * sxi);
+        div_v *= (TV)(2.0 / 3.0) * (TV)ld(g.invvj + j) / (syk * sxi);
+        TV txx = visc * r * ((TV)2.0 * (TV)(s_vx[lj][li + 1] - s_vx[lj][li]) / (TV)zsx(m, g, i, j, 0) - div_v);
+        txx += visc * r * (TV)(s_vy[lj + 1][li] + s_vy[lj][li]) / (TV)ld(g.ymed + j);
         s_txx[lj][li] = txx;
-        s_tyy[lj][li] = visc * r * ((T)2.0 * (s_vy[lj + 1][li] - s_vy[lj][li]) / (ld(g.ymin + j + 1) - ld(g.ymin + j)) - div_v);
+        s_tyy[lj][li] = visc * r * ((TV)2.0 * (TV)(s_vy[lj + 1][li] - s_vy[lj][li]) /
+                                    (TV)(ld(g.ymin + j + 1) - ld(g.ymin + j)) - div_v);
       }
       if (li >= 1 && lj >= 1) {
-        s_tyx[lj][li] = viscm * (T)0.25 * (s_rho[lj][li] + s_rho[lj][li - 1] + s_rho[lj - 1][li] + s_rho[lj - 1][li - 1]) *
-                        ((s_vy[lj][li] - s_vy[lj][li - 1]) * ld(g.invdiffxmed + i) / ld(g.ymin + j) +
-                         (s_vx[lj][li] - s_vx[lj - 1][li]) / (ld(g.ymed + j) - ld(g.ymed + j - 1)) -
-                         (T)0.5 * (s_vx[lj][li] + s_vx[lj - 1][li]) / ld(g.ymin + j));
+        s_tyx[lj][li] = viscm * (TV)0.25 *
+                        (TV)(s_rho[lj][li] + s_rho[lj][li - 1] + s_rho[lj - 1][li] + s_rho[lj - 1][li - 1]) *
+                        ((TV)(s_vy[lj][li] - s_vy[lj][li - 1]) * (TV)ld(g.invdiffxmed + i) / (TV)ld(g.ymin + j) +
+                         (TV)(s_vx[lj][li] - s_vx[lj - 1][li]) / (TV)(ld(g.ymed + j) - ld(g.ymed + j - 1)) -
+                         (TV)0.5 * (TV)(s_vx[lj][li] + s_vx[lj - 1][li]) / (TV)ld(g.ymin + j));
       }
     }
     __syncthreads();
@@ -365,11 +376,15 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   ay -= (T)((s_pot[lj][li] - s_pot[lj - 1][li]) * dt / (double)(ym - ymm));
   if (viscous) {
     // addviscosity_cyl (addviscosity_cyl.c:106-124)
-    ax += (T)2.0 * (s_txx[lj][li] - s_txx[lj][li - 1]) * izx / ((r + rxm)) * (T)dt;
-    ax += (T)2.0 * (yip * yip * s_tyx[lj + 1][li] - yi * yi * s_tyx[lj][li]) / ((yip - yi) * ym * ym * (rxm + r)) * (T)dt;
-    ay += (T)2.0 * (ym * s_tyy[lj][li] - ymm * s_tyy[lj - 1][li]) / ((ym - ymm) * (r + rym) * yi) * (T)dt;
-    ay += (T)2.0 * (s_tyx[lj][li + 1] - s_tyx[lj][li]) / ((ld(g.xmin + i + 1) - ld(g.xmin + i)) * yi * (r + rym)) * (T)dt;
-    ay -= (s_txx[lj][li] + s_txx[lj - 1][li]) / (yi * (r + rym)) * (T)dt;
+    const TV vr = (TV)r, vrxm = (TV)rxm, vrym = (TV)rym, vizx = (TV)izx, vdt = (TV)dt;
+    const TV vym = (TV)ym, vymm = (TV)ymm, vyi = (TV)yi, vyip = (TV)yip;
+    ax += (T)((TV)2.0 * (s_txx[lj][li] - s_txx[lj][li - 1]) * vizx / ((vr + vrxm)) * vdt);
+    ax += (T)((TV)2.0 * (vyip * vyip * s_tyx[lj + 1][li] - vyi * vyi * s_tyx[lj][li]) /
+              ((vyip - vyi) * vym * vym * (vrxm + vr)) * vdt);
+    ay += (T)((TV)2.0 * (vym * s_tyy[lj][li] - vymm * s_tyy[lj - 1][li]) / ((vym - vymm) * (vr + vrym) * vyi) * vdt);
+    ay += (T)((TV)2.0 * (s_tyx[lj][li + 1] - s_tyx[lj][li]) /
+              ((TV)(ld(g.xmin + i + 1) - ld(g.xmin + i)) * vyi * (vr + vrym)) * vdt);
+    ay -= (T)((s_txx[lj][li] + s_txx[lj - 1][li]) / (vyi * (vr + vrym)) * vdt);
   }
   // SubStep2_a / SubStep2_b (substep2_a.c:107-129, substep2_b.c:150-175)
   const T c2 = (T)FB_CVNR;
@@ -1087,6 +1102,11 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
   const int nx = m.nx, tpr = nx / C, rpc = NT / tpr, nf = 1 + nq;
+  // rings in shared memory are padded by one element per 128 bytes, so the
+  // stride-C window reads of a warp fall into distinct banks
+  constexpr int PS = sizeof(T) == 4 ? 5 : 4;
+  const int nxp = nx + (nx >> PS) + 1;
+  auto P = [](int i) { return i + (i >> PS); };
   const int slot = threadIdx.x / tpr, lt = threadIdx.x - slot * tpr, c0 = lt * C;
   const int r = bid.x * rpc + slot;
   const bool active = slot < rpc && r < nrings;
@@ -1094,19 +1114,19 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
   S *qg[6] = {q0, q1, q2, q3, q4, q5};
   const double dtd = scp->dt;
   const T dt = (T)dtd;
-  // shared layout: buffers A and B of [slot][field][nx] (field 0 rho, 1.. the
-  // momenta), then the residual-velocity source vxt [slot][nx]
-  const size_t bufsz = (size_t)rpc * nf * nx;
+  // shared layout: buffers A and B of [slot][field][nxp] (field 0 rho, 1.. the
+  // momenta), then the residual-velocity source vxt [slot][nxp]
+  const size_t bufsz = (size_t)rpc * nf * nxp;
   T *bufA = sm, *bufB = sm + bufsz, *svx = sm + 2 * bufsz;
   for (int e = threadIdx.x; e < rpc * nx; e += NT) {
     const int s = e / nx, i = e - s * nx, rr = bid.x * rpc + s;
     if (rr < nrings) {
       const int jj = jlo + rr % nj, kk = m.is3d ? klo + rr / nj : 0;
       const long long l = m.l(i, jj, kk);
-      T *b = bufA + (size_t)s * nf * nx;
-      b[i] = rho[l];
-      for (int q = 0; q < nq; q++) b[(1 + q) * nx + i] = qg[q][l];
-      svx[s * nx + i] = vxt[l];
+      T *b = bufA + (size_t)s * nf * nxp;
+      b[P(i)] = rho[l];
+      for (int q = 0; q < nq; q++) b[(1 + q) * nxp + P(i)] = qg[q][l];
+      svx[s * nxp + P(i)] = vxt[l];
     }
   }
   __syncthreads();
@@ -1116,13 +1136,13 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
   auto zone = [&](int u) -> T { return zsx(m, g, wrap(c0 - 2 + u), j, k); };
   const T sxj = ld(g.sxj + j), sxk = ld(g.sxk + k), ivj = ld(g.invvj + j), syk = ld(g.syk + k);
   for (int pass = 0; pass < 2; pass++) {
-    const T *src = (pass == 0 ? bufA : bufB) + (size_t)sl0 * nf * nx;
-    T *dst = (pass == 0 ? bufB : bufA) + (size_t)sl0 * nf * nx;
+    const T *src = (pass == 0 ? bufA : bufB) + (size_t)sl0 * nf * nxp;
+    T *dst = (pass == 0 ? bufB : bufA) + (size_t)sl0 * nf * nxp;
     if (active) {
       T v[C + 1];
       if (pass == 0) {
 #pragma unroll
-        for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nx + wrap(c0 + f)] - vm);  // residual
+        for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nxp + P(wrap(c0 + f))] - vm);  // residual
       } else {
 #pragma unroll
         for (int f = 0; f <= C; f++) {  // uniform fractional velocity (compute_residual.c:68-73), FP64
@@ -1134,24 +1154,24 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
       }
       T wr[C + 6], rs[C + 1];
 #pragma unroll
-      for (int u = 0; u < C + 6; u++) wr[u] = src[wrap(c0 - 3 + u)];
+      for (int u = 0; u < C + 6; u++) wr[u] = src[P(wrap(c0 - 3 + u))];
       chunk_iface<T, C>(wr, v, zone, dt, pass == 1, rs);
       for (int q = 0; q < nq; q++) {
-        const T *sq = src + (1 + q) * nx;
+        const T *sq = src + (1 + q) * nxp;
         T wq[C + 6], qs[C + 1];
 #pragma unroll
-        for (int u = 0; u < C + 6; u++) wq[u] = sq[wrap(c0 - 3 + u)] / wr[u];  // DivideByRho
+        for (int u = 0; u < C + 6; u++) wq[u] = sq[P(wrap(c0 - 3 + u))] / wr[u];  // DivideByRho
         chunk_iface<T, C>(wq, v, zone, dt, pass == 1, qs);
 #pragma unroll
         for (int u = 0; u < C; u++) {
           const T fl = v[u] * qs[u] * rs[u] - v[u + 1] * qs[u + 1] * rs[u + 1];
-          dst[(1 + q) * nx + c0 + u] = sq[c0 + u] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+          dst[(1 + q) * nxp + P(c0 + u)] = sq[P(c0 + u)] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
         }
       }
 #pragma unroll
       for (int u = 0; u < C; u++) {
         const T fl = v[u] * rs[u] - v[u + 1] * rs[u + 1];
-        dst[c0 + u] = wr[u + 3] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+        dst[P(c0 + u)] = wr[u + 3] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
       }
     }
     __syncthreads();
@@ -1167,10 +1187,10 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
     if (i == 0 && nshift_out) nshift_out[jj + kk * m.sy] = nsh;
     int it = (i - nsh) % nx;
     if (it < 0) it += nx;
-    const T *b = bufA + (size_t)s * nf * nx;
+    const T *b = bufA + (size_t)s * nf * nxp;
     const long long l = m.l(i, jj, kk);
-    rho[l] = b[it];
-    for (int q = 0; q < nq; q++) qg[q][l] = b[(1 + q) * nx + it];
+    rho[l] = b[P(it)];
+    for (int q = 0; q < nq; q++) qg[q][l] = b[(1 + q) * nxp + P(it)];
   }
 }
 
@@ -1280,7 +1300,8 @@ __global__ void __launch_bounds__(128) k_collisions(const fb_disk_dev D, Dims m,
 // shared memory of b_sweep_x2 for a ring of nx cells (rpc rings per CTA)
 __host__ __device__ inline size_t sweep_x2_smem(int nx, int C, int nt, int nq, size_t esz) {
   const int rpc = nt / (nx / C);
-  return (size_t)rpc * nx * (2 * (1 + nq) + 1) * esz;
+  const int nxp = nx + (nx >> (esz == 4 ? 5 : 4)) + 1;  // padded ring (b_sweep_x2)
+  return (size_t)rpc * nxp * (2 * (1 + nq) + 1) * esz;
 }
 
 // the chunk width a ring of nx cells uses with NT threads per CTA (0: none fits)

@@ -230,7 +230,7 @@ int FB_CAT(fb_launch_rowsum, FB_SUF)(const fb_disk_dev *d, int fluid, int which,
   return fb::launch_rowsum<FB_REAL, FB_STORE>(d, fluid, which, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_cfl, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
-  return fb::launch_cfl<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
+  return fb::launch_cfl<FB_REAL_TR, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_sources, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
   return fb::launch_sources<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
