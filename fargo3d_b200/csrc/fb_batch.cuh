@@ -52,8 +52,20 @@ __global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 
            (const S *)F.vz, F.vxmed, scp, D.cfl, D.mindx, (unsigned long long *)D.dtmin, bid);
 }
 
+// resident CTAs per SM the FP32-storage kernels are compiled for (register
+// caps 64 / 64 / 128: measured on the batched 64-disk step, where the
+// latency-bound kernels gain more from occupancy than they lose to spills)
+#ifndef FB_SRC_MINB
+#define FB_SRC_MINB 4
+#endif
+#ifndef FB_SX_MINB32
+#define FB_SX_MINB32 4
+#endif
+#ifndef FB_COL_MINB32
+#define FB_COL_MINB32 4
+#endif
 template <typename T, typename S>
-__global__ void __launch_bounds__(SRC2_TX *SRC2_TY) kb_sources_cyl(const fb_disk_dev *ds, const int4 *items, int f) {
+__global__ void __launch_bounds__(SRC2_TX *SRC2_TY, sizeof(S) == 4 ? FB_SRC_MINB : 1) kb_sources_cyl(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   b_sources_cyl<T, SRC2_TX, SRC2_TY, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), (const S *)F.rho,
                                      (const S *)F.cs, (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, scp,
@@ -87,7 +99,7 @@ __global__ void __launch_bounds__(128) kb_collisions(const fb_disk_dev *ds, cons
 }
 
 template <typename T, int DIR, int COL_NS, typename S>
-__global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? 4 : 1) kb_sweep_col(const fb_disk_dev *ds, const int4 *items, int f) {
+__global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? FB_COL_MINB32 : 1) kb_sweep_col(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   Dims m = dims_of(D);
   const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;
@@ -116,7 +128,7 @@ __global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? 4 : 1) kb_sweep_col(c
 }
 
 template <typename T, int C, typename S>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) kb_sweep_x(const fb_disk_dev *ds, const int4 *items, int f) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? FB_SX_MINB32 : 1) kb_sweep_x(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   Dims m = dims_of(D);
   const bool b = m.is3d;
