@@ -26,8 +26,24 @@ enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_COLL, ST_Z4, ST_Z8,
 constexpr int NXC = 5, NNS = 3;
 
 // tile shapes shared with the one-disk launchers (fb_launch.cuh)
+// CFL_R rings per CFL CTA and NV_R rows per NewVelocity CTA: enough work per
+// CTA to amortise its descriptor loads
+constexpr int CFL_R = 4, NV_R = 4;
 constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_BX = 128, BND_BX = 128,
               NV_BX = 128;
+
+// resident CTAs per SM the FP32-storage kernels are compiled for (register
+// caps 64 / 64 / 128: measured on the batched 64-disk step, where the
+// latency-bound kernels gain more from occupancy than they lose to spills)
+#ifndef FB_SRC_MINB
+#define FB_SRC_MINB 4
+#endif
+#ifndef FB_SX_MINB32
+#define FB_SX_MINB32 4
+#endif
+#ifndef FB_COL_MINB32
+#define FB_COL_MINB32 4
+#endif
 
 #define FB_TILE                                        \
   const int4 w = items[blockIdx.x];                    \
@@ -48,22 +64,20 @@ __global__ void __launch_bounds__(256) kb_rowsum(const fb_disk_dev *ds, const in
 template <typename T, typename S>
 __global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
-  b_cfl<T, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), (const S *)F.rho, (const S *)F.cs, (const S *)F.vx, (const S *)F.vy,
-           (const S *)F.vz, F.vxmed, scp, D.cfl, D.mindx, (unsigned long long *)D.dtmin, bid);
+  // CFL_R rings per CTA, one minimum folded per CTA
+  const Dims m = dims_of(D);
+  const Geo<T> g = geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom);
+  const int k = m.is3d ? FB_NGH + (int)bid.y : 0;
+  double mn = 1e20;
+  for (int r = 0; r < CFL_R; r++) {
+    const int j = FB_NGH + (int)bid.x * CFL_R + r;
+    if (j >= m.ny + FB_NGH) break;
+    mn = fmin(mn, cfl_ring<T, S>(m, g, (const S *)F.rho, (const S *)F.cs, (const S *)F.vx, (const S *)F.vy,
+                                 (const S *)F.vz, F.vxmed, scp, D.cfl, D.mindx, (unsigned long long *)D.dtmin, j, k));
+  }
+  cfl_commit(mn, (unsigned long long *)D.dtmin);
 }
 
-// resident CTAs per SM the FP32-storage kernels are compiled for (register
-// caps 64 / 64 / 128: measured on the batched 64-disk step, where the
-// latency-bound kernels gain more from occupancy than they lose to spills)
-#ifndef FB_SRC_MINB
-#define FB_SRC_MINB 4
-#endif
-#ifndef FB_SX_MINB32
-#define FB_SX_MINB32 4
-#endif
-#ifndef FB_COL_MINB32
-#define FB_COL_MINB32 4
-#endif
 template <typename T, typename S>
 __global__ void __launch_bounds__(SRC2_TX *SRC2_TY, sizeof(S) == 4 ? FB_SRC_MINB : 1) kb_sources_cyl(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
@@ -145,11 +159,16 @@ __global__ void __launch_bounds__(NV_BX) kb_newvel(const fb_disk_dev *ds, const 
   FB_TILE
   Dims m = dims_of(D);
   const bool b = m.is3d;
-  b_newvel<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), (const S *)(b ? F.rho_b : F.rho_a), (const S *)(b ? F.mpx_b : F.mpx),
-              (const S *)(b ? F.mmx_b : F.mmx), (const S *)(b ? F.mpy_b : F.mpy), (const S *)(b ? F.mmy_b : F.mmy),
-              (const S *)(b ? F.mpz_b : F.mpz), (const S *)(b ? F.mmz_b : F.mmz), (S *)F.rho, (S *)F.vx,
-              (S *)F.vy, (S *)F.vz, (const S *)F.rho0, (const S *)F.vx0, (const S *)F.vy0, (const S *)F.vz0,
-              D.ramps, D.stockholm, scp, bid);
+  const Geo<T> g = geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom);
+  for (int r = 0; r < NV_R; r++) {   // NV_R rows per CTA
+    const uint3 rb = make_uint3(bid.x, bid.y * NV_R + r, bid.z);
+    if ((int)rb.y >= m.ny) break;
+    b_newvel<T, S>(m, g, (const S *)(b ? F.rho_b : F.rho_a), (const S *)(b ? F.mpx_b : F.mpx),
+                (const S *)(b ? F.mmx_b : F.mmx), (const S *)(b ? F.mpy_b : F.mpy), (const S *)(b ? F.mmy_b : F.mmy),
+                (const S *)(b ? F.mpz_b : F.mpz), (const S *)(b ? F.mmz_b : F.mmz), (S *)F.rho, (S *)F.vx,
+                (S *)F.vy, (S *)F.vz, (const S *)F.rho0, (const S *)F.vx0, (const S *)F.vy0, (const S *)F.vz0,
+                D.ramps, D.stockholm, scp, rb);
+  }
 }
 
 // The scalar work of the step for every disk, one thread per disk; then the
@@ -215,7 +234,7 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
     dim3 g(1, 1, 1);
     switch (st) {
       case ST_ROWSUM: g = dim3((sy * sz + 31) / 32); break;
-      case ST_CFL: g = dim3(ny, D.is3d ? nz : 1); break;
+      case ST_CFL: g = dim3((ny + CFL_R - 1) / CFL_R, D.is3d ? nz : 1); break;
       case ST_SOURCES:
         g = D.is3d ? dim3((nx + SRC3_TX - 1) / SRC3_TX, (ny + SRC3_TY - 1) / SRC3_TY, nz)
                    : dim3((nx + SRC2_TX - 1) / SRC2_TX, (ny + SRC2_TY - 1) / SRC2_TY);
@@ -241,7 +260,7 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
         g = dim3((nr + rpc - 1) / rpc);
         break;
       }
-      case ST_NEWVEL: g = dim3((nx + NV_BX - 1) / NV_BX, ny, D.is3d ? nz : 1); break;
+      case ST_NEWVEL: g = dim3((nx + NV_BX - 1) / NV_BX, (ny + NV_R - 1) / NV_R, D.is3d ? nz : 1); break;
     }
     for (unsigned z = 0; z < g.z; z++)
       for (unsigned y = 0; y < g.y; y++)

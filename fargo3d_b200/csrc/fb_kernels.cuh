@@ -169,14 +169,15 @@ __device__ __forceinline__ T zsz(const Dims &m, const Geo<T> &g, int j, int k) {
   return (ld(g.zmin + k + 1) - ld(g.zmin + k));
 }
 
+// This thread's share of ring (j, k): the minimum of its cells' limits (and,
+// for thread 0, the ring's shear limit); non-finite steps or non-positive
+// densities raise the flag word dtmin[1].
 template <typename T, typename S = T>
-__device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const S *__restrict__ rho, const S *__restrict__ cs,
-                                             const S *__restrict__ vx, const S *__restrict__ vy,
-                                             const S *__restrict__ vz, const double *__restrict__ vxmed,
-                                             const fb_scalars *__restrict__ sc, double cfl_num,
-                                             double mindx, unsigned long long *__restrict__ dtmin, uint3 bid) {
-  const int j = FB_NGH + bid.x;
-  const int k = m.is3d ? FB_NGH + bid.y : 0;
+__device__ __forceinline__ double cfl_ring(Dims m, Geo<T> g, const S *__restrict__ rho, const S *__restrict__ cs,
+                                           const S *__restrict__ vx, const S *__restrict__ vy,
+                                           const S *__restrict__ vz, const double *__restrict__ vxmed,
+                                           const fb_scalars *__restrict__ sc, double cfl_num, double mindx,
+                                           unsigned long long *__restrict__ dtmin, int j, int k) {
   const double vm = vxmed[j + k * m.sy];
   const T nu = (T)sc->nu, alpha = (T)sc->alpha;
   double mn = 1e20;
@@ -221,6 +222,11 @@ __device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const S *__restrict__ rh
         fabs(vm / (double)ld(g.ymed + j) - vxmed[j + 1 + k * m.sy] / (double)ld(g.ymed + j + 1));
     if (shear < mn) mn = shear;
   }
+  return mn;
+}
+
+// Block minimum of the threads' shares, folded into the device-wide minimum.
+__device__ __forceinline__ void cfl_commit(double mn, unsigned long long *__restrict__ dtmin) {
   for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
   __shared__ double wm[32];
   if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mn;
@@ -231,6 +237,18 @@ __device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const S *__restrict__ rh
     if (threadIdx.x == 0 && v > 0.0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
   }
 }
+
+template <typename T, typename S = T>
+__device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const S *__restrict__ rho, const S *__restrict__ cs,
+                                             const S *__restrict__ vx, const S *__restrict__ vy,
+                                             const S *__restrict__ vz, const double *__restrict__ vxmed,
+                                             const fb_scalars *__restrict__ sc, double cfl_num,
+                                             double mindx, unsigned long long *__restrict__ dtmin, uint3 bid) {
+  const int j = FB_NGH + bid.x;
+  const int k = m.is3d ? FB_NGH + bid.y : 0;
+  cfl_commit(cfl_ring<T, S>(m, g, rho, cs, vx, vy, vz, vxmed, sc, cfl_num, mindx, dtmin, j, k), dtmin);
+}
+
 template <typename T, typename S = T>
 __global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const S *__restrict__ rho, const S *__restrict__ cs,
                                              const S *__restrict__ vx, const S *__restrict__ vy,
