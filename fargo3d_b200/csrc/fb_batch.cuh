@@ -57,8 +57,10 @@ constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_BX = 128
 template <typename T, bool ORDERED, typename S>
 __global__ void __launch_bounds__(256) kb_rowsum(const fb_disk_dev *ds, const int4 *items, int f, int which) {
   FB_TILE
-  b_rowsum<T, ORDERED, S>(dims_of(D), geo_of<double>(D.geomd), (const S *)(which == 0 ? F.vx : F.vxt),
-                       which == 0 ? F.vxmed : F.vxmed_t, D.xlen, bid);
+  const S *v = (const S *)(which == 0 ? F.vx : F.vxt);
+  double *out = which == 0 ? F.vxmed : F.vxmed_t;
+  if (ORDERED) b_rowsum<T, true, S>(dims_of(D), geo_of<double>(D.geomd), v, out, D.xlen, bid);  // 32 rings / CTA
+  else b_rowsum_warp<S>(dims_of(D), geo_of<double>(D.geomd), v, out, D.xlen, bid);           // 8 rings / CTA
 }
 
 template <typename T, typename S>
@@ -233,7 +235,7 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
     const int nx = D.nx, ny = D.ny, nz = D.nz, sy = D.sy, sz = D.sz;
     dim3 g(1, 1, 1);
     switch (st) {
-      case ST_ROWSUM: g = dim3((sy * sz + 31) / 32); break;
+      case ST_ROWSUM: g = dim3(B->precision == FB_FP64 ? (sy * sz + 31) / 32 : (sy * sz + 7) / 8); break;
       case ST_CFL: g = dim3((ny + CFL_R - 1) / CFL_R, D.is3d ? nz : 1); break;
       case ST_SOURCES:
         g = D.is3d ? dim3((nx + SRC3_TX - 1) / SRC3_TX, (ny + SRC3_TY - 1) / SRC3_TY, nz)

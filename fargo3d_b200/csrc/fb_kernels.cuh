@@ -130,6 +130,28 @@ __device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const S *__rest
     out[myring] = tot / xlen;
   }
 }
+// Order-free ring sums (FP32 storage): one warp per ring, lanes striding
+// over the ring with an FP64 accumulator, then a shuffle tree; 8 rings per
+// CTA of 256 threads, no shared memory and no barrier.
+template <typename S>
+__device__ __forceinline__ void b_rowsum_warp(Dims m, Geo<double> gd, const S *__restrict__ v,
+                                              double *__restrict__ out, double xlen, uint3 bid) {
+  const int ring = bid.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (ring >= m.sy * m.sz) return;
+  const int j = ring % m.sy, k = ring / m.sy;
+  const S *row = v + m.l(0, j, k);
+  double acc = 0.0;
+  for (int i = lane; i < m.nx; i += 32) acc += (double)row[i] * (ld(gd.xmin + i + 1) - ld(gd.xmin + i));
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) out[ring] = acc / xlen;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_rowsum_warp(Dims m, Geo<double> gd, const S *__restrict__ v,
+                                                      double *__restrict__ out, double xlen) {
+  b_rowsum_warp<S>(m, gd, v, out, xlen, blockIdx);
+}
+
 template <typename T, bool ORDERED, typename S = T, int R = 32>
 __global__ void __launch_bounds__(256) k_rowsum(Dims m, Geo<double> gd, const S *__restrict__ v,
                                                  double *__restrict__ out, double xlen) {

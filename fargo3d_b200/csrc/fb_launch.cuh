@@ -23,6 +23,10 @@ static int launch_rowsum(const fb_disk_dev *d, int f, int which, cudaStream_t st
   const int nring = m.sy * m.sz;
   const S *v = (const S *)(which == 0 ? F.vx : F.vxt);
   double *out = which == 0 ? F.vxmed : F.vxmed_t;
+  if (d->precision != FB_FP64) {  // order-free: one warp per ring
+    k_rowsum_warp<S><<<(nring + 7) / 8, 256, 0, st>>>(m, gd, v, out, d->xlen);
+    return (int)cudaGetLastError();
+  }
   if (nring < 32 * 148) {  // few rings: 8 per CTA
     dim3 grid((nring + 7) / 8);
     if (d->precision == FB_FP64) k_rowsum<T, true, S, 8><<<grid, 256, 0, st>>>(m, gd, v, out, d->xlen);
