@@ -22,6 +22,9 @@ typedef struct {
   /* frame-rotation radius tables (FP32 path): ymed^2, its row differences,
      sin^2(zmed) and its layer differences, differenced in double */
   const void *r2_j, *dr2_j, *s2_k, *ds2_k;
+  /* per-row reciprocals and the star's potential (FP32-storage sources):
+     1/Ymed, 1/Ymin, 1/(Ymed(j) - Ymed(j-1)), -G M / r at Ymed */
+  const void *inv_ymed, *inv_ymin, *inv_dymed, *pot_star;
 } fb_geom_dev;
 
 typedef struct {

@@ -192,6 +192,8 @@ static int upload_geometry(fb_disk *D) {
   double *t_visc = malloc(sizeof(double) * sy), *t_viscm = malloc(sizeof(double) * sy), *t_tau = malloc(sizeof(double) * sy);
   double *t_r2 = malloc(sizeof(double) * sy), *t_dr2 = malloc(sizeof(double) * sy);
   double *t_s2 = malloc(sizeof(double) * (sz + 1)), *t_ds2 = malloc(sizeof(double) * (sz + 1));
+  double *t_iym = malloc(sizeof(double) * sy), *t_iyi = malloc(sizeof(double) * sy);
+  double *t_idy = malloc(sizeof(double) * sy), *t_pst = malloc(sizeof(double) * sy);
   for (k = 0; k < sz; k++) { t_szmed[k] = sin(D->zmed[k]); t_czmed[k] = cos(D->zmed[k]); }
   for (k = 0; k < sz + 1; k++) { t_szmin[k] = sin(D->zmin[k]); t_czmin[k] = cos(D->zmin[k]); }
   t_szmed[sz] = t_czmed[sz] = 0.0;
@@ -207,6 +209,14 @@ static int upload_geometry(fb_disk *D) {
   for (j = 0; j < sy; j++) {
     t_r2[j] = D->ymed[j] * D->ymed[j];
     t_dr2[j] = j > 0 ? D->ymed[j] * D->ymed[j] - D->ymed[j - 1] * D->ymed[j - 1] : 0.0;
+  }
+  for (j = 0; j < sy; j++) {
+    t_iym[j] = 1.0 / D->ymed[j];
+    t_iyi[j] = 1.0 / D->ymin[j];
+    t_idy[j] = j > 0 ? 1.0 / (D->ymed[j] - D->ymed[j - 1]) : 0.0;
+    /* potential.c:101-106: the star's term, -G M / r (r = Ymed in spherical
+       meshes, sqrt(Ymed^2 + Zmed^2) with Zmed = 0 in 2D cylindrical ones) */
+    t_pst[j] = D->d.spherical ? -G * MSTAR / D->ymed[j] : -G * MSTAR / sqrt(D->ymed[j] * D->ymed[j]);
   }
   for (k = 0; k < sz + 1; k++) t_s2[k] = t_szmed[k] * t_szmed[k];
   for (k = 0; k < sz + 1; k++) t_ds2[k] = k > 0 && k < sz ? t_s2[k] - t_s2[k - 1] : 0.0;
@@ -226,6 +236,7 @@ static int upload_geometry(fb_disk *D) {
     UP(cos_xmed, t_cx, sx); UP(sin_xmed, t_sx, sx);
     UP(visc_j, t_visc, sy); UP(viscm_j, t_viscm, sy); UP(tau_j, t_tau, sy);
     UP(r2_j, t_r2, sy); UP(dr2_j, t_dr2, sy); UP(s2_k, t_s2, sz + 1); UP(ds2_k, t_ds2, sz + 1);
+    UP(inv_ymed, t_iym, sy); UP(inv_ymin, t_iyi, sy); UP(inv_dymed, t_idy, sy); UP(pot_star, t_pst, sy);
 #undef UP
   }
   rc = FB_OK;
@@ -233,6 +244,7 @@ out:
   free(t_szmed); free(t_czmed); free(t_szmin); free(t_czmin); free(t_cx); free(t_sx);
   free(t_visc); free(t_viscm); free(t_tau);
   free(t_r2); free(t_dr2); free(t_s2); free(t_ds2);
+  free(t_iym); free(t_iyi); free(t_idy); free(t_pst);
   return rc;
 }
 

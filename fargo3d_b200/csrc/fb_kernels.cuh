@@ -36,6 +36,7 @@ struct Geo {
   const T *cos_xmed, *sin_xmed;
   const T *visc_j, *viscm_j, *tau_j;
   const T *r2_j, *dr2_j, *s2_k, *ds2_k;
+  const T *inv_ymed, *inv_ymin, *inv_dymed, *pot_star;
 };
 
 template <typename T>
@@ -52,6 +53,8 @@ __host__ __device__ inline Geo<T> geo_of(const fb_geom_dev &g) {
   o.cos_xmed = (const T *)g.cos_xmed; o.sin_xmed = (const T *)g.sin_xmed;
   o.visc_j = (const T *)g.visc_j; o.viscm_j = (const T *)g.viscm_j; o.tau_j = (const T *)g.tau_j;
   o.r2_j = (const T *)g.r2_j; o.dr2_j = (const T *)g.dr2_j; o.s2_k = (const T *)g.s2_k; o.ds2_k = (const T *)g.ds2_k;
+  o.inv_ymed = (const T *)g.inv_ymed; o.inv_ymin = (const T *)g.inv_ymin; o.inv_dymed = (const T *)g.inv_dymed;
+  o.pot_star = (const T *)g.pot_star;
   return o;
 }
 
@@ -307,6 +310,32 @@ __device__ __forceinline__ double potential_at(const Dims &m, const Geo<double> 
   return pot;
 }
 
+// The same potential for FP32-storage disks: the star's term from the per-row
+// table, the indirect term with the planets' m / d^3 precomputed (ind[n]),
+// the planets' terms with an FP64 reciprocal square root.
+__device__ __forceinline__ double potential_fast(const Dims &m, const Geo<double> &gd, const fb_scalars &sc,
+                                                 const double *ind, int i, int j, int k) {
+  double XC, YC, ZC;
+  const double ym = ld(gd.ymed + j);
+  if (m.sph) {
+    XC = ym * ld(gd.cos_xmed + i) * ld(gd.sin_zmed + k);
+    YC = ym * ld(gd.sin_xmed + i) * ld(gd.sin_zmed + k);
+    ZC = ym * ld(gd.cos_zmed + k);
+  } else {
+    XC = ym * ld(gd.cos_xmed + i);
+    YC = ym * ld(gd.sin_xmed + i);
+    ZC = ld(gd.zmed + k);
+  }
+  double pot = ld(gd.pot_star + j);
+  for (int n = 0; n < sc.nplanets; n++) {
+    const double xp = sc.px[n], yp = sc.py[n], zp = sc.pz[n];
+    const double dist = ((XC - xp) * (XC - xp) + (YC - yp) * (YC - yp) + (ZC - zp) * (ZC - zp));
+    if (sc.indirect_term) pot += ind[n] * (XC * xp + YC * yp + ZC * zp);
+    pot -= sc.pmass[n] * rsqrt(dist + sc.psmooth2[n]);
+  }
+  return pot;
+}
+
 }  // namespace fb
 
 namespace fb {
@@ -330,9 +359,16 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   using TV = typename std::conditional<(sizeof(S) < sizeof(T)), float, T>::type;
   __shared__ TV s_txx[H][W], s_tyy[H][W], s_tyx[H][W];
   __shared__ fb_scalars sc;
+  __shared__ double s_ind[FB_MAXPLANETS];
+  // FP32 storage: the FP64 balance with per-row reciprocals and the fast
+  // potential (one division per density-dependent denominator, reused)
+  constexpr bool FAST = sizeof(S) < sizeof(T);
   const int i0 = bid.x * TX, j0 = FB_NGH + bid.y * TY;
   const int tid = threadIdx.x + threadIdx.y * TX;
-  if (tid == 0) sc = *scp;
+  if (tid == 0) {
+    sc = *scp;
+    for (int n = 0; n < sc.nplanets; n++) s_ind[n] = sc.pmass[n] / sc.pdist3[n];
+  }
   __syncthreads();
   const double dt = sc.dt;
   const T domega = (T)sc.domega, of = (T)sc.omegaframe;
@@ -350,7 +386,7 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
       s_vx[lj][li] = vx[l] - domega * ld(g.ymed + j);
       s_vy[lj][li] = vy[l];
       s_p[lj][li] = r * c * c;
-      s_pot[lj][li] = potential_at(m, gd, sc, i, j, 0);
+      s_pot[lj][li] = FAST ? potential_fast(m, gd, sc, s_ind, i, j, 0) : potential_at(m, gd, sc, i, j, 0);
     }
   }
   __syncthreads();
@@ -397,23 +433,44 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   const int im = wrapx(i - 1, m.nx);
   const long long l = m.l(i, j, 0);
   const T r = s_rho[lj][li], rxm = s_rho[lj][li - 1], rym = s_rho[lj - 1][li];
-  const T izx = izsxmed(m, g, i, j, 0);
+  const T izx = FAST ? ld(g.invdiffxmed + i) * ld(g.inv_ymed + j) : izsxmed(m, g, i, j, 0);
   // SubStep1_x (substep1_x.c:107-117)
   const T dxmed = (T)0.5 * (ld(g.sxi + i) + ld(g.sxi + im));
-  const T dtorx = (T)2. * (T)dt / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * dxmed;
+  T idenx = 0, ideny = 0;
+  T dtorx;
+  if (FAST) {
+    idenx = (T)1.0 / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im));
+    dtorx = (T)2. * (T)dt * idenx * dxmed;
+  } else {
+    dtorx = (T)2. * (T)dt / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * dxmed;
+  }
   T ax = s_vx[lj][li];
   if (!dust) ax -= dtorx * (s_p[lj][li] - s_p[lj][li - 1]) * izx;
   ax -= (T)((s_pot[lj][li] - s_pot[lj][li - 1]) * dt) * izx;
   // SubStep1_y (substep1_y.c:146-192, cylindrical)
   const T ym = ld(g.ymed + j), ymm = ld(g.ymed + j - 1), yi = ld(g.ymin + j), yip = ld(g.ymin + j + 1),
           yim = ld(g.ymin + j - 1);
-  const T dtory = (T)2.0 * (T)dt / (r * (yip - yi) + rym * (yi - yim)) * (ym - ymm);
+  T dtory;
+  if (FAST) {
+    ideny = (T)1.0 / (r * (yip - yi) + rym * (yi - yim));
+    dtory = (T)2.0 * (T)dt * ideny * (ym - ymm);
+  } else {
+    dtory = (T)2.0 * (T)dt / (r * (yip - yi) + rym * (yi - yim)) * (ym - ymm);
+  }
   T ay = s_vy[lj][li];
-  if (!dust) ay -= dtory * (s_p[lj][li] - s_p[lj - 1][li]) / (ym - ymm);
+  if (!dust) {
+    if (FAST) ay -= dtory * (s_p[lj][li] - s_p[lj - 1][li]) * ld(g.inv_dymed + j);
+    else ay -= dtory * (s_p[lj][li] - s_p[lj - 1][li]) / (ym - ymm);
+  }
   T vphi = (T)0.25 * (s_vx[lj][li] + s_vx[lj][li + 1] + s_vx[lj - 1][li] + s_vx[lj - 1][li + 1]);
   vphi += yi * of;
-  ay += vphi * vphi / yi * (T)dt;
-  ay -= (T)((s_pot[lj][li] - s_pot[lj - 1][li]) * dt / (double)(ym - ymm));
+  if (FAST) {
+    ay += vphi * vphi * ld(g.inv_ymin + j) * (T)dt;
+    ay -= (T)((s_pot[lj][li] - s_pot[lj - 1][li]) * dt) * ld(g.inv_dymed + j);
+  } else {
+    ay += vphi * vphi / yi * (T)dt;
+    ay -= (T)((s_pot[lj][li] - s_pot[lj - 1][li]) * dt / (double)(ym - ymm));
+  }
   if (viscous) {
     // addviscosity_cyl (addviscosity_cyl.c:106-124)
     const TV vr = (TV)r, vrxm = (TV)rxm, vrym = (TV)rym, vizx = (TV)izx, vdt = (TV)dt;
@@ -436,8 +493,13 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   const T qy = dv < (T)0.0 ? c2 * c2 * r * dv * dv : (T)0.0;
   dv = s_vy[lj][li] - s_vy[lj - 1][li];
   const T qym = dv < (T)0.0 ? c2 * c2 * rym * dv * dv : (T)0.0;
-  ax += -(T)2.0 * (T)dt * dxmed * (qx - qxm) / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * izx;
-  ay += -(T)2.0 * (qy - qym) / (r * (yip - yi) + rym * (yi - yim)) * (T)dt;
+  if (FAST) {
+    ax += -(T)2.0 * (T)dt * dxmed * (qx - qxm) * idenx * izx;
+    ay += -(T)2.0 * (qy - qym) * ideny * (T)dt;
+  } else {
+    ax += -(T)2.0 * (T)dt * dxmed * (qx - qxm) / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * izx;
+    ay += -(T)2.0 * (qy - qym) / (r * (yip - yi) + rym * (yi - yim)) * (T)dt;
+  }
   vxt[l] = ax;
   vyt[l] = ay;
 }
