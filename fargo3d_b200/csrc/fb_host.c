@@ -79,6 +79,11 @@ struct fb_disk {
   void *allocs[MAXALLOC];
   int nalloc;
   size_t bytes;                 /* device bytes requested by this disk */
+  /* one device arena per disk, sized by fb_params_bytes and zeroed once:
+     the fields and tables are carved from it (creation costs one
+     cudaMalloc + one memset instead of one of each per array) */
+  char *arena;
+  size_t arena_size, arena_used;
   /* optional per-launch timing (fb_disk_profile) */
   int prof;
   int nev;
@@ -101,6 +106,13 @@ static void mark(fb_disk *D, const char *name) {
 /* ------------------------------------------------------------------------ */
 static int dalloc(fb_disk *D, void **p, size_t bytes) {
   cudaError_t e;
+  size_t need = ((bytes ? bytes : 16) + 255) & ~(size_t)255;
+  if (D->arena && D->arena_used + need <= D->arena_size) {
+    *p = D->arena + D->arena_used;   /* 256-byte aligned, already zero */
+    D->arena_used += need;
+    D->bytes += bytes ? bytes : 16;
+    return FB_OK;
+  }
   if (D->nalloc >= MAXALLOC) return fail(FB_ERR_NOMEM, "too many device allocations");
   e = cudaMalloc(p, bytes ? bytes : 16);
   if (e != cudaSuccess) return fail(FB_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
@@ -445,6 +457,19 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
     fb_disk_destroy(D);
     return fail(FB_ERR_CUDA, "cudaStreamCreate failed");
   }
+  {
+    size_t est = 0;
+    if (fb_params_bytes(p, precision, &est) == FB_OK) {
+      est += (size_t)MAXALLOC * 256; /* alignment of each carved array */
+      if (cudaMalloc((void **)&D->arena, est) == cudaSuccess && cudaMemset(D->arena, 0, est) == cudaSuccess)
+        D->arena_size = est;
+      else {
+        if (D->arena) cudaFree(D->arena);
+        D->arena = NULL;     /* fall back to one allocation per array */
+        cudaGetLastError();
+      }
+    }
+  }
   if ((rc = upload_geometry(D)) || (rc = upload_tables(D))) { fb_disk_destroy(D); return rc; }
   for (f = 0; f < p->nfluids; f++) {
     fb_fluid_dev *F = &D->d.fl[f];
@@ -491,6 +516,7 @@ int fb_disk_destroy(fb_disk *D) {
   if (D->device >= 0) cudaSetDevice(D->device);
   if (D->stream) cudaStreamSynchronize(D->stream);
   for (i = 0; i < D->nalloc; i++) cudaFree(D->allocs[i]);
+  if (D->arena) cudaFree(D->arena);
   if (D->h_dtmin) cudaFreeHost(D->h_dtmin);
   for (i = 0; i < 32; i++)
     if (D->ev[i]) cudaEventDestroy(D->ev[i]);
