@@ -194,7 +194,7 @@ static __global__ void kb_scalars(const fb_disk_dev *ds, fb_psys *ps, int n, dou
     } else if (dm[1] != 0ull) {
       S.status = FB_ERR_NONFINITE;
       sc.skip = 1;
-    } else if (fb_psys_step(&S, cflmin, S.t_end > 0.0 ? S.t_end : DT, &sc) < 0.0) {
+    } else if (fb_psys_step(&S, cflmin, S.t_end > 0.0 ? S.t_end : DT, &sc, nullptr) < 0.0) {
       sc.skip = 1;
     } else if (S.t_end > 0.0 && S.dtemp >= S.t_end) {
       S.status = FB_DONE;

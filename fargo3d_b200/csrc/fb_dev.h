@@ -89,7 +89,9 @@ typedef struct {
   int fb_launch_sweep_cols_##SUF(const fb_disk_dev *d, int fluid, void *stream);    \
   int fb_launch_sweep_x_##SUF(const fb_disk_dev *d, int fluid, void *stream);       \
   int fb_launch_newvel_##SUF(const fb_disk_dev *d, int fluid, void *stream);        \
-  int fb_launch_collisions_##SUF(const fb_disk_dev *d, void *stream);
+  int fb_launch_collisions_##SUF(const fb_disk_dev *d, void *stream);                 \
+  int fb_launch_disk_force_##SUF(const fb_disk_dev *d, double x, double y, double z, double rs, double *ring3, \
+                                 double *out3, void *stream);
 
 FB_DECL_LAUNCHERS(f64)
 FB_DECL_LAUNCHERS(f32)

@@ -75,7 +75,9 @@ struct fb_disk {
   /* planetary system, frame and time (fb_psys.h) */
   fb_psys ps;
   fb_scalars sc;
-  double *h_dtmin;              /* pinned */
+  double *h_dtmin;              /* pinned: [0..1] CFL minimum + flag, [8..] disk accelerations */
+  double *d_ring3, *d_facc;     /* disk-force scratch: ring sums, accelerations (3 per planet) */
+  int feeldisk;                 /* some planet feels the disk */
   void *allocs[MAXALLOC];
   int nalloc;
   size_t bytes;                 /* device bytes requested by this disk */
@@ -499,8 +501,18 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
     fb_disk_destroy(D);
     return rc;
   }
-  if (cudaMallocHost((void **)&D->h_dtmin, 64) != cudaSuccess) { fb_disk_destroy(D); return fail(FB_ERR_CUDA, "pinned"); }
-  fb_psys_init(&D->ps, p->nplanets, p->pl_dist, p->pl_mass, p->pl_feelothers, p->eccentricity, p->inclination,
+  if (cudaMallocHost((void **)&D->h_dtmin, 8 * (8 + 3 * FB_MAXPLANETS)) != cudaSuccess) {
+    fb_disk_destroy(D);
+    return fail(FB_ERR_CUDA, "pinned");
+  }
+  for (f = 0; f < p->nplanets; f++) D->feeldisk |= p->pl_feeldisk[f] != 0;
+  if (D->feeldisk &&
+      ((rc = dalloc(D, (void **)&D->d_ring3, sizeof(double) * 3 * D->d.sy * D->d.sz)) ||
+       (rc = dalloc(D, (void **)&D->d_facc, sizeof(double) * 3 * FB_MAXPLANETS)))) {
+    fb_disk_destroy(D);
+    return rc;
+  }
+  fb_psys_init(&D->ps, p->nplanets, p->pl_dist, p->pl_mass, p->pl_feeldisk, p->pl_feelothers, p->eccentricity, p->inclination,
                p->frame, p->omegaframe, p->indirect_term, p->roche_smoothing, p->aspectratio, p->flaringindex,
                p->thickness_smoothing);
   D->sc.nu = p->nu; D->sc.alpha = p->alpha; D->sc.cfl = p->cfl;
@@ -631,13 +643,28 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   mark(D, "rowsum");
   for (f = 0; f < D->p.nfluids; f++) LCH(LAUNCH(cfl, &D->d, f, D->stream));
   mark(D, "cfl");
+  /* AdvanceSystemFromDisk's accelerations (planets.c:86-114): the disk's
+   * pull at each planet that feels it, from the state at the step start */
+  if (D->feeldisk) {
+    int n;
+    for (n = 0; n < D->ps.np; n++) {
+      double m = D->ps.pmass[n], x = D->ps.px[n], y = D->ps.py[n], z = D->ps.pz[n], r, sm;
+      if (!D->ps.feeldisk[n]) continue;
+      r = sqrt(x * x + y * y + z * z);
+      if (D->p.roche_smoothing != 0) sm = r * pow(m / 3. / MSTAR, 1. / 3.) * D->p.roche_smoothing;
+      else sm = D->p.aspectratio * pow(r / R0, D->p.flaringindex) * r * D->p.thickness_smoothing;
+      LCH(LAUNCH(disk_force, &D->d, x, y, z, sm, D->d_ring3, D->d_facc + 3 * n, D->stream));
+    }
+    CU(cudaMemcpyAsync(D->h_dtmin + 8, D->d_facc, sizeof(double) * 3 * D->ps.np, cudaMemcpyDeviceToHost, D->stream));
+    mark(D, "disk_force");
+  }
   CU(cudaMemcpyAsync(D->h_dtmin, D->d.dtmin, 16, cudaMemcpyDeviceToHost, D->stream));
   CU(cudaStreamSynchronize(D->stream));
   if (((const uint64_t *)D->h_dtmin)[1] != 0)
     return fail(FB_ERR_NONFINITE, "non-finite time step or non-positive density in the state");
   /* CflFluidsMin (cfl_fluids_min.c:3-22), the DT clip (main.c:388-395) and
    * compute_potential's planetary update (potential.c:10-49) */
-  dt = fb_psys_step(&D->ps, D->h_dtmin[0], DT, &D->sc);
+  dt = fb_psys_step(&D->ps, D->h_dtmin[0], DT, &D->sc, D->feeldisk ? D->h_dtmin + 8 : NULL);
   if (dt < 0.0) return fail(FB_ERR_NULL_DT, "null time step (CFL minimum %g)", D->h_dtmin[0]);
   if ((rc = push_scalars(D))) return rc;
   /* Sources (algogas.c:30-120) with its closing FillGhosts on V_temp */

@@ -1399,6 +1399,79 @@ __global__ void __launch_bounds__(128) k_collisions(const fb_disk_dev D, Dims m,
   b_collisions<T, N, S>(D, m, gd, scp, blockIdx);
 }
 
+// ---------------------------------------------------------------------------
+// The disk's gravitational acceleration at a point (x, y, z) with smoothing
+// rs: ComputeAccel (planets.c:62-84) over _ComputeForce_cpu
+// (compute_force.c:16-219), in FP64 and in the reference's summation order:
+// each active ring's cells in order of i (reduction_SUM), then the rings in
+// order of k then j (reduction_full_SUM), the inner rings (up to the point's
+// radius) and the outer ones separately.  Density = the sum of the fluids'
+// densities in fluid order (ComputeTotalDensity).
+template <typename S>
+__global__ void __launch_bounds__(128) k_disk_force_rings(const fb_disk_dev D, double x, double y, double z,
+                                                          double rs, double *__restrict__ ring3) {
+  const Dims m = dims_of(D);
+  const Geo<double> gd = geo_of<double>(D.geomd);
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m.ny * (m.is3d ? m.nz : 1)) return;
+  const int j = FB_NGH + r % m.ny, k = m.is3d ? FB_NGH + r / m.ny : 0;
+  const double ym = ld(gd.ymed + j), syk = ld(gd.syk + k), ivj = ld(gd.invvj + j);
+  double sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int i = 0; i < m.nx; i++) {
+    const long long l = m.l(i, j, k);
+    double dens = 0.0;
+    for (int f = 0; f < D.nfluids; f++) dens += (double)((const S *)D.fl[f].rho)[l];
+    const double cellmass = syk * ld(gd.sxi + i) / ivj * dens;
+    double dx, dy, dz;
+    if (m.sph) {
+      dx = ym * ld(gd.cos_xmed + i) * ld(gd.sin_zmed + k) - x;
+      dy = ym * ld(gd.sin_xmed + i) * ld(gd.sin_zmed + k) - y;
+      dz = ym * ld(gd.cos_zmed + k) - z;
+    } else {
+      dx = ym * ld(gd.cos_xmed + i) - x;
+      dy = ym * ld(gd.sin_xmed + i) - y;
+      dz = ld(gd.zmed + k) - z;
+    }
+    double dist2 = dx * dx + dy * dy + dz * dz;
+    dist2 += rs * rs;
+    const double distance = sqrt(dist2);
+    double inv3 = 1.0 / (dist2 * distance);
+    inv3 *= 1.0 * cellmass;  // G = 1
+    sx += dx * inv3;
+    sy += dy * inv3;
+    sz += dz * inv3;
+  }
+  const int n2 = m.sy * m.sz, q = j + k * m.sy;
+  ring3[q] = sx;
+  ring3[n2 + q] = sy;
+  ring3[2 * n2 + q] = sz;
+}
+
+// one thread: fold the ring sums into inner + outer (compute_force.c:161-214)
+static __global__ void k_disk_force_fold(const fb_disk_dev D, double x, double y, double z,
+                                  const double *__restrict__ ring3, double *__restrict__ out3) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const Dims m = dims_of(D);
+  const Geo<double> gd = geo_of<double>(D.geomd);
+  const int k0 = m.is3d ? FB_NGH : 0, k1 = m.is3d ? m.nz + FB_NGH : 1, n2 = m.sy * m.sz;
+  const double aa = sqrt(x * x + y * y + z * z);
+  const int index = (int)(((aa - ld(gd.ymin + FB_NGH)) / (ld(gd.ymin + m.ny + FB_NGH + 1) - ld(gd.ymin + FB_NGH))) *
+                          (double)m.ny) + FB_NGH;
+  int ilo = FB_NGH, ihi = FB_NGH, olo = FB_NGH, ohi = m.ny + FB_NGH;   // default: all outer
+  if (index >= FB_NGH) {
+    if (index < m.ny + FB_NGH) { ihi = index; olo = index; }
+    else { ihi = m.ny + FB_NGH; olo = ohi; }
+  }
+  for (int c = 0; c < 3; c++) {
+    double fin = 0.0, fout = 0.0;
+    for (int k = k0; k < k1; k++)
+      for (int j = ilo; j < ihi; j++) fin = ring3[c * n2 + j + k * m.sy] + fin;
+    for (int k = k0; k < k1; k++)
+      for (int j = olo; j < ohi; j++) fout = ring3[c * n2 + j + k * m.sy] + fout;
+    out3[c] = fin + fout;
+  }
+}
+
 // shared memory of b_sweep_x2 for a ring of nx cells (rpc rings per CTA)
 __host__ __device__ inline size_t sweep_x2_smem(int nx, int C, int nt, int nq, size_t esz) {
   const int rpc = nt / (nx / C);

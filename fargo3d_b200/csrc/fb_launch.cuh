@@ -224,6 +224,16 @@ static int launch_collisions(const fb_disk_dev *d, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+// the disk's acceleration at one point (ComputeAccel), FP64 in every precision
+template <typename S>
+static int launch_disk_force(const fb_disk_dev *d, double x, double y, double z, double rs, double *ring3,
+                             double *out3, cudaStream_t st) {
+  const int nr = d->ny * (d->is3d ? d->nz : 1);
+  k_disk_force_rings<S><<<(nr + 127) / 128, 128, 0, st>>>(*d, x, y, z, rs, ring3);
+  k_disk_force_fold<<<1, 32, 0, st>>>(*d, x, y, z, ring3, out3);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace fb
 
 #define FB_CAT2(a, b) a##_##b
@@ -253,5 +263,9 @@ int FB_CAT(fb_launch_newvel, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
 }
 int FB_CAT(fb_launch_collisions, FB_SUF)(const fb_disk_dev *d, void *s) {
   return fb::launch_collisions<FB_REAL, FB_STORE>(d, (cudaStream_t)s);
+}
+int FB_CAT(fb_launch_disk_force, FB_SUF)(const fb_disk_dev *d, double x, double y, double z, double rs,
+                                          double *ring3, double *out3, void *s) {
+  return fb::launch_disk_force<FB_STORE>(d, x, y, z, rs, ring3, out3, (cudaStream_t)s);
 }
 }

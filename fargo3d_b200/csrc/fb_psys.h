@@ -32,6 +32,7 @@
 typedef struct fb_psys_s {
   int np, frame, indirect_term;
   int feelothers[FB_MAXPLANETS];
+  int feeldisk[FB_MAXPLANETS];   /* AdvanceSystemFromDisk applies (planets.c:93) */
   double px[FB_MAXPLANETS], py[FB_MAXPLANETS], pz[FB_MAXPLANETS];
   double pvx[FB_MAXPLANETS], pvy[FB_MAXPLANETS], pvz[FB_MAXPLANETS], pmass[FB_MAXPLANETS];
   double xmark, ymark, xaxis_rot;
@@ -186,7 +187,11 @@ static FB_HD inline void fb_psys_fill_scalars(const fb_psys *S, fb_scalars *sc) 
  * disk (the MIN over fluids and shear limits): dt with the DT-interval clip,
  * then compute_potential's planetary update.  Returns dt, or -1 on a null
  * time step (cfl_fluids_min.c:18-21). */
-static FB_HD inline double fb_psys_step(fb_psys *S, double cflmin, double DT, fb_scalars *sc) {
+/* One step of the planetary system (compute_potential, potential.c:10-49).
+ * dacc: the disk's acceleration at each planet's position (3 per planet,
+ * ComputeAccel), applied to the planets that feel the disk before the RK5
+ * substeps (AdvanceSystemFromDisk, planets.c:86-114); NULL when none does. */
+static FB_HD inline double fb_psys_step(fb_psys *S, double cflmin, double DT, fb_scalars *sc, const double *dacc) {
   double step = 1e30, dt;
   int f;
   if (S->dtemp >= DT) S->dtemp = 0.0;
@@ -200,6 +205,13 @@ static FB_HD inline double fb_psys_step(fb_psys *S, double cflmin, double DT, fb
   if (S->dtemp > DT) dt = DT - (S->dtemp - dt);
   if (S->frame != FB_FRAME_FIXED) fb_psys_info(S, FB_PS_MARK);
   fb_psys_fill_scalars(S, sc);
+  if (dacc)
+    for (f = 0; f < S->np; f++)
+      if (S->feeldisk[f]) {
+        S->pvx[f] += dt * dacc[3 * f];
+        S->pvy[f] += dt * dacc[3 * f + 1];
+        S->pvz[f] += dt * dacc[3 * f + 2];
+      }
   for (f = 0; f < 5; f++) fb_nbody_rk5(S, 1.0 / ((double)(5)) * dt);
   if (S->frame != FB_FRAME_FIXED) {
     double omeganew = fb_psys_info(S, FB_PS_GET) / dt;
@@ -219,7 +231,7 @@ static FB_HD inline double fb_psys_step(fb_psys *S, double cflmin, double DT, fb
 
 /* Initial planetary system (psys.c:190-210) and frame (main.c:240-242). */
 static FB_HD inline void fb_psys_init(fb_psys *S, int np, const double *dist, const double *mass,
-                                      const int *feelothers, double ecc, double inc, int frame,
+                                      const int *feeldisk, const int *feelothers, double ecc, double inc, int frame,
                                       double omegaframe, int indirect_term, double roche_smoothing,
                                       double aspectratio, double flaringindex, double thickness_smoothing) {
   int n;
@@ -242,6 +254,7 @@ static FB_HD inline void fb_psys_init(fb_psys *S, int np, const double *dist, co
     S->pvx[n] = -0.0000000000 * S->pvy[n];
     S->pvz[n] = S->pvy[n] * sin(inc) / cos(inc);
     S->feelothers[n] = feelothers[n];
+    S->feeldisk[n] = feeldisk[n];
   }
   S->omegaframe = omegaframe;
   if (frame != FB_FRAME_FIXED && np > 0) S->omegaframe = fb_psys_info(S, FB_PS_FREQUENCY);

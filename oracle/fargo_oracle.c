@@ -425,9 +425,14 @@ static void pressure_iso(fo_disk *d) {
 
 /* _ComputeForce_cpu (compute_force.c:16-219) for x=y=z=0 (the star): only the
  * "outer" partial sums survive (index < NGHY), which ComputeAccel adds. */
-static void compute_star_accel(fo_disk *d, double *ax, double *ay, double *az) {
-  int i, j, k, k0 = d->is3d ? NG : 0, k1 = d->is3d ? d->nz + NG : 1;
+/* ComputeAccel (planets.c:62-84) with _ComputeForce_cpu (compute_force.c:16-219):
+ * the gravitational acceleration the disk (Total_Density) exerts at the
+ * point (x, y, z) with smoothing rs, as the sum of the inner and outer
+ * contributions split at the point's radius (HILLCUT and EXCLUDEHILL off). */
+static void compute_accel(fo_disk *d, double x, double y, double z, double rs, double *ax, double *ay, double *az) {
+  int i, j, k, k0 = d->is3d ? NG : 0, k1 = d->is3d ? d->nz + NG : 1, index;
   const double *dens = d->totdens;
+  double aa, fin[3] = {0.0, 0.0, 0.0}, fout[3] = {0.0, 0.0, 0.0};
   for (k = k0; k < k1; k++)
     for (j = NG; j < d->ny + NG; j++)
       for (i = 0; i < d->nx; i++) {
@@ -435,16 +440,16 @@ static void compute_star_accel(fo_disk *d, double *ax, double *ay, double *az) {
         double cellmass = Syk(k) * Sxi(i) / InvVj(j) * dens[l];
         double dx, dy, dz, dist2, distance, inv3;
         if (d->p.spherical) {
-          dx = Ymed(j) * cos(Xmed(i)) * sin(Zmed(k)) - 0.0;
-          dy = Ymed(j) * sin(Xmed(i)) * sin(Zmed(k)) - 0.0;
-          dz = Ymed(j) * cos(Zmed(k)) - 0.0;
+          dx = Ymed(j) * cos(Xmed(i)) * sin(Zmed(k)) - x;
+          dy = Ymed(j) * sin(Xmed(i)) * sin(Zmed(k)) - y;
+          dz = Ymed(j) * cos(Zmed(k)) - z;
         } else {
-          dx = Ymed(j) * cos(Xmed(i)) - 0.0;
-          dy = Ymed(j) * sin(Xmed(i)) - 0.0;
-          dz = Zmed(k) - 0.0;
+          dx = Ymed(j) * cos(Xmed(i)) - x;
+          dy = Ymed(j) * sin(Xmed(i)) - y;
+          dz = Zmed(k) - z;
         }
         dist2 = dx * dx + dy * dy + dz * dz;
-        dist2 += 0.0 * 0.0;
+        dist2 += rs * rs;
         distance = sqrt(dist2);
         inv3 = 1.0 / (dist2 * distance);
         inv3 *= G * cellmass;
@@ -455,10 +460,54 @@ static void compute_star_accel(fo_disk *d, double *ax, double *ay, double *az) {
         d->fl[d->cur].vxt[l] = 0.0; /* fyhi */
         d->fl[d->cur].vyt[l] = 0.0; /* fzhi */
       }
-  /* compute_force.c:163-214, "all is outer force" branch */
-  *ax = 0.0 + reduction_full_sum(d, d->mmx, NG, d->ny + NG, k0, k1);
-  *ay = 0.0 + reduction_full_sum(d, d->mpx, NG, d->ny + NG, k0, k1);
-  *az = 0.0 + reduction_full_sum(d, d->mmy, NG, d->ny + NG, k0, k1);
+  /* compute_force.c:161-214: inner rings up to the point's radius index */
+  aa = sqrt(x * x + y * y + z * z);
+  index = (int)(((aa - Ymin(NG)) / (Ymin(d->ny + NG + 1) - Ymin(NG))) * (double)d->ny) + NG;
+  if (index >= NG) {
+    if (index < d->ny + NG) {
+      fin[0] = reduction_full_sum(d, d->mmx, NG, index, k0, k1);
+      fin[1] = reduction_full_sum(d, d->mpx, NG, index, k0, k1);
+      fin[2] = reduction_full_sum(d, d->mmy, NG, index, k0, k1);
+      fout[0] = reduction_full_sum(d, d->mmx, index, d->ny + NG, k0, k1);
+      fout[1] = reduction_full_sum(d, d->mpx, index, d->ny + NG, k0, k1);
+      fout[2] = reduction_full_sum(d, d->mmy, index, d->ny + NG, k0, k1);
+    } else {
+      fin[0] = reduction_full_sum(d, d->mmx, NG, d->ny + NG, k0, k1);
+      fin[1] = reduction_full_sum(d, d->mpx, NG, d->ny + NG, k0, k1);
+      fin[2] = reduction_full_sum(d, d->mmy, NG, d->ny + NG, k0, k1);
+    }
+  } else {
+    fout[0] = reduction_full_sum(d, d->mmx, NG, d->ny + NG, k0, k1);
+    fout[1] = reduction_full_sum(d, d->mpx, NG, d->ny + NG, k0, k1);
+    fout[2] = reduction_full_sum(d, d->mmy, NG, d->ny + NG, k0, k1);
+  }
+  *ax = fin[0] + fout[0];
+  *ay = fin[1] + fout[1];
+  *az = fin[2] + fout[2];
+}
+
+/* DiskOnPrimaryAcceleration = ComputeAccel(0, 0, 0, 0, 0) (potential.c:29). */
+static void compute_star_accel(fo_disk *d, double *ax, double *ay, double *az) {
+  compute_accel(d, 0.0, 0.0, 0.0, 0.0, ax, ay, az);
+}
+
+/* AdvanceSystemFromDisk (planets.c:86-114): a planet that feels the disk
+ * gets dt times the disk's acceleration at its position (GASINDIRECTTERM
+ * off). */
+static void advance_system_from_disk(fo_disk *d, double dt) {
+  int n;
+  for (n = 0; n < d->np; n++) {
+    double m, x, y, z, r, smoothing, gx, gy, gz;
+    if (!d->pfeeldisk[n]) continue;
+    m = d->pmass[n]; x = d->px[n]; y = d->py[n]; z = d->pz[n];
+    r = sqrt(x * x + y * y + z * z);
+    if (d->p.roche_smoothing != 0) smoothing = r * pow(m / 3. / MSTAR, 1. / 3.) * d->p.roche_smoothing;
+    else smoothing = d->p.aspectratio * pow(r / R0, d->p.flaringindex) * r * d->p.thickness_smoothing;
+    compute_accel(d, x, y, z, smoothing, &gx, &gy, &gz);
+    d->pvx[n] += dt * gx;
+    d->pvy[n] += dt * gy;
+    d->pvz[n] += dt * gz;
+  }
 }
 
 /* Potential_cpu (potential.c:51-208), taper = 1 (MASSTAPER = 0). */
@@ -513,7 +562,7 @@ static void compute_potential(fo_disk *d, double dt) {
     else { d->indirect_x = d->indirect_y = d->indirect_z = 0.0; }
   }
   potential(d);
-  /* AdvanceSystemFromDisk (planets.c:86-114): planets here never feel the disk. */
+  advance_system_from_disk(d, dt);
   for (i = 0; i < 5; i++) advance_rk5(d, 1.0 / ((double)(5)) * dt);
   d->potential_done_at = (int)d->timestep_count;
   if (d->p.frame != FO_FRAME_FIXED) {

@@ -22,6 +22,10 @@ def cases():
         "sph3d": (config_p3disof(16, 12, 6, seed=5), 6, 1e30),
         # setups/fargo_multifluid flags: gas + 4 dust species, implicit drag
         "mf5": (config_multifluid(32, 16, seed=6), 12, 1e30),
+        # planets that feel the disk (AdvanceSystemFromDisk + ComputeAccel) and each other
+        "cyl2d_feeldisk": (config_fargo2d(32, 16, seed=8).replace(
+            frame="F", omegaframe=1.0, indirect_term=False,
+            planets=[Planet(1.0, 1e-3, True, True), Planet(1.4, 3e-4, True, True)]), 15, 1e30),
     }
 
 
