@@ -12,6 +12,7 @@
 #include <stdarg.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -86,6 +87,8 @@ struct fb_disk {
      cudaMalloc + one memset instead of one of each per array) */
   char *arena;
   size_t arena_size, arena_used;
+  char *hstage;                 /* host image of the arena's table region, sent in one copy */
+  size_t hstage_size, hstage_hi;
   /* optional per-launch timing (fb_disk_profile) */
   int prof;
   int nev;
@@ -124,21 +127,70 @@ static int dalloc(fb_disk *D, void **p, size_t bytes) {
   return FB_OK;
 }
 
+/* Pinned 256-byte slots for the per-step readback (CFL minimum, flag, disk
+ * accelerations), carved from 64 KiB pinned blocks and recycled through a
+ * free list: creating a disk pins no memory of its own. */
+#define PIN_SLOT 256
+#define PIN_BLOCK (64 * 1024)
+static pthread_mutex_t g_pin_mu = PTHREAD_MUTEX_INITIALIZER;
+static void *g_pin_free = NULL;             /* singly linked through the slots */
+static char *g_pin_block = NULL;
+static size_t g_pin_used = PIN_BLOCK;
+
+static double *pinned_slot(void) {
+  void *p = NULL;
+  pthread_mutex_lock(&g_pin_mu);
+  if (g_pin_free) {
+    p = g_pin_free;
+    g_pin_free = *(void **)p;
+  } else {
+    if (g_pin_used + PIN_SLOT > PIN_BLOCK) {
+      char *b = NULL;
+      if (cudaMallocHost((void **)&b, PIN_BLOCK) == cudaSuccess) {
+        g_pin_block = b;
+        g_pin_used = 0;
+      }
+    }
+    if (g_pin_block && g_pin_used + PIN_SLOT <= PIN_BLOCK) {
+      p = g_pin_block + g_pin_used;
+      g_pin_used += PIN_SLOT;
+    }
+  }
+  pthread_mutex_unlock(&g_pin_mu);
+  if (p) memset(p, 0, PIN_SLOT);
+  return (double *)p;
+}
+
+static void pinned_release(double *p) {
+  pthread_mutex_lock(&g_pin_mu);
+  *(void **)p = g_pin_free;
+  g_pin_free = p;
+  pthread_mutex_unlock(&g_pin_mu);
+}
+
 /* upload a double table, converted to the disk's precision when asked */
 static int upload(fb_disk *D, const void **dst, const double *src, int n, int as_float) {
   void *p;
-  int rc;
+  int rc, i;
+  const size_t bytes = (as_float ? sizeof(float) : sizeof(double)) * (size_t)n;
+  rc = dalloc(D, &p, bytes);
+  if (rc) return rc;
+  if (D->hstage && (char *)p >= D->arena && (size_t)((char *)p - D->arena) + bytes <= D->hstage_size) {
+    char *h = D->hstage + ((char *)p - D->arena);   /* staged: sent with the others */
+    if (as_float)
+      for (i = 0; i < n; i++) ((float *)h)[i] = (float)src[i];
+    else
+      memcpy(h, src, bytes);
+    if ((size_t)((char *)p - D->arena) + bytes > D->hstage_hi) D->hstage_hi = (size_t)((char *)p - D->arena) + bytes;
+    *dst = p;
+    return FB_OK;
+  }
   if (as_float) {
     float *tmp = (float *)malloc(sizeof(float) * (n ? n : 1));
-    int i;
     for (i = 0; i < n; i++) tmp[i] = (float)src[i];
-    rc = dalloc(D, &p, sizeof(float) * n);
-    if (rc) { free(tmp); return rc; }
     cudaMemcpy(p, tmp, sizeof(float) * n, cudaMemcpyHostToDevice);
     free(tmp);
   } else {
-    rc = dalloc(D, &p, sizeof(double) * n);
-    if (rc) return rc;
     cudaMemcpy(p, src, sizeof(double) * n, cudaMemcpyHostToDevice);
   }
   *dst = p;
@@ -472,7 +524,22 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
       }
     }
   }
-  if ((rc = upload_geometry(D)) || (rc = upload_tables(D))) { fb_disk_destroy(D); return rc; }
+  if (D->arena) {  /* host image of the table region (tables are carved first) */
+    size_t sy = (size_t)D->d.sy, sz = (size_t)D->d.sz;
+    D->hstage_size = 2 * sizeof(double) * (6 * ((size_t)p->nx + 1) + 32 * (sy + 1) + 24 * (sz + 1)) +
+                     sizeof(double) * (18 + 6 * sz + 6 * sy + 6 + sy + 2 * sz) + (size_t)128 * 256;
+    if (D->hstage_size > D->arena_size) D->hstage_size = D->arena_size;
+    D->hstage = (char *)calloc(1, D->hstage_size);
+    if (!D->hstage) D->hstage_size = 0;
+  }
+  rc = upload_geometry(D);
+  if (!rc) rc = upload_tables(D);
+  if (!rc && D->hstage && D->hstage_hi > 0 &&
+      cudaMemcpy(D->arena, D->hstage, D->hstage_hi, cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(FB_ERR_CUDA, "table upload");
+  free(D->hstage);
+  D->hstage = NULL;
+  if (rc) { fb_disk_destroy(D); return rc; }
   for (f = 0; f < p->nfluids; f++) {
     fb_fluid_dev *F = &D->d.fl[f];
     size_t fb = D->esz * nc, f2 = sizeof(double) * D->d.sy * D->d.sz, e2 = D->esz * D->d.sy * D->d.sz;
@@ -501,9 +568,9 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
     fb_disk_destroy(D);
     return rc;
   }
-  if (cudaMallocHost((void **)&D->h_dtmin, 8 * (8 + 3 * FB_MAXPLANETS)) != cudaSuccess) {
+  if (!(D->h_dtmin = pinned_slot())) {
     fb_disk_destroy(D);
-    return fail(FB_ERR_CUDA, "pinned");
+    return fail(FB_ERR_CUDA, "pinned host memory");
   }
   for (f = 0; f < p->nplanets; f++) D->feeldisk |= p->pl_feeldisk[f] != 0;
   if (D->feeldisk &&
@@ -529,7 +596,7 @@ int fb_disk_destroy(fb_disk *D) {
   if (D->stream) cudaStreamSynchronize(D->stream);
   for (i = 0; i < D->nalloc; i++) cudaFree(D->allocs[i]);
   if (D->arena) cudaFree(D->arena);
-  if (D->h_dtmin) cudaFreeHost(D->h_dtmin);
+  if (D->h_dtmin) pinned_release(D->h_dtmin);
   for (i = 0; i < 32; i++)
     if (D->ev[i]) cudaEventDestroy(D->ev[i]);
   if (D->stream) cudaStreamDestroy(D->stream);
