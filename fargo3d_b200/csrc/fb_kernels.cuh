@@ -938,9 +938,14 @@ __device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
   __shared__ T t_xx[2][H][W], t_zz[2][H][W], t_yy[H][W];   // planes k-1, k
   __shared__ T t_xz[2][H][W], t_zy[2][H][W], t_yx[H][W];   // planes k, k+1
   __shared__ fb_scalars sc;
+  __shared__ double s_ind[FB_MAXPLANETS];
+  constexpr bool FAST = sizeof(S) < sizeof(T);  // FP32 storage: fast potential
   const int i0 = bid.x * TX, j0 = FB_NGH + bid.y * TY, kc = FB_NGH + bid.z;
   const int tid = threadIdx.x + threadIdx.y * TX;
-  if (tid == 0) sc = *scp;
+  if (tid == 0) {
+    sc = *scp;
+    for (int n = 0; n < sc.nplanets; n++) s_ind[n] = sc.pmass[n] / sc.pdist3[n];
+  }
   __syncthreads();
   const double dt = sc.dt;
   const T domega = (T)sc.domega, of = (T)sc.omegaframe;
@@ -955,7 +960,7 @@ __device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
       s_vx[lk][lj][li] = vx[l] - domega * ld(g.ymed + j) * ld(g.sin_zmed + k);
       s_vy[lk][lj][li] = vy[l];
       s_vz[lk][lj][li] = vz[l];
-      if (lk < 2) s_pot[lk][lj][li] = potential_at(m, gd, sc, i, j, k);
+      if (lk < 2) s_pot[lk][lj][li] = FAST ? potential_fast(m, gd, sc, s_ind, i, j, k) : potential_at(m, gd, sc, i, j, k);
     }
   }
   __syncthreads();
