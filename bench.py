@@ -64,6 +64,14 @@ LAUNCH_WORDS = {
     "3d": {"rowsum": 1, "cfl": 5, "sources": 8, "bnd_vtemp": 0, "rowsum_vtemp": 1,
            "sweep_cols": 26, "sweep_x": 15, "newvel": 11, "bnd": 0, "scalars": 0},
 }
+# DRAM bytes (read + write) per launch from one ncu capture of the batched
+# FP32 step (profiles/batched64_fp32_launches_and_top_kernels.md, --set full
+# on 3 eager steps); None where no capture of the workload exists
+TRAFFIC_BYTES = {("batched", "fp32"): {"sweep_x": (191.7184 + 331.205376) * 1e6,
+                                       "sources": (130.313216 + 44.268544) * 1e6,
+                                       "sweep_cols": (98.627328 + 123.73964) * 1e6,
+                                       "cfl": (127.243008 + 3.932928) * 1e6,
+                                       "newvel": (159.164928 + 64.728832) * 1e6}}
 KERNELS_PER_GROUP = {"2d": {"sweep_cols": 1, "bnd": 1, "bnd_vtemp": 1},
                      "3d": {"sweep_cols": 2, "bnd": 2, "bnd_vtemp": 2}}
 
@@ -337,7 +345,8 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": 5 * nstored * 8 / args.steps,
                 "d2h_bytes_per_step": 4 * nstored * 8 / args.steps + (0 if batched else 16)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "traffic": TRAFFIC_BYTES.get((args.workload, precision), {}).get(dom),
                      "alg_bytes_per_launch": dom_bytes, "launch_ms": prof[dom],
                      "step_alg_frac": (ALG_WORDS[dim] + (ALG_WORDS[dim] - 1) * (nf - 1)) * esz * cells
                                       * args.steps / (ms / 1e3) / 1e9 / hbm},
