@@ -667,6 +667,102 @@ int fb_disk_get_state(fb_disk *D, int f, double *rho, double *vx, double *vy, do
   return FB_OK;
 }
 
+/* ---- FARGO3D output files (output.c) ------------------------------------
+ * Merged field files <dir>/<fluid><field><n>.dat (WriteMerging,
+ * output.c:283-315): the active cells only, as raw doubles, x fastest, then
+ * y, then z; fields dens, energy (the isothermal sound speed, as FARGO3D
+ * stores it), vx, vy and, in 3D, vz.  The reader is the inverse (the
+ * restart path of LowTasks.c:816-1049 with merged files); it replaces the
+ * active cells of the fluid's state and keeps its ghosts. */
+static int dat_path(char *buf, size_t n, const char *dir, const char *fluid, const char *field, int num) {
+  int k = snprintf(buf, n, "%s%s%s%s%d.dat", dir, (*dir && dir[strlen(dir) - 1] != '/') ? "/" : "", fluid, field, num);
+  return k > 0 && (size_t)k < n ? FB_OK : FB_ERR_ARG;
+}
+
+static int dat_write(fb_disk *D, const char *path, const double *full) {
+  FILE *fo = fopen(path, "wb");
+  int j, k, k0 = D->d.is3d ? NG : 0, k1 = D->d.is3d ? D->d.nz + NG : 1;
+  if (!fo) return fail(FB_ERR_ARG, "cannot write %s", path);
+  for (k = k0; k < k1; k++)
+    for (j = NG; j < D->d.ny + NG; j++)
+      if (fwrite(full + (size_t)k * D->d.stride + (size_t)j * D->d.pitch, sizeof(double), D->d.nx, fo) != (size_t)D->d.nx) {
+        fclose(fo);
+        return fail(FB_ERR_ARG, "short write to %s", path);
+      }
+  fclose(fo);
+  return FB_OK;
+}
+
+static int dat_read(fb_disk *D, const char *path, double *full) {
+  FILE *fi = fopen(path, "rb");
+  int j, k, k0 = D->d.is3d ? NG : 0, k1 = D->d.is3d ? D->d.nz + NG : 1;
+  if (!fi) return fail(FB_ERR_ARG, "cannot read %s", path);
+  for (k = k0; k < k1; k++)
+    for (j = NG; j < D->d.ny + NG; j++)
+      if (fread(full + (size_t)k * D->d.stride + (size_t)j * D->d.pitch, sizeof(double), D->d.nx, fi) != (size_t)D->d.nx) {
+        fclose(fi);
+        return fail(FB_ERR_ARG, "%s is shorter than the mesh", path);
+      }
+  fclose(fi);
+  return FB_OK;
+}
+
+int fb_disk_write_dat(fb_disk *D, int f, const char *dir, const char *fluid, int num) {
+  static const char *names[5] = {"dens", "vx", "vy", "vz", "energy"};
+  double *a[5];
+  char path[1024];
+  int q, rc = FB_OK;
+  if (!D || !dir || !fluid || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad arguments");
+  CU(cudaSetDevice(D->device));
+  for (q = 0; q < 5; q++) a[q] = (double *)malloc(sizeof(double) * (size_t)D->ncell);
+  rc = fb_disk_get_state(D, f, a[0], a[1], a[2], a[3]);
+  if (!rc) rc = get(D, a[4], D->d.fl[f].cs);
+  for (q = 0; q < 5 && !rc; q++) {
+    if (q == 3 && !D->d.is3d) continue;
+    if (!(rc = dat_path(path, sizeof path, dir, fluid, names[q], num))) rc = dat_write(D, path, a[q]);
+  }
+  for (q = 0; q < 5; q++) free(a[q]);
+  return rc;
+}
+
+int fb_disk_read_dat(fb_disk *D, int f, const char *dir, const char *fluid, int num) {
+  static const char *names[5] = {"dens", "vx", "vy", "vz", "energy"};
+  double *a[5];
+  char path[1024];
+  int q, rc = FB_OK;
+  if (!D || !dir || !fluid || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad arguments");
+  CU(cudaSetDevice(D->device));
+  for (q = 0; q < 5; q++) a[q] = (double *)malloc(sizeof(double) * (size_t)D->ncell);
+  rc = fb_disk_get_state(D, f, a[0], a[1], a[2], a[3]);   /* ghosts kept */
+  if (!rc) rc = get(D, a[4], D->d.fl[f].cs);
+  for (q = 0; q < 5 && !rc; q++) {
+    if (q == 3 && !D->d.is3d) continue;
+    if (!(rc = dat_path(path, sizeof path, dir, fluid, names[q], num))) rc = dat_read(D, path, a[q]);
+  }
+  if (!rc) rc = fb_disk_set_state(D, f, a[0], a[1], a[2], D->d.is3d ? a[3] : NULL, a[4]);
+  for (q = 0; q < 5; q++) free(a[q]);
+  return rc;
+}
+
+/* planet<k>.dat lines (WritePlanetFile, output.c:46-75): output number,
+ * x, y, z, vx, vy, vz, mass, physical time, OMEGAFRAME. */
+int fb_disk_write_planets(fb_disk *D, const char *dir, int num) {
+  char path[1024];
+  int n;
+  if (!D || !dir) return fail(FB_ERR_ARG, "bad arguments");
+  for (n = 0; n < D->ps.np; n++) {
+    FILE *fo;
+    int k = snprintf(path, sizeof path, "%s%splanet%d.dat", dir, (*dir && dir[strlen(dir) - 1] != '/') ? "/" : "", n);
+    if (k <= 0 || (size_t)k >= sizeof path) return fail(FB_ERR_ARG, "path too long");
+    if (!(fo = fopen(path, "a"))) return fail(FB_ERR_ARG, "cannot append to %s", path);
+    fprintf(fo, "%d\t%#.18g\t%#.18g\t%#.18g\t%#.18g\t%#.18g\t%#.18g\t%#.18g\t%#.18g\t%#.18g\n", num, D->ps.px[n],
+            D->ps.py[n], D->ps.pz[n], D->ps.pvx[n], D->ps.pvy[n], D->ps.pvz[n], D->ps.pmass[n], D->ps.phys_time,
+            D->ps.omegaframe);
+    fclose(fo);
+  }
+  return FB_OK;
+}
+
 static int push_scalars(fb_disk *D) {
   D->sc.omegaframe = D->ps.omegaframe;
   D->sc.omegaframe0 = D->ps.omegaframe0;

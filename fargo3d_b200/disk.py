@@ -80,6 +80,25 @@ class Disk:
     def stream(self) -> int:
         return _abi.lib().fb_disk_stream(self._h)
 
+    @staticmethod
+    def fluid_name(fluid: int) -> str:
+        """FARGO3D's fluid names (setups/fargo_multifluid/condinit.c): gas, dust1, ..."""
+        return "gas" if fluid == 0 else "dust%d" % fluid
+
+    def write_dat(self, outdir: str, n: int):
+        """Every fluid's merged output files <outdir>/<fluid><field><n>.dat
+        (FARGO3D's WriteMerging layout) and the planet files' next line."""
+        L = _abi.lib()
+        for f in range(self.cfg.nfluids):
+            _abi.check(L.fb_disk_write_dat(self._h, f, outdir.encode(), self.fluid_name(f).encode(), n))
+        _abi.check(L.fb_disk_write_planets(self._h, outdir.encode(), n))
+
+    def read_dat(self, outdir: str, n: int):
+        """Replace the active cells of every fluid with output number n."""
+        L = _abi.lib()
+        for f in range(self.cfg.nfluids):
+            _abi.check(L.fb_disk_read_dat(self._h, f, outdir.encode(), self.fluid_name(f).encode(), n))
+
     def close(self):
         if getattr(self, "_h", None):
             _abi.lib().fb_disk_destroy(self._h)

@@ -80,6 +80,18 @@ int fb_disk_step(fb_disk *d, double dt_interval, double *dt_out);
 /* [0] PhysicalTime [1] OMEGAFRAME [2] last dt [3..6] planet 0 x, y, vx, vy [7] Domega */
 int fb_disk_get_scalars(fb_disk *d, double out8[8]);
 
+/* FARGO3D's output files (output.c): merged field files
+ * <dir>/<fluid><field><n>.dat for field = dens, energy (the isothermal sound
+ * speed), vx, vy[, vz] -- active cells, raw doubles, x fastest
+ * (WriteMerging, output.c:283-315) -- and the restart read of the same files
+ * (it replaces the active cells, keeps the ghosts; call fb_disk_initialize
+ * after reading a new run's first state).  fluid is FARGO3D's fluid name
+ * ("gas", "dust1", ...).  fb_disk_write_planets appends one line per planet
+ * to <dir>/planet<k>.dat (WritePlanetFile, output.c:46-75). */
+int fb_disk_write_dat(fb_disk *d, int fluid, const char *dir, const char *fluid_name, int n);
+int fb_disk_read_dat(fb_disk *d, int fluid, const char *dir, const char *fluid_name, int n);
+int fb_disk_write_planets(fb_disk *d, const char *dir, int n);
+
 /* The planetary system and frame rotation (Sys, OMEGAFRAME and the initial
  * OMEGAFRAME0 of main.c:242; psys.c): set
  * replaces the circular orbits built from pl_dist (a running simulation

@@ -1,0 +1,63 @@
+"""FARGO3D output files: merged .dat layout (active cells, x fastest, raw
+doubles), write -> read round trip, planet files (output.c)."""
+import os
+
+import numpy as np
+import pytest
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["cyl2d", "sph3d", "mf"])
+def test_dat_layout_and_round_trip(tmp_path, which):
+    from fargo3d_b200 import Disk, config_fargo2d, config_multifluid, config_p3disof, initial_state
+    cfg = {"cyl2d": config_fargo2d(64, 32, seed=3), "sph3d": config_p3disof(32, 16, 8, seed=4),
+           "mf": config_multifluid(32, 16, nfluids=3, seed=5)}[which]
+    d = Disk(cfg, "fp64")
+    for f in range(cfg.nfluids):
+        d.set_state(*initial_state(cfg, f), fluid=f)
+    d.initialize()
+    d.run(3)
+    out = str(tmp_path)
+    d.write_dat(out, 7)
+    nz = cfg.nz if cfg.is3d else 1
+    g = 3
+    for f in range(cfg.nfluids):
+        st = d.state(f)
+        name = Disk.fluid_name(f)
+        for k in ("rho", "vx", "vy") + (("vz",) if cfg.is3d else ()):
+            field = {"rho": "dens"}.get(k, k)
+            a = np.fromfile(os.path.join(out, "%s%s7.dat" % (name, field)), dtype=np.float64)
+            assert a.size == cfg.nx * cfg.ny * nz
+            active = st[k][g:g + nz, g:g + cfg.ny, :] if cfg.is3d else st[k][0, g:g + cfg.ny, :]
+            assert np.array_equal(a.reshape(active.shape), active), (f, k)
+        assert os.path.exists(os.path.join(out, "%senergy7.dat" % name))
+    # read back into a disk that ran further: the active cells return
+    want = [d.state(f) for f in range(cfg.nfluids)]
+    d.run(2)
+    d.read_dat(out, 7)
+    for f in range(cfg.nfluids):
+        st = d.state(f)
+        sl = (slice(g, g + nz), slice(g, g + cfg.ny)) if cfg.is3d else (0, slice(g, g + cfg.ny))
+        for k in ("rho", "vx", "vy"):
+            assert np.array_equal(st[k][sl], want[f][k][sl]), (f, k)
+    d.close()
+
+
+@pytest.mark.gpu
+def test_planet_file_lines(tmp_path):
+    from fargo3d_b200 import Disk, Planet, config_fargo2d
+    cfg = config_fargo2d(32, 16, seed=6).replace(planets=[Planet(1.0, 1e-3), Planet(1.5, 2e-4)])
+    d = Disk(cfg, "fp64")
+    d.load_initial_state()
+    out = str(tmp_path)
+    for n in range(3):
+        d.run(2)
+        d.write_dat(out, n)
+    sc = d.scalars()
+    for k in range(2):
+        rows = [ln.split("\t") for ln in open(os.path.join(out, "planet%d.dat" % k)).read().splitlines()]
+        assert [int(r[0]) for r in rows] == [0, 1, 2]
+        assert all(len(r) == 10 for r in rows)
+    last = [float(v) for v in open(os.path.join(out, "planet0.dat")).read().splitlines()[-1].split("\t")]
+    assert last[1] == sc[3] and last[2] == sc[4] and last[8] == sc[0] and last[9] == sc[1]
+    d.close()
