@@ -640,13 +640,56 @@ static int get(fb_disk *D, double *dst, const void *src) {
   return FB_OK;
 }
 
+/* Host staging for the state transfers of FP32 disks: one process-wide
+ * pinned buffer (grown on demand, guarded by a lock), so a state moves with
+ * asynchronous copies and a single synchronisation instead of one pageable
+ * copy and wait per field. */
+static pthread_mutex_t g_stage_mu = PTHREAD_MUTEX_INITIALIZER;
+static float *g_stage = NULL;
+static size_t g_stage_n = 0;
+
+static float *stage_lock(size_t n) {
+  pthread_mutex_lock(&g_stage_mu);
+  if (g_stage_n < n) {
+    if (g_stage) cudaFreeHost(g_stage);
+    g_stage = NULL;
+    g_stage_n = 0;
+    if (cudaMallocHost((void **)&g_stage, n * sizeof(float)) != cudaSuccess) {
+      g_stage = NULL;
+      pthread_mutex_unlock(&g_stage_mu);
+      return NULL;
+    }
+    g_stage_n = n;
+  }
+  return g_stage;
+}
+static void stage_unlock(void) { pthread_mutex_unlock(&g_stage_mu); }
+
 int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, const double *vy, const double *vz,
                       const double *cs) {
   fb_fluid_dev *F;
-  int rc;
+  int rc = FB_OK, q;
   if (!D || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
   CU(cudaSetDevice(D->device));
   F = &D->d.fl[f];
+  if (D->d.precision == FB_FP32) {
+    const double *src[5] = {rho, vx, vy, D->d.is3d ? vz : NULL, cs};
+    void *dst[5] = {F->rho, F->vx, F->vy, F->vz, F->cs};
+    const size_t n = (size_t)D->ncell;
+    float *st = stage_lock(5 * n);
+    if (!st) return fail(FB_ERR_CUDA, "pinned staging");
+    for (q = 0; q < 5 && !rc; q++) {
+      size_t i;
+      float *h = st + q * n;
+      if (!src[q] || !dst[q]) continue;
+      for (i = 0; i < n; i++) h[i] = (float)src[q][i];
+      if (cudaMemcpyAsync(dst[q], h, n * sizeof(float), cudaMemcpyHostToDevice, D->stream) != cudaSuccess)
+        rc = fail(FB_ERR_CUDA, "state upload");
+    }
+    if (cudaStreamSynchronize(D->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state upload");
+    stage_unlock();
+    return rc;
+  }
   if ((rc = put(D, F->rho, rho)) || (rc = put(D, F->vx, vx)) || (rc = put(D, F->vy, vy)) ||
       (rc = put(D, F->cs, cs)))
     return rc;
@@ -657,10 +700,30 @@ int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, co
 
 int fb_disk_get_state(fb_disk *D, int f, double *rho, double *vx, double *vy, double *vz) {
   fb_fluid_dev *F;
-  int rc;
+  int rc = FB_OK, q;
   if (!D || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
   CU(cudaSetDevice(D->device));
   F = &D->d.fl[f];
+  if (D->d.precision == FB_FP32) {
+    double *dst[4] = {rho, vx, vy, D->d.is3d ? vz : NULL};
+    const void *src[4] = {F->rho, F->vx, F->vy, F->vz};
+    const size_t n = (size_t)D->ncell;
+    float *st = stage_lock(4 * n);
+    if (!st) return fail(FB_ERR_CUDA, "pinned staging");
+    for (q = 0; q < 4 && !rc; q++)
+      if (dst[q] && src[q] &&
+          cudaMemcpyAsync(st + q * n, src[q], n * sizeof(float), cudaMemcpyDeviceToHost, D->stream) != cudaSuccess)
+        rc = fail(FB_ERR_CUDA, "state download");
+    if (cudaStreamSynchronize(D->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state download");
+    for (q = 0; q < 4 && !rc; q++) {
+      size_t i;
+      if (!dst[q] || !src[q]) continue;
+      for (i = 0; i < n; i++) dst[q][i] = st[q * n + i];
+    }
+    stage_unlock();
+    if (!D->d.is3d && vz) memset(vz, 0, sizeof(double) * D->ncell);
+    return rc;
+  }
   if ((rc = get(D, rho, F->rho)) || (rc = get(D, vx, F->vx)) || (rc = get(D, vy, F->vy))) return rc;
   if (D->d.is3d && (rc = get(D, vz, F->vz))) return rc;
   if (!D->d.is3d && vz) memset(vz, 0, sizeof(double) * D->ncell);
