@@ -372,8 +372,6 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   __syncthreads();
   const double dt = sc.dt;
   const T domega = (T)sc.domega, of = (T)sc.omegaframe;
-  const bool corot = sc.domega != 0.0 || true;
-  (void)corot;
   // stage inputs; vx carries CorrectVtheta (correct_vtheta.c:55-60)
   for (int e = tid; e < H * W; e += TX * TY) {
     const int lj = e / W, li = e - lj * W;
@@ -813,13 +811,7 @@ namespace fb {
 // new state (rho, vx, vy, vz).
 // Correctly rounded division in either precision (IEEE division even where
 // the FP32 build approximates '/').
-__device__ __forceinline__ float div_rn(float a, float b) {
-#ifdef FB_NV_FASTDIV
-  return a / b;
-#else
-  return __fdiv_rn(a, b);
-#endif
-}
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ double div_rn(double a, double b) { return a / b; }
 
 template <typename T, typename S = T>
