@@ -41,14 +41,14 @@ SMEM_MAX = 227 * 1024
 
 def cx_candidates(nx: int, precision: str = "fp32", is3d: bool = False):
     """Widths that tile a ring in 256 threads and whose whole rings per CTA
-    (two buffers of 1 + nq fields and the velocity ring, each padded by one
-    element per 128 bytes) fit in shared memory."""
+    (two buffers of 1 + nq fields and the velocity ring, each row padded by
+    16 bytes) fit in shared memory."""
     esz, nq = (8 if precision == "fp64" else 4), (6 if is3d else 4)
     out = []
     for c in CX_CANDIDATES:
         if nx % c or nx // c > 256:
             continue
-        nxp = nx + (nx >> (5 if esz == 4 else 4)) + 1       # padded ring in shared memory
+        nxp = nx + 16 // esz                                 # padded ring row in shared memory
         if (256 // (nx // c)) * nxp * (2 * (1 + nq) + 1) * esz <= SMEM_MAX:
             out.append(c)
     return out

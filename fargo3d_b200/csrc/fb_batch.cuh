@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? FB_SX_MINB32 : 1) kb_swe
                         nj, nrings, (S *)(b ? F.rho_b : F.rho_a), (S *)(b ? F.mpx_b : F.mpx),
                         (S *)(b ? F.mmx_b : F.mmx), (S *)(b ? F.mpy_b : F.mpy), (S *)(b ? F.mmy_b : F.mmy),
                         (S *)(b ? F.mpz_b : F.mpz), (S *)(b ? F.mmz_b : F.mmz), (const S *)F.vxt, F.vxmed_t, F.nshift,
-                        scp, bid);
+                        scp, (unsigned long long *)D.dtmin + 1, bid);
 }
 
 template <typename T, typename S>

@@ -430,7 +430,7 @@ int fb_disk_set_tiles(fb_disk *D, int cx, int ns) {
     /* whole rings per CTA of 256 threads, two buffers of (1 + nq) fields
      * plus the velocity ring, in the sweep's element size: at most 227 KiB */
     size_t rpc = 256 / (D->d.nx / cx), nq = D->d.is3d ? 6 : 4;
-    size_t nxp = (size_t)D->d.nx + (D->d.nx >> (D->esz == 4 ? 5 : 4)) + 1; /* padded ring */
+    size_t nxp = (size_t)D->d.nx + 16 / D->esz; /* padded ring row */
     size_t bytes = rpc * nxp * (2 * (1 + nq) + 1) * D->esz;
     if (bytes > FB_SMEM_MAX)
       return fail(FB_ERR_ARG, "azimuthal chunk %d on Nx = %d needs %zu bytes of shared memory", cx, D->d.nx, bytes);
@@ -886,6 +886,8 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   }
   CU(cudaMemcpyAsync(D->h_dtmin, D->d.dtmin, 16, cudaMemcpyDeviceToHost, D->stream));
   CU(cudaStreamSynchronize(D->stream));
+  if (((const uint64_t *)D->h_dtmin)[1] & 2)
+    return fail(FB_ERR_NONFINITE, "a staged ring load of the azimuthal sweep did not complete in time");
   if (((const uint64_t *)D->h_dtmin)[1] != 0)
     return fail(FB_ERR_NONFINITE, "non-finite time step or non-positive density in the state");
   /* CflFluidsMin (cfl_fluids_min.c:3-22), the DT clip (main.c:388-395) and

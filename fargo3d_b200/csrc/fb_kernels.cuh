@@ -1197,15 +1197,15 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
                                            int klo, int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,
                                            S *q5, const S *__restrict__ vxt, const double *__restrict__ vxmed_t,
                                            int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp,
-                                           uint3 bid) {
+                                           unsigned long long *__restrict__ errflag, uint3 bid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long mbar;
   T *sm = reinterpret_cast<T *>(smem_raw);
   const int nx = m.nx, tpr = nx / C, rpc = NT / tpr, nf = 1 + nq;
-  // rings in shared memory are padded by one element per 128 bytes, so the
-  // stride-C window reads of a warp fall into distinct banks
-  constexpr int PS = sizeof(T) == 4 ? 5 : 4;
-  const int nxp = nx + (nx >> PS) + 1;
-  auto P = [](int i) { return i + (i >> PS); };
+  // ring rows in shared memory, each padded by 16 bytes (rows stay 16-byte
+  // aligned for the bulk copies and successive rows start in other banks)
+  const int nxp = nx + 16 / (int)sizeof(T);
+  auto P = [](int i) { return i; };
   const int slot = threadIdx.x / tpr, lt = threadIdx.x - slot * tpr, c0 = lt * C;
   const int r = bid.x * rpc + slot;
   const bool active = slot < rpc && r < nrings;
@@ -1217,15 +1217,68 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
   // momenta), then the residual-velocity source vxt [slot][nxp]
   const size_t bufsz = (size_t)rpc * nf * nxp;
   T *bufA = sm, *bufB = sm + bufsz, *svx = sm + 2 * bufsz;
-  for (int e = threadIdx.x; e < rpc * nx; e += NT) {
-    const int s = e / nx, i = e - s * nx, rr = bid.x * rpc + s;
-    if (rr < nrings) {
-      const int jj = jlo + rr % nj, kk = m.is3d ? klo + rr / nj : 0;
-      const long long l = m.l(i, jj, kk);
-      T *b = bufA + (size_t)s * nf * nxp;
-      b[P(i)] = rho[l];
-      for (int q = 0; q < nq; q++) b[(1 + q) * nxp + P(i)] = qg[q][l];
-      svx[s * nxp + P(i)] = vxt[l];
+  // Ring rows are contiguous in HBM: when storage and compute types agree and
+  // every row is 16-byte aligned, one thread hands all rows of this CTA to the
+  // bulk-copy (TMA) engine, completing on an mbarrier; otherwise (FP32
+  // storage with FP64 arithmetic, odd ring lengths) the threads load them.
+  bool bulk = sizeof(S) == sizeof(T) && ((size_t)nx * sizeof(T)) % 16 == 0;
+  if (bulk) {
+    uintptr_t a = (uintptr_t)rho | (uintptr_t)vxt;
+    for (int q = 0; q < nq; q++) a |= (uintptr_t)qg[q];
+    bulk = (a & 15) == 0;
+  }
+  if (bulk) {
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&mbar);
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t row = (uint32_t)(nx * sizeof(T));
+      int nval = 0;
+      for (int s2 = 0; s2 < rpc; s2++)
+        if (bid.x * rpc + s2 < nrings) nval++;
+      const uint32_t total = row * (uint32_t)(nf + 1) * (uint32_t)nval;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total) : "memory");
+      for (int s2 = 0; s2 < rpc; s2++) {
+        const int rr = bid.x * rpc + s2;
+        if (rr >= nrings) continue;
+        const int jj = jlo + rr % nj, kk = m.is3d ? klo + rr / nj : 0;
+        const long long l0 = m.l(0, jj, kk);
+        for (int q = 0; q <= nf; q++) {   // rho, the momenta, vxt
+          const S *src = q == 0 ? rho + l0 : (q < nf ? qg[q - 1] + l0 : vxt + l0);
+          T *dstp = q < nf ? bufA + (size_t)s2 * nf * nxp + (size_t)q * nxp : svx + (size_t)s2 * nxp;
+          asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                       ::"r"((uint32_t)__cvta_generic_to_shared(dstp)), "l"(src), "r"(row), "r"(bar)
+                       : "memory");
+        }
+      }
+    }
+    // bounded wait: past the limit the disk is flagged (its next step stops
+    // it), the copies in flight get a second bounded wait, and the CTA leaves
+    uint32_t done = 0;
+    for (long it = 0; it < (1l << 22) && !done; it++)
+      asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                   : "=r"(done) : "r"(bar), "r"(0) : "memory");
+    if (!done) {
+      if (threadIdx.x == 0) atomicOr(errflag, 2ull);
+      for (long it = 0; it < (1l << 22) && !done; it++)
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(bar), "r"(0) : "memory");
+      return;
+    }
+  } else {
+    for (int e = threadIdx.x; e < rpc * nx; e += NT) {
+      const int s = e / nx, i = e - s * nx, rr = bid.x * rpc + s;
+      if (rr < nrings) {
+        const int jj = jlo + rr % nj, kk = m.is3d ? klo + rr / nj : 0;
+        const long long l = m.l(i, jj, kk);
+        T *b = bufA + (size_t)s * nf * nxp;
+        b[P(i)] = rho[l];
+        for (int q = 0; q < nq; q++) b[(1 + q) * nxp + P(i)] = qg[q][l];
+        svx[s * nxp + P(i)] = vxt[l];
+      }
     }
   }
   __syncthreads();
@@ -1472,7 +1525,7 @@ static __global__ void k_disk_force_fold(const fb_disk_dev D, double x, double y
 // shared memory of b_sweep_x2 for a ring of nx cells (rpc rings per CTA)
 __host__ __device__ inline size_t sweep_x2_smem(int nx, int C, int nt, int nq, size_t esz) {
   const int rpc = nt / (nx / C);
-  const int nxp = nx + (nx >> (esz == 4 ? 5 : 4)) + 1;  // padded ring (b_sweep_x2)
+  const size_t nxp = (size_t)nx + 16 / esz;  // padded ring row (b_sweep_x2)
   return (size_t)rpc * nxp * (2 * (1 + nq) + 1) * esz;
 }
 
@@ -1497,9 +1550,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_sweep_x2(Dims m
                                                   int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,
                                                   S *q5, const S *__restrict__ vxt,
                                                   const double *__restrict__ vxmed_t, int *__restrict__ nshift_out,
-                                                  const fb_scalars *__restrict__ scp) {
+                                                  const fb_scalars *__restrict__ scp,
+                                                  unsigned long long *__restrict__ errflag) {
   b_sweep_x2<T, C, 256, S>(m, g, gd, nq, jlo, klo, nj, nrings, rho, q0, q1, q2, q3, q4, q5, vxt, vxmed_t, nshift_out,
-                        scp, blockIdx);
+                        scp, errflag, blockIdx);
 }
 
 }  // namespace fb

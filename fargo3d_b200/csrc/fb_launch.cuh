@@ -174,7 +174,7 @@ static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
     }                                                                                                      \
     k_sweep_x2<T, CC, S><<<gx, 256, smem, st>>>(m, g, gd, nq, ylo, klo, nj, nrings, rho_out, q[0], q[1], q[2], \
                                              q[3], q[4], q[5], (const S *)F.vxt, F.vxmed_t, F.nshift,      \
-                                             d->scal_dev);                                                 \
+                                             d->scal_dev, (unsigned long long *)d->dtmin + 1);                                                 \
   }
   switch (C) {
     case 16: FB_SX(16) break;
