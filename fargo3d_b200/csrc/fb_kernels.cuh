@@ -1304,27 +1304,54 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
           v[f] = (T)((ntilde - nround) * zx / dtd);
         }
       }
-      T wr[C + 6], rs[C + 1];
+      // the C + 6 values around this thread's cells (halo 3 by wrap); FP32
+      // rings of 4 cells per thread read three aligned float4 blocks (the
+      // left neighbour's, its own, the right neighbour's: conflict-free)
+      constexpr bool VEC = C == 4 && sizeof(T) == 4;
+      const int tm = lt > 0 ? lt - 1 : tpr - 1, tp = lt < tpr - 1 ? lt + 1 : 0;
+      auto window = [&](const T *row, T *w) {
+        if constexpr (VEC) {
+          const float4 a = reinterpret_cast<const float4 *>(row)[tm];
+          const float4 b = reinterpret_cast<const float4 *>(row)[lt];
+          const float4 c = reinterpret_cast<const float4 *>(row)[tp];
+          w[0] = a.y; w[1] = a.z; w[2] = a.w; w[3] = b.x; w[4] = b.y;
+          w[5] = b.z; w[6] = b.w; w[7] = c.x; w[8] = c.y; w[9] = c.z;
+        } else {
 #pragma unroll
-      for (int u = 0; u < C + 6; u++) wr[u] = src[P(wrap(c0 - 3 + u))];
+          for (int u = 0; u < C + 6; u++) w[u] = row[P(wrap(c0 - 3 + u))];
+        }
+      };
+      auto store = [&](T *row, const T *o) {
+        if constexpr (VEC) {
+          reinterpret_cast<float4 *>(row)[lt] = make_float4(o[0], o[1], o[2], o[3]);
+        } else {
+#pragma unroll
+          for (int u = 0; u < C; u++) row[P(c0 + u)] = o[u];
+        }
+      };
+      T wr[C + 6], rs[C + 1], out[C];
+      window(src, wr);
       chunk_iface<T, C>(wr, v, zone, dt, pass == 1, rs);
       for (int q = 0; q < nq; q++) {
         const T *sq = src + (1 + q) * nxp;
-        T wq[C + 6], qs[C + 1];
+        T raw[C + 6], wq[C + 6], qs[C + 1];
+        window(sq, raw);
 #pragma unroll
-        for (int u = 0; u < C + 6; u++) wq[u] = sq[P(wrap(c0 - 3 + u))] / wr[u];  // DivideByRho
+        for (int u = 0; u < C + 6; u++) wq[u] = raw[u] / wr[u];  // DivideByRho
         chunk_iface<T, C>(wq, v, zone, dt, pass == 1, qs);
 #pragma unroll
         for (int u = 0; u < C; u++) {
           const T fl = v[u] * qs[u] * rs[u] - v[u + 1] * qs[u + 1] * rs[u + 1];
-          dst[(1 + q) * nxp + P(c0 + u)] = sq[P(c0 + u)] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+          out[u] = raw[u + 3] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
         }
+        store(dst + (1 + q) * nxp, out);
       }
 #pragma unroll
       for (int u = 0; u < C; u++) {
         const T fl = v[u] * rs[u] - v[u + 1] * rs[u + 1];
-        dst[P(c0 + u)] = wr[u + 3] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+        out[u] = wr[u + 3] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
       }
+      store(dst, out);
     }
     __syncthreads();
   }
