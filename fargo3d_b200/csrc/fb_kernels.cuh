@@ -1285,7 +1285,15 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
   const int sl0 = slot < rpc ? slot : 0;
   const double vm = active ? vxmed_t[j + k * m.sy] : 0.0;
   auto wrap = [&](int i) { i += (i < 0) ? nx : 0; i -= (i >= nx) ? nx : 0; return i; };
-  auto zone = [&](int u) -> T { return zsx(m, g, wrap(c0 - 2 + u), j, k); };
+  // FP32: the azimuthal spacing is uniform (FARGO's shift requires it), so a
+  // ring's zone size is one value, formed once in FP64, instead of a table
+  // load per window cell and quantity; FP64 keeps the reference's per-cell
+  // zone_size_x
+  const T zring = (T)((ld(gd.xmin + 1) - ld(gd.xmin + 0)) * ld(gd.ymed + j) * (m.sph ? ld(gd.sin_zmed + k) : 1.0));
+  auto zone = [&](int u) -> T {
+    if constexpr (sizeof(T) == 4) return zring;
+    else return zsx(m, g, wrap(c0 - 2 + u), j, k);
+  };
   const T sxj = ld(g.sxj + j), sxk = ld(g.sxk + k), ivj = ld(g.invvj + j), syk = ld(g.syk + k);
   for (int pass = 0; pass < 2; pass++) {
     const T *src = (pass == 0 ? bufA : bufB) + (size_t)sl0 * nf * nxp;
