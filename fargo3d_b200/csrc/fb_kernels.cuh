@@ -1295,6 +1295,14 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
     else return zsx(m, g, wrap(c0 - 2 + u), j, k);
   };
   const T sxj = ld(g.sxj + j), sxk = ld(g.sxk + k), ivj = ld(g.invvj + j), syk = ld(g.syk + k);
+  // FP32: with uniform spacing the update factor dt Surf / Vol is one value
+  // per ring (formed in FP64); FP64 keeps the reference's per-cell form
+  const T upd_ring = (T)((double)ld(gd.sxj + j) * ld(gd.sxk + k) * dtd * ld(gd.invvj + j) /
+                         ((double)ld(gd.syk + k) * ld(gd.sxi + 0)));
+  auto upd = [&](int u) -> T {
+    if constexpr (sizeof(T) == 4) return upd_ring;
+    else return sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+  };
   for (int pass = 0; pass < 2; pass++) {
     const T *src = (pass == 0 ? bufA : bufB) + (size_t)sl0 * nf * nxp;
     T *dst = (pass == 0 ? bufB : bufA) + (size_t)sl0 * nf * nxp;
@@ -1350,14 +1358,14 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
 #pragma unroll
         for (int u = 0; u < C; u++) {
           const T fl = v[u] * qs[u] * rs[u] - v[u + 1] * qs[u + 1] * rs[u + 1];
-          out[u] = raw[u + 3] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+          out[u] = raw[u + 3] + (sizeof(T) == 4 ? fl * upd(u) : fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u)));
         }
         store(dst + (1 + q) * nxp, out);
       }
 #pragma unroll
       for (int u = 0; u < C; u++) {
         const T fl = v[u] * rs[u] - v[u + 1] * rs[u + 1];
-        out[u] = wr[u + 3] + fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u));
+        out[u] = wr[u + 3] + (sizeof(T) == 4 ? fl * upd(u) : fl * sxj * sxk * dt * ivj / (syk * ld(g.sxi + c0 + u)));
       }
       store(dst, out);
     }
