@@ -404,12 +404,14 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
       if (m.alpha) visc = alpha * (TV)s_cs[lj][li] * (TV)s_cs[lj][li] * (TV)ld(g.visc_j + j);
       if (li <= TX && lj <= TY) {
         const TV r = (TV)s_rho[lj][li];
-        const TV sxi = (TV)ld(g.sxi + i), syk = (TV)ld(g.syk + 0), sxk = (TV)ld(g.sxk + 0);
+        // FP32 storage: uniform azimuthal spacing, the x factors of cell 0
+        const int ix = FAST ? 0 : i;
+        const TV sxi = (TV)ld(g.sxi + ix), syk = (TV)ld(g.syk + 0), sxk = (TV)ld(g.sxk + 0);
         TV div_v = 0.0;
         div_v += (TV)(s_vx[lj][li + 1] - s_vx[lj][li]) * (TV)ld(g.sxj + j) * sxk;
         div_v += ((TV)s_vy[lj + 1][li] * (TV)ld(g.syj + j + 1) * syk * sxi - (TV)s_vy[lj][li] * (TV)ld(g.syj + j) * syk * sxi);
         div_v *= (TV)(2.0 / 3.0) * (TV)ld(g.invvj + j) / (syk * sxi);
-        TV txx = visc * r * ((TV)2.0 * (TV)(s_vx[lj][li + 1] - s_vx[lj][li]) / (TV)zsx(m, g, i, j, 0) - div_v);
+        TV txx = visc * r * ((TV)2.0 * (TV)(s_vx[lj][li + 1] - s_vx[lj][li]) / (TV)zsx(m, g, ix, j, 0) - div_v);
         txx += visc * r * (TV)(s_vy[lj + 1][li] + s_vy[lj][li]) / (TV)ld(g.ymed + j);
         s_txx[lj][li] = txx;
         s_tyy[lj][li] = visc * r * ((TV)2.0 * (TV)(s_vy[lj + 1][li] - s_vy[lj][li]) /
@@ -418,7 +420,7 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
       if (li >= 1 && lj >= 1) {
         s_tyx[lj][li] = viscm * (TV)0.25 *
                         (TV)(s_rho[lj][li] + s_rho[lj][li - 1] + s_rho[lj - 1][li] + s_rho[lj - 1][li - 1]) *
-                        ((TV)(s_vy[lj][li] - s_vy[lj][li - 1]) * (TV)ld(g.invdiffxmed + i) / (TV)ld(g.ymin + j) +
+                        ((TV)(s_vy[lj][li] - s_vy[lj][li - 1]) * (TV)ld(g.invdiffxmed + (FAST ? 0 : i)) / (TV)ld(g.ymin + j) +
                          (TV)(s_vx[lj][li] - s_vx[lj - 1][li]) / (TV)(ld(g.ymed + j) - ld(g.ymed + j - 1)) -
                          (TV)0.5 * (TV)(s_vx[lj][li] + s_vx[lj - 1][li]) / (TV)ld(g.ymin + j));
       }
@@ -429,15 +431,17 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
   if (i >= m.nx || j > m.ny + FB_NGH - 1) return;
   const int im = wrapx(i - 1, m.nx);
+  // FP32 storage: uniform azimuthal spacing, the x factors of cell 0
+  const int ix = FAST ? 0 : i, ixm = FAST ? 0 : im;
   const long long l = m.l(i, j, 0);
   const T r = s_rho[lj][li], rxm = s_rho[lj][li - 1], rym = s_rho[lj - 1][li];
-  const T izx = FAST ? ld(g.invdiffxmed + i) * ld(g.inv_ymed + j) : izsxmed(m, g, i, j, 0);
+  const T izx = FAST ? ld(g.invdiffxmed + ix) * ld(g.inv_ymed + j) : izsxmed(m, g, i, j, 0);
   // SubStep1_x (substep1_x.c:107-117)
-  const T dxmed = (T)0.5 * (ld(g.sxi + i) + ld(g.sxi + im));
+  const T dxmed = (T)0.5 * (ld(g.sxi + ix) + ld(g.sxi + ixm));
   T idenx = 0, ideny = 0;
   T dtorx;
   if (FAST) {
-    idenx = (T)1.0 / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im));
+    idenx = (T)1.0 / (r * ld(g.sxi + ix) + rxm * ld(g.sxi + ixm));
     dtorx = (T)2. * (T)dt * idenx * dxmed;
   } else {
     dtorx = (T)2. * (T)dt / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * dxmed;
@@ -478,7 +482,7 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
               ((vyip - vyi) * vym * vym * (vrxm + vr)) * vdt);
     ay += (T)((TV)2.0 * (vym * s_tyy[lj][li] - vymm * s_tyy[lj - 1][li]) / ((vym - vymm) * (vr + vrym) * vyi) * vdt);
     ay += (T)((TV)2.0 * (s_tyx[lj][li + 1] - s_tyx[lj][li]) /
-              ((TV)(ld(g.xmin + i + 1) - ld(g.xmin + i)) * vyi * (vr + vrym)) * vdt);
+              ((TV)(FAST ? ld(g.sxi + ix) : ld(g.xmin + i + 1) - ld(g.xmin + i)) * vyi * (vr + vrym)) * vdt);
     ay -= (T)((s_txx[lj][li] + s_txx[lj - 1][li]) / (vyi * (vr + vrym)) * vdt);
   }
   // SubStep2_a / SubStep2_b (substep2_a.c:107-129, substep2_b.c:150-175)
