@@ -33,10 +33,10 @@ constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_BX = 128
               NV_BX = 128;
 
 // resident CTAs per SM the FP32-storage kernels are compiled for (register
-// caps 64 / 64 / 128: measured on the batched 64-disk step, where the
+// caps 40 / 64 / 128: measured on the batched 64-disk step, where the
 // latency-bound kernels gain more from occupancy than they lose to spills)
 #ifndef FB_SRC_MINB
-#define FB_SRC_MINB 4
+#define FB_SRC_MINB 6
 #endif
 #ifndef FB_SX_MINB32
 #define FB_SX_MINB32 4
