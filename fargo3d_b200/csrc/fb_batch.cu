@@ -25,6 +25,10 @@ Prof *g_prof = nullptr;
 extern "C" int fb_batch_launch_step_f64(fb_batch *B, double DT);
 extern "C" int fb_batch_launch_step_f32(fb_batch *B, double DT);
 extern "C" size_t fb_batch_sweep_x_esz_f32(void);
+// fb_host.c: lend a region of one batch-wide allocation and the batch's
+// stream to the next fb_disk_create on this thread
+extern "C" void fb_disk_internal_provide(void *arena, size_t size, void *stream);
+extern "C" size_t fb_disk_internal_arena_bytes(const fb_params *p, int precision);
 
 static int launch_step_any(fb_batch *B, double DT) {
   return B->precision == FB_FP64 ? fb_batch_launch_step_f64(B, DT) : fb_batch_launch_step_f32(B, DT);
@@ -82,6 +86,7 @@ int fb_batch_destroy(fb_batch *B) {
   if (B->d_psys) cudaFree(B->d_psys);
   for (fb_disk *d : B->disks)
     if (d) fb_disk_destroy(d);
+  if (B->arena) cudaFree(B->arena);
   if (B->stream) cudaStreamDestroy(B->stream);
   delete B;
   return FB_OK;
@@ -191,9 +196,23 @@ int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_ba
   fb_batch *B = nullptr;
   int rc = fb_batch_create_slots(n, precision, device, ps[0].nz > 1, ps[0].nfluids, &B);
   if (rc) return rc;
+  // one zeroed allocation for every member's arena and the batch's stream
+  // for all of them: creation costs one cudaMalloc + one memset in total
+  std::vector<size_t> off(n + 1, 0);
+  for (int i = 0; i < n; i++) off[i + 1] = off[i] + ((fb_disk_internal_arena_bytes(&ps[i], precision) + 255) & ~(size_t)255);
+  if (off[n] > 0 && cudaMalloc((void **)&B->arena, off[n]) == cudaSuccess &&
+      cudaMemsetAsync(B->arena, 0, off[n], B->stream) == cudaSuccess &&
+      cudaStreamSynchronize(B->stream) == cudaSuccess) {
+  } else {
+    if (B->arena) cudaFree(B->arena);
+    B->arena = nullptr;   // members allocate their own
+    cudaGetLastError();
+  }
   for (int i = 0; i < n; i++) {
     int s;
+    if (B->arena) fb_disk_internal_provide(B->arena + off[i], off[i + 1] - off[i], B->stream);
     rc = fb_batch_add(B, &ps[i], 0.0, &s);
+    fb_disk_internal_provide(nullptr, 0, nullptr);
     if (rc) { fb_batch_destroy(B); return rc; }
   }
   *out = B;

@@ -216,6 +216,7 @@ struct fb_batch {
   std::vector<int> state;
   std::vector<double> t_end;
   int dirty;
+  char *arena;   // one allocation lent to the members of fb_batch_create (or null)
   cudaStream_t stream;
   std::vector<fb_disk *> disks;
   fb_disk_dev *d_disks;

@@ -87,6 +87,7 @@ struct fb_disk {
      cudaMalloc + one memset instead of one of each per array) */
   char *arena;
   size_t arena_size, arena_used;
+  int arena_owned, stream_owned;  /* 0: lent by a batch (fb_disk_internal_provide) */
   char *hstage;                 /* host image of the arena's table region, sent in one copy */
   size_t hstage_size, hstage_hi;
   /* optional per-launch timing (fb_disk_profile) */
@@ -458,6 +459,27 @@ int fb_disk_bytes(fb_disk *D, size_t *out) {
 #define LAUNCH(name, ...) \
   (D->d.precision == FB_FP64 ? fb_launch_##name##_f64(__VA_ARGS__) : fb_launch_##name##_f32(__VA_ARGS__))
 
+/* A batch creating all its members at once lends each one a zeroed region of
+ * one batch-wide allocation and the batch's stream: the next fb_disk_create
+ * on this thread uses them instead of its own cudaMalloc / stream. */
+static __thread char *g_lent_arena = NULL;
+static __thread size_t g_lent_size = 0;
+static __thread cudaStream_t g_lent_stream = NULL;
+
+void fb_disk_internal_provide(void *arena, size_t size, void *stream) {
+  g_lent_arena = (char *)arena;
+  g_lent_size = size;
+  g_lent_stream = (cudaStream_t)stream;
+}
+
+/* device bytes one disk's arena takes: the fields and tables bound plus
+ * 256-byte alignment of every carved array */
+size_t fb_disk_internal_arena_bytes(const fb_params *p, int precision) {
+  size_t est = 0;
+  if (fb_params_bytes(p, precision, &est) != FB_OK) return 0;
+  return est + (size_t)MAXALLOC * 256;
+}
+
 int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out) {
   fb_disk *D;
   int f, n, rc, ndev = 0;
@@ -507,23 +529,36 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
   D->sxk = calloc(D->d.sz, 8); D->syk = calloc(D->d.sz, 8); D->szk = calloc(D->d.sz, 8);
   mesh(D);
   D->d.mindx = D->mindx;
-  if (cudaStreamCreateWithFlags(&D->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    fb_disk_destroy(D);
-    return fail(FB_ERR_CUDA, "cudaStreamCreate failed");
+  if (g_lent_stream) {
+    D->stream = g_lent_stream;
+    D->stream_owned = 0;
+  } else {
+    if (cudaStreamCreateWithFlags(&D->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      D->stream = NULL;
+      fb_disk_destroy(D);
+      return fail(FB_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    D->stream_owned = 1;
   }
-  {
-    size_t est = 0;
-    if (fb_params_bytes(p, precision, &est) == FB_OK) {
-      est += (size_t)MAXALLOC * 256; /* alignment of each carved array */
-      if (cudaMalloc((void **)&D->arena, est) == cudaSuccess && cudaMemset(D->arena, 0, est) == cudaSuccess)
-        D->arena_size = est;
-      else {
-        if (D->arena) cudaFree(D->arena);
-        D->arena = NULL;     /* fall back to one allocation per array */
-        cudaGetLastError();
-      }
+  if (g_lent_arena && g_lent_size >= fb_disk_internal_arena_bytes(p, precision)) {
+    D->arena = g_lent_arena;   /* zeroed by the lender */
+    D->arena_size = g_lent_size;
+    D->arena_owned = 0;
+  } else {
+    size_t est = fb_disk_internal_arena_bytes(p, precision);
+    if (est && cudaMalloc((void **)&D->arena, est) == cudaSuccess && cudaMemsetAsync(D->arena, 0, est, D->stream) == cudaSuccess &&
+        cudaStreamSynchronize(D->stream) == cudaSuccess) {
+      D->arena_size = est;
+      D->arena_owned = 1;
+    } else {
+      if (D->arena && D->arena_owned) cudaFree(D->arena);
+      D->arena = NULL;     /* fall back to one allocation per array */
+      cudaGetLastError();
     }
   }
+  g_lent_arena = NULL;
+  g_lent_size = 0;
+  g_lent_stream = NULL;
   if (D->arena) {  /* host image of the table region (tables are carved first) */
     size_t sy = (size_t)D->d.sy, sz = (size_t)D->d.sz;
     D->hstage_size = 2 * sizeof(double) * (6 * ((size_t)p->nx + 1) + 32 * (sy + 1) + 24 * (sz + 1)) +
@@ -595,11 +630,11 @@ int fb_disk_destroy(fb_disk *D) {
   if (D->device >= 0) cudaSetDevice(D->device);
   if (D->stream) cudaStreamSynchronize(D->stream);
   for (i = 0; i < D->nalloc; i++) cudaFree(D->allocs[i]);
-  if (D->arena) cudaFree(D->arena);
+  if (D->arena && D->arena_owned) cudaFree(D->arena);
   if (D->h_dtmin) pinned_release(D->h_dtmin);
   for (i = 0; i < 32; i++)
     if (D->ev[i]) cudaEventDestroy(D->ev[i]);
-  if (D->stream) cudaStreamDestroy(D->stream);
+  if (D->stream && D->stream_owned) cudaStreamDestroy(D->stream);
   free(D->xmin); free(D->ymin); free(D->zmin); free(D->xmed); free(D->ymed); free(D->zmed);
   free(D->invdiffxmed); free(D->sxi); free(D->sxj); free(D->syj); free(D->szj); free(D->invvj);
   free(D->sxk); free(D->syk); free(D->szk);
