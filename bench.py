@@ -312,6 +312,10 @@ def run_ours(args, rank, world, local_rank):
     # end-to-end through the public API from pinned host buffers
     pinned = [[[torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in st] for st in sts]
               for sts in inits]
+    # result buffers, page-locked like the inputs (vz only for 3D disks)
+    keys = ("rho", "vx", "vy", "vz") if dim == "3d" else ("rho", "vx", "vy")
+    results = [[{k: torch.empty(c.shape, dtype=torch.float64).pin_memory().numpy() for k in keys}
+                for _ in range(nf)] for c in cfgs]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     if batched:
@@ -321,14 +325,14 @@ def run_ours(args, rank, world, local_rank):
                 r2.set_state(i, *[p.numpy() for p in st], fluid=f)
         r2.initialize()
         r2.run(args.steps)
-        outs = [r2.state(i, fluid=f) for i in range(len(cfgs)) for f in range(nf)]
+        outs = [r2.state(i, fluid=f, out=results[i][f]) for i in range(len(cfgs)) for f in range(nf)]
     else:
         r2 = Disk(cfgs[0], precision, device=local_rank)
         for f, st in enumerate(pinned[0]):
             r2.set_state(*[p.numpy() for p in st], fluid=f)
         r2.initialize()
         r2.run(args.steps)
-        outs = [r2.state(f) for f in range(nf)]
+        outs = [r2.state(f, out=results[0][f]) for f in range(nf)]
     t_e2e = time.perf_counter() - t0
     r2.close()
     nstored = sum(int(np.prod(c.shape)) for c in cfgs) * nf
@@ -342,8 +346,8 @@ def run_ours(args, rank, world, local_rank):
                    "mode": "batched launches + CUDA graph" if batched else "plain, one disk",
                    "l2": "state (%d MB) larger than L2 (126 MB); no flush needed" % (nstored * esz * 5 // 2 ** 20)},
         "e2e": {"value": cells * args.steps * world / t_e2e, "unit": "cell-updates/s",
-                "h2d_bytes_per_step": 5 * nstored * 8 / args.steps,
-                "d2h_bytes_per_step": 4 * nstored * 8 / args.steps + (0 if batched else 16)},
+                "h2d_bytes_per_step": (5 if dim == "3d" else 4) * nstored * 8 / args.steps,
+                "d2h_bytes_per_step": len(keys) * nstored * 8 / args.steps + (0 if batched else 16)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
                      "traffic": TRAFFIC_BYTES.get((args.workload, precision), {}).get(dom),

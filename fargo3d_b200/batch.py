@@ -11,6 +11,7 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
+from .disk import _out_arrays
 from .setups import initial_state
 
 
@@ -68,13 +69,17 @@ class Batch:
     def sync(self):
         _abi.check(_abi.lib().fb_batch_sync(self._h))
 
-    def state(self, i, fluid: int = 0):
+    def state(self, i, fluid: int = 0, out: dict | None = None):
+        """Disk i's current fields as float64 arrays (``out``: preallocated
+        arrays to fill, as for :meth:`Disk.state`)."""
         self.sync()
         m = self._members[i]
-        out = [np.empty(m.shape) for _ in range(4)]
-        p = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in out]
+        is3d = self.cfgs[i].nz > 1
+        res = _out_arrays(m.shape, is3d, out)
+        p = [res[k].ctypes.data_as(C.POINTER(C.c_double)) if (k != "vz" or is3d) else None
+             for k in ("rho", "vx", "vy", "vz")]
         _abi.check(_abi.lib().fb_disk_get_state(m._h, fluid, *p))
-        return {"rho": out[0], "vx": out[1], "vy": out[2], "vz": out[3]}
+        return res
 
     def scalars(self, i):
         o = np.zeros(8)

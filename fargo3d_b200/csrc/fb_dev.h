@@ -103,6 +103,8 @@ struct fb_psys_s *fb_disk_internal_psys(struct fb_disk *d);
 void *fb_disk_internal_scalars(struct fb_disk *d);
 size_t fb_disk_internal_esz(struct fb_disk *d);
 int fb_internal_fail(int code, const char *what, int cuda_err);
+/* FP64 <-> FP32 copy of n values on the device (fb_kernels_f64.cu) */
+int fb_launch_convert(void *dst, const void *src, size_t n, int to_f32, void *stream);
 
 #ifdef __cplusplus
 }

@@ -675,30 +675,50 @@ static int get(fb_disk *D, double *dst, const void *src) {
   return FB_OK;
 }
 
-/* Host staging for the state transfers of FP32 disks: one process-wide
- * pinned buffer (grown on demand, guarded by a lock), so a state moves with
- * asynchronous copies and a single synchronisation instead of one pageable
- * copy and wait per field. */
+/* Device staging for the state transfers of FP32 disks: one chunk buffer
+ * per device (made on first use, kept for the life of the process, guarded
+ * by a lock; outside the disks' own arenas).  The caller's doubles are
+ * copied into it as they are, a chunk at a time, and rounded to the FP32
+ * field by a kernel on the disk's stream (and the reverse for reads), so a
+ * page-locked caller buffer moves by DMA with no host-side conversion. */
+#define FB_MAXDEV 64
+#define DSTAGE_N ((size_t)4 << 20) /* doubles per chunk (32 MB) */
 static pthread_mutex_t g_stage_mu = PTHREAD_MUTEX_INITIALIZER;
-static float *g_stage = NULL;
-static size_t g_stage_n = 0;
+static double *g_dstage[FB_MAXDEV];
 
-static float *stage_lock(size_t n) {
+static double *dstage_lock(int device) {
   pthread_mutex_lock(&g_stage_mu);
-  if (g_stage_n < n) {
-    if (g_stage) cudaFreeHost(g_stage);
-    g_stage = NULL;
-    g_stage_n = 0;
-    if (cudaMallocHost((void **)&g_stage, n * sizeof(float)) != cudaSuccess) {
-      g_stage = NULL;
-      pthread_mutex_unlock(&g_stage_mu);
-      return NULL;
-    }
-    g_stage_n = n;
+  if (device < 0 || device >= FB_MAXDEV) {
+    pthread_mutex_unlock(&g_stage_mu);
+    return NULL;
   }
-  return g_stage;
+  if (!g_dstage[device] && cudaMalloc((void **)&g_dstage[device], DSTAGE_N * sizeof(double)) != cudaSuccess) {
+    g_dstage[device] = NULL;
+    cudaGetLastError();
+    pthread_mutex_unlock(&g_stage_mu);
+    return NULL;
+  }
+  return g_dstage[device];
 }
 static void stage_unlock(void) { pthread_mutex_unlock(&g_stage_mu); }
+
+/* host doubles -> FP32 field (to_f32) or FP32 field -> host doubles */
+static int stage_move(fb_disk *D, double *st, double *host, void *field, size_t n, int to_f32) {
+  size_t o;
+  for (o = 0; o < n; o += DSTAGE_N) {
+    size_t c = n - o < DSTAGE_N ? n - o : DSTAGE_N;
+    if (to_f32) {
+      if (cudaMemcpyAsync(st, host + o, c * sizeof(double), cudaMemcpyHostToDevice, D->stream) != cudaSuccess ||
+          fb_launch_convert((float *)field + o, st, c, 1, D->stream) != cudaSuccess)
+        return 1;
+    } else {
+      if (fb_launch_convert(st, (float *)field + o, c, 0, D->stream) != cudaSuccess ||
+          cudaMemcpyAsync(host + o, st, c * sizeof(double), cudaMemcpyDeviceToHost, D->stream) != cudaSuccess)
+        return 1;
+    }
+  }
+  return 0;
+}
 
 int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, const double *vy, const double *vz,
                       const double *cs) {
@@ -711,16 +731,11 @@ int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, co
     const double *src[5] = {rho, vx, vy, D->d.is3d ? vz : NULL, cs};
     void *dst[5] = {F->rho, F->vx, F->vy, F->vz, F->cs};
     const size_t n = (size_t)D->ncell;
-    float *st = stage_lock(5 * n);
-    if (!st) return fail(FB_ERR_CUDA, "pinned staging");
-    for (q = 0; q < 5 && !rc; q++) {
-      size_t i;
-      float *h = st + q * n;
-      if (!src[q] || !dst[q]) continue;
-      for (i = 0; i < n; i++) h[i] = (float)src[q][i];
-      if (cudaMemcpyAsync(dst[q], h, n * sizeof(float), cudaMemcpyHostToDevice, D->stream) != cudaSuccess)
+    double *st = dstage_lock(D->device);
+    if (!st) return fail(FB_ERR_CUDA, "device staging");
+    for (q = 0; q < 5 && !rc; q++)
+      if (src[q] && dst[q] && stage_move(D, st, (double *)src[q], dst[q], n, 1))
         rc = fail(FB_ERR_CUDA, "state upload");
-    }
     if (cudaStreamSynchronize(D->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state upload");
     stage_unlock();
     return rc;
@@ -743,18 +758,12 @@ int fb_disk_get_state(fb_disk *D, int f, double *rho, double *vx, double *vy, do
     double *dst[4] = {rho, vx, vy, D->d.is3d ? vz : NULL};
     const void *src[4] = {F->rho, F->vx, F->vy, F->vz};
     const size_t n = (size_t)D->ncell;
-    float *st = stage_lock(4 * n);
-    if (!st) return fail(FB_ERR_CUDA, "pinned staging");
+    double *st = dstage_lock(D->device);
+    if (!st) return fail(FB_ERR_CUDA, "device staging");
     for (q = 0; q < 4 && !rc; q++)
-      if (dst[q] && src[q] &&
-          cudaMemcpyAsync(st + q * n, src[q], n * sizeof(float), cudaMemcpyDeviceToHost, D->stream) != cudaSuccess)
+      if (dst[q] && src[q] && stage_move(D, st, dst[q], (void *)src[q], n, 0))
         rc = fail(FB_ERR_CUDA, "state download");
     if (cudaStreamSynchronize(D->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state download");
-    for (q = 0; q < 4 && !rc; q++) {
-      size_t i;
-      if (!dst[q] || !src[q]) continue;
-      for (i = 0; i < n; i++) dst[q][i] = st[q * n + i];
-    }
     stage_unlock();
     if (!D->d.is3d && vz) memset(vz, 0, sizeof(double) * D->ncell);
     return rc;

@@ -14,6 +14,20 @@ from . import _abi
 from .setups import DiskConfig, initial_state
 
 
+def _out_arrays(shape, is3d: bool, out):
+    res = {}
+    for k in ("rho", "vx", "vy", "vz"):
+        a = None if out is None else out.get(k)
+        if a is None:
+            a = np.empty(shape) if (k != "vz" or is3d) else np.zeros(shape)
+        elif not (a.dtype == np.float64 and a.flags.c_contiguous and a.size == int(np.prod(shape))):
+            raise ValueError("out[%r] must be a C-contiguous float64 array of %d values" % (k, int(np.prod(shape))))
+        elif k == "vz" and not is3d:
+            a.fill(0.0)
+        res[k] = a.reshape(shape)
+    return res
+
+
 def _ptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
 
@@ -43,10 +57,14 @@ class Disk:
                 for a in (rho, vx, vy, vz, cs)]
         _abi.check(_abi.lib().fb_disk_set_state(self._h, fluid, *[_ptr(a) for a in arrs]))
 
-    def state(self, fluid: int = 0):
-        out = [np.empty(self.shape) for _ in range(4)]
-        _abi.check(_abi.lib().fb_disk_get_state(self._h, fluid, *[_ptr(a) for a in out]))
-        return {"rho": out[0], "vx": out[1], "vy": out[2], "vz": out[3]}
+    def state(self, fluid: int = 0, out: dict | None = None):
+        """Current fields as float64 arrays.  ``out`` may hold preallocated
+        C-contiguous float64 arrays (page-locked ones move by DMA) for any of
+        rho / vx / vy / vz; vz of a 2D disk is zero and not read back."""
+        res = _out_arrays(self.shape, self.cfg.nz > 1, out)
+        p = [_ptr(res[k]) if (k != "vz" or self.cfg.nz > 1) else None for k in ("rho", "vx", "vy", "vz")]
+        _abi.check(_abi.lib().fb_disk_get_state(self._h, fluid, *p))
+        return res
 
     def initialize(self):
         _abi.check(_abi.lib().fb_disk_initialize(self._h))

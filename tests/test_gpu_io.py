@@ -61,3 +61,35 @@ def test_planet_file_lines(tmp_path):
     last = [float(v) for v in open(os.path.join(out, "planet0.dat")).read().splitlines()[-1].split("\t")]
     assert last[1] == sc[3] and last[2] == sc[4] and last[8] == sc[0] and last[9] == sc[1]
     d.close()
+
+
+@pytest.mark.gpu
+def test_fp32_state_transfer_rounds_like_a_host_cast():
+    """FP32 disks take the caller's doubles over the bus and round them on the
+    device: the stored values are the host's (float) casts, subnormals and
+    ties to even included, across staging-chunk boundaries (a disk of more
+    than 4 Mi values), into caller-supplied page-locked buffers too."""
+    import torch
+    from fargo3d_b200 import Disk, config_fargo2d
+    cfg = config_fargo2d(2048, 2048, seed=5)
+    n = int(np.prod(cfg.shape))
+    assert n > 4 << 20
+    rng = np.random.default_rng(7)
+    vals = [rng.standard_normal(n) * 10.0 ** rng.integers(-46, 37, n) for _ in range(4)]
+    vals[0][:8] = [0.0, -0.0, 1e-40, -3e-42, 1.5e-45, 3.0e38, 2.9e-39, 1.0 + 2.0 ** -24]
+    vals[1][n - 3:] = [1.0 + 3 * 2.0 ** -24, -1e-44, 7.0]
+    rho, vx, vy, cs = [v.reshape(cfg.shape) for v in vals]
+    d = Disk(cfg, "fp32")
+    d.set_state(rho, vx, vy, None, cs)
+    got = d.state()
+    for k, v in (("rho", rho), ("vx", vx), ("vy", vy)):
+        assert np.array_equal(got[k], v.astype(np.float32).astype(np.float64)), k
+    assert got["vz"].shape == cfg.shape and not got["vz"].any()
+    out = {k: torch.empty(cfg.shape, dtype=torch.float64).pin_memory().numpy() for k in ("rho", "vx", "vy")}
+    got2 = d.state(out=out)
+    for k in out:
+        assert np.shares_memory(got2[k], out[k])
+        assert np.array_equal(got2[k], got[k]), k
+    with pytest.raises(ValueError):
+        d.state(out={"rho": np.empty(10)})
+    d.close()
