@@ -21,8 +21,10 @@
 
 #ifdef __CUDACC__
 #define FB_HD __host__ __device__
+#define FB_FI __forceinline__
 #else
 #define FB_HD
+#define FB_FI inline
 #endif
 
 #define FB_G 1.0
@@ -103,8 +105,8 @@ static FB_HD inline void fb_psys_rotate(fb_psys *S, double angle) {
   }
 }
 
-static FB_HD inline void fb_nbody_deriv(const fb_psys *S, const double *q, const double *ms, double *der, int n,
-                                        double dt) {
+static FB_HD FB_FI void fb_nbody_deriv(const fb_psys *S, const double *q, const double *ms, double *der, int n,
+                                       double dt) {
   const double *x = q, *y = q + n, *z = q + 2 * n, *vx = q + 3 * n, *vy = q + 4 * n, *vz = q + 5 * n;
   double dist[FB_MAXPLANETS], coef, dd;
   int i, j;
@@ -130,13 +132,14 @@ static FB_HD inline void fb_nbody_deriv(const fb_psys *S, const double *q, const
   for (i = 0; i < 6 * n; i++) der[i] *= dt;
 }
 
-static FB_HD inline void fb_nbody_rk5(fb_psys *S, double dt) {
+static FB_HD FB_FI void fb_nbody_rk5_n(fb_psys *S, double dt, const int n) {
   enum { M6 = 6 * FB_MAXPLANETS };
-  int n = S->np, i;
+  int i;
   double q0[M6], q1[M6], ms[FB_MAXPLANETS];
   double k1[M6], k2[M6], k3[M6], k4[M6], k5[M6], k6[M6];
   if (!n) return;
-  for (i = 0; i < M6; i++) { q0[i] = q1[i] = k1[i] = k2[i] = k3[i] = k4[i] = k5[i] = k6[i] = 0.0; }
+  /* the stages read k2..k5 (times 0.0) before writing them: zero the used part */
+  for (i = 0; i < 6 * n; i++) { k2[i] = k3[i] = k4[i] = k5[i] = 0.0; }
   for (i = 0; i < n; i++) {
     q0[i] = S->px[i]; q0[i + n] = S->py[i]; q0[i + 2 * n] = S->pz[i];
     q0[i + 3 * n] = S->pvx[i]; q0[i + 4 * n] = S->pvy[i]; q0[i + 5 * n] = S->pvz[i];
@@ -162,6 +165,13 @@ static FB_HD inline void fb_nbody_rk5(fb_psys *S, double dt) {
     S->px[i] = q1[i]; S->py[i] = q1[i + n]; S->pz[i] = q1[i + 2 * n];
     S->pvx[i] = q1[i + 3 * n]; S->pvy[i] = q1[i + 4 * n]; S->pvz[i] = q1[i + 5 * n];
   }
+}
+
+/* With one planet the count is a constant: the loops unroll and the stage
+ * arrays stay in registers (the same operations in the same order). */
+static FB_HD inline void fb_nbody_rk5(fb_psys *S, double dt) {
+  if (S->np == 1) fb_nbody_rk5_n(S, dt, 1);
+  else fb_nbody_rk5_n(S, dt, S->np);
 }
 
 /* Per-step scalars the kernels read (the planet terms of Potential_cpu that do
