@@ -70,14 +70,31 @@ __global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 
   const Dims m = dims_of(D);
   const Geo<T> g = geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom);
   const int k = m.is3d ? FB_NGH + (int)bid.y : 0;
+  const int j0 = FB_NGH + (int)bid.x * CFL_R;
+  const int nr = min(CFL_R, m.ny + FB_NGH - j0);
+  const T nu = (T)scp->nu, alpha = (T)scp->alpha;
+  unsigned long long *dtmin = (unsigned long long *)D.dtmin;
   double mn = 1e20;
-  for (int r = 0; r < CFL_R; r++) {
-    const int j = FB_NGH + (int)bid.x * CFL_R + r;
-    if (j >= m.ny + FB_NGH) break;
-    mn = fmin(mn, cfl_ring<T, S>(m, g, (const S *)F.rho, (const S *)F.cs, (const S *)F.vx, (const S *)F.vy,
-                                 (const S *)F.vz, F.vxmed, scp, D.cfl, D.mindx, (unsigned long long *)D.dtmin, j, k));
+  bool bad = false;
+  // the CTA's cells, ring after ring, spread over all its threads (rings of
+  // 128 cells keep all 256 busy); min and OR do not depend on the order
+  int r = 0, i = threadIdx.x;
+  while (i >= m.nx) { i -= m.nx; r++; }
+#pragma unroll 2
+  for (; r < nr;) {
+    const int j = j0 + r;
+    mn = fmin(mn, (double)cfl_cell<T, S>(m, g, (const S *)F.rho, (const S *)F.cs, (const S *)F.vx, (const S *)F.vy,
+                                         (const S *)F.vz, F.vxmed[j + k * m.sy], nu, alpha, D.cfl, i, j, k, bad));
+    i += blockDim.x;
+    while (i >= m.nx) { i -= m.nx; r++; }
   }
-  cfl_commit(mn, (unsigned long long *)D.dtmin);
+  if (bad) atomicOr(dtmin + 1, 1ull);
+  if ((int)threadIdx.x < nr) {
+    const int j = j0 + threadIdx.x;
+    const double shear = cfl_shear(g, F.vxmed, D.cfl, D.mindx, j + k * m.sy, j);
+    if (shear < mn) mn = shear;
+  }
+  cfl_commit(mn, dtmin);
 }
 
 template <typename T, typename S>

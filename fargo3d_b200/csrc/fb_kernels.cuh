@@ -197,6 +197,53 @@ __device__ __forceinline__ T zsz(const Dims &m, const Geo<T> &g, int j, int k) {
 // This thread's share of ring (j, k): the minimum of its cells' limits (and,
 // for thread 0, the ring's shear limit); non-finite steps or non-positive
 // densities raise the flag word dtmin[1].
+// Time-step limit of one cell (cfl.c:142-250); `bad` collects the failure
+// flags (a non-finite limit or a non-positive density) without a memory
+// operation, so the loads of consecutive cells can overlap.
+template <typename T, typename S>
+__device__ __forceinline__ T cfl_cell(const Dims &m, const Geo<T> &g, const S *__restrict__ rho,
+                                      const S *__restrict__ cs, const S *__restrict__ vx,
+                                      const S *__restrict__ vy, const S *__restrict__ vz, double vm, T nu,
+                                      T alpha, double cfl_num, int i, int j, int k, bool &bad) {
+  const long long l = m.l(i, j, k);
+  const long long lxp = (i < m.nx - 1) ? l + 1 : l - (m.nx - 1);
+  const T vxx = vx[l] - (T)vm, vxxp = vx[lxp] - (T)vm;
+  const T c = cs[l];
+  const T ss2 = c * c;
+  T visc;
+  if (m.alpha) visc = alpha * c * c * ld(g.visc_j + j);
+  else visc = nu;
+  const T ss = sqrt(ss2);
+  const T zx = zsx(m, g, i, j, k), zy = zsy(g, j);
+  T c1a = ss / zx, c1b = ss / zy, c1c = 0, c4 = 0, c5c = 0, c7c = 0;
+  T zz = 1;
+  if (m.is3d) { zz = zsz(m, g, j, k); c1c = ss / zz; }
+  const T c1 = (T)dmax3(c1a, c1b, c1c);
+  const T c2 = (T)(dmax2(fabs(vxx), fabs(vxxp))) / zx;
+  const T c3 = (T)(dmax2(fabs(vy[l]), fabs(vy[l + m.pitch]))) / zy;
+  if (m.is3d) c4 = (T)(dmax2(fabs(vz[l]), fabs(vz[l + m.stride]))) / zz;
+  const T c5a = fabs(vx[lxp] - vx[l]) / zx;
+  const T c5b = fabs(vy[l + m.pitch] - vy[l]) / zy;
+  if (m.is3d) c5c = fabs(vz[l + m.stride] - vz[l]) / zz;
+  const T c5 = (T)dmax3(c5a, c5b, c5c) * (T)4.0 * (T)FB_CVNR;
+  const T c7a = (T)1.0 / zx, c7b = (T)1.0 / zy;
+  if (m.is3d) c7c = (T)1.0 / zz;
+  const T mx7 = (T)dmax3(c7a, c7b, c7c);
+  const T c7 = (T)4.0 * visc * (mx7 * mx7);
+  const T zero = 0;
+  const T dtc = (T)cfl_num / sqrt(c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4 + c5 * c5 + zero * zero + c7 * c7 +
+                                  zero * zero + zero * zero + zero * zero);
+  bad |= !(dtc == dtc) || !(rho[l] > (T)0);
+  return dtc;
+}
+
+// Shear limit of ring j (cfl_b.c:20-31).
+template <typename T>
+__device__ __forceinline__ double cfl_shear(const Geo<T> &g, const double *__restrict__ vxmed, double cfl_num,
+                                            double mindx, int jk, int j) {
+  return cfl_num * mindx / fabs(vxmed[jk] / (double)ld(g.ymed + j) - vxmed[jk + 1] / (double)ld(g.ymed + j + 1));
+}
+
 template <typename T, typename S = T>
 __device__ __forceinline__ double cfl_ring(Dims m, Geo<T> g, const S *__restrict__ rho, const S *__restrict__ cs,
                                            const S *__restrict__ vx, const S *__restrict__ vy,
@@ -206,45 +253,13 @@ __device__ __forceinline__ double cfl_ring(Dims m, Geo<T> g, const S *__restrict
   const double vm = vxmed[j + k * m.sy];
   const T nu = (T)sc->nu, alpha = (T)sc->alpha;
   double mn = 1e20;
-  for (int i = threadIdx.x; i < m.nx; i += blockDim.x) {
-    const long long l = m.l(i, j, k);
-    const long long lxp = (i < m.nx - 1) ? l + 1 : l - (m.nx - 1);
-    const T vxx = vx[l] - (T)vm, vxxp = vx[lxp] - (T)vm;
-    const T c = cs[l];
-    const T ss2 = c * c;
-    T visc;
-    if (m.alpha) visc = alpha * c * c * ld(g.visc_j + j);
-    else visc = nu;
-    const T ss = sqrt(ss2);
-    const T zx = zsx(m, g, i, j, k), zy = zsy(g, j);
-    T c1a = ss / zx, c1b = ss / zy, c1c = 0, c4 = 0, c5c = 0, c7c = 0;
-    T zz = 1;
-    if (m.is3d) { zz = zsz(m, g, j, k); c1c = ss / zz; }
-    const T c1 = (T)dmax3(c1a, c1b, c1c);
-    const T c2 = (T)(dmax2(fabs(vxx), fabs(vxxp))) / zx;
-    const T c3 = (T)(dmax2(fabs(vy[l]), fabs(vy[l + m.pitch]))) / zy;
-    if (m.is3d) c4 = (T)(dmax2(fabs(vz[l]), fabs(vz[l + m.stride]))) / zz;
-    const T c5a = fabs(vx[lxp] - vx[l]) / zx;
-    const T c5b = fabs(vy[l + m.pitch] - vy[l]) / zy;
-    if (m.is3d) c5c = fabs(vz[l + m.stride] - vz[l]) / zz;
-    const T c5 = (T)dmax3(c5a, c5b, c5c) * (T)4.0 * (T)FB_CVNR;
-    const T c7a = (T)1.0 / zx, c7b = (T)1.0 / zy;
-    if (m.is3d) c7c = (T)1.0 / zz;
-    const T mx7 = (T)dmax3(c7a, c7b, c7c);
-    const T c7 = (T)4.0 * visc * (mx7 * mx7);
-    const T zero = 0;
-    const T dtc = (T)cfl_num / sqrt(c1 * c1 + c2 * c2 + c3 * c3 + c4 * c4 + c5 * c5 + zero * zero + c7 * c7 +
-                                    zero * zero + zero * zero + zero * zero);
-    mn = fmin(mn, (double)dtc);
-    // failure detection: a non-finite time step or a non-positive density
-    // flags the disk (dtmin[1]); the host or the batch scalar kernel reacts
-    if (!(dtc == dtc) || !(rho[l] > (T)0)) atomicOr(dtmin + 1, 1ull);
-  }
-  // shear limit (cfl_b.c:27-33)
+  bool bad = false;
+  for (int i = threadIdx.x; i < m.nx; i += blockDim.x)
+    mn = fmin(mn, (double)cfl_cell<T, S>(m, g, rho, cs, vx, vy, vz, vm, nu, alpha, cfl_num, i, j, k, bad));
+  // failure detection: the host or the batch scalar kernel reacts to dtmin[1]
+  if (bad) atomicOr(dtmin + 1, 1ull);
   if (threadIdx.x == 0) {
-    const double shear =
-        cfl_num * mindx /
-        fabs(vm / (double)ld(g.ymed + j) - vxmed[j + 1 + k * m.sy] / (double)ld(g.ymed + j + 1));
+    const double shear = cfl_shear(g, vxmed, cfl_num, mindx, j + k * m.sy, j);
     if (shear < mn) mn = shear;
   }
   return mn;
