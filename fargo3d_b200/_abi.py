@@ -87,6 +87,9 @@ def lib():
     L.fb_disk_step.argtypes = [C.c_void_p, C.c_double, _D]
     L.fb_disk_get_scalars.argtypes = [C.c_void_p, _D]
     L.fb_disk_device_fields.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]
+    L.fb_disk_get_background.argtypes = [C.c_void_p, C.c_int, _D]
+    L.fb_disk_set_wait_limit.argtypes = [C.c_void_p, C.c_longlong]
+    L.fb_disk_mass.argtypes = [C.c_void_p, C.c_int, _D]
     L.fb_disk_stream.restype = C.c_void_p
     L.fb_disk_stream.argtypes = [C.c_void_p]
     L.fb_params_bytes.argtypes = [C.POINTER(FbParams), C.c_int, C.POINTER(C.c_size_t)]

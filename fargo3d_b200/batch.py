@@ -88,6 +88,13 @@ class Batch:
                                                    C.byref(st)))
         return o, st.value
 
+    def mass(self, i, fluid: int = 0) -> float:
+        """Total mass of disk i's fluid (compensated FP64 sum on the device)."""
+        self.sync()
+        m = C.c_double()
+        _abi.check(_abi.lib().fb_disk_mass(self._members[i]._h, fluid, C.byref(m)))
+        return m.value
+
     def set_tiles(self, i, sweep_x_cells: int = 0, col_segment: int = 0):
         _abi.check(_abi.lib().fb_batch_set_tiles(self._h, i, sweep_x_cells, col_segment))
 

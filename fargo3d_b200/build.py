@@ -60,6 +60,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     fast32 = [] if os.environ.get("FB_FP32_IEEE") else ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
     cu_flags = {"fb_kernels_f64.cu": ["--fmad=false"], "fb_kernels_f32.cu": fast32, "fb_noalloc.cu": ["--fmad=false"],
                 "fb_batch_f64.cu": ["--fmad=false"], "fb_batch_f32.cu": fast32}
+    cmds = []
     for f in sorted(os.listdir(CSRC)):
         src = os.path.join(CSRC, f)
         obj = os.path.join(BUILD, f + ".o")
@@ -71,10 +72,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
                    "-I/usr/local/cuda/include"] + INC + ["-c", src, "-o", obj]
         else:
             continue
-        out = _run(cmd)
-        if verbose:
-            sys.stdout.write(out)
+        cmds.append(cmd)
         objs.append(obj)
+    # translation units are independent: compile them concurrently
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for out in ex.map(_run, cmds):
+            if verbose:
+                sys.stdout.write(out)
     _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lm", "-lpthread"])
     return LIB
 

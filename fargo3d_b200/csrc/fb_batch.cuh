@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(256) kb_rowsum(const fb_disk_dev *ds, const in
   const S *v = (const S *)(which == 0 ? F.vx : F.vxt);
   double *out = which == 0 ? F.vxmed : F.vxmed_t;
   if (ORDERED) b_rowsum<T, true, S>(dims_of(D), geo_of<double>(D.geomd), v, out, D.xlen, bid);  // 32 rings / CTA
-  else b_rowsum_warp<S>(dims_of(D), geo_of<double>(D.geomd), v, out, D.xlen, bid);           // 8 rings / CTA
+  else b_rowsum_warp<S>(dims_of(D), geo_of<double>(D.geomd), v, out, D.xlen, F.vbg, bid);    // 8 rings / CTA
 }
 
 template <typename T, typename S>
@@ -84,7 +84,8 @@ __global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 
   for (; r < nr;) {
     const int j = j0 + r;
     mn = fmin(mn, (double)cfl_cell<T, S>(m, g, (const S *)F.rho, (const S *)F.cs, (const S *)F.vx, (const S *)F.vy,
-                                         (const S *)F.vz, F.vxmed[j + k * m.sy], nu, alpha, D.cfl, i, j, k, bad));
+                                         (const S *)F.vz, F.vxmed[j + k * m.sy] - bg_at(F.vbg, j + k * m.sy), nu,
+                                         alpha, D.cfl, i, j, k, bad));
     i += blockDim.x;
     while (i >= m.nx) { i -= m.nx; r++; }
   }
@@ -102,7 +103,7 @@ __global__ void __launch_bounds__(SRC2_TX *SRC2_TY, sizeof(S) == 4 ? FB_SRC_MINB
   FB_TILE
   b_sources_cyl<T, SRC2_TX, SRC2_TY, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), (const S *)F.rho,
                                      (const S *)F.cs, (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, scp,
-                                     F.dust, !F.dust, bid);
+                                     F.dust, !F.dust, F.vbg, bid);
 }
 
 template <typename T, typename S>
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(SRC3_TX *SRC3_TY) kb_sources_sph(const fb_disk
   FB_TILE
   b_sources_sph<T, SRC3_TX, SRC3_TY, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), (const S *)F.rho,
                                      (const S *)F.cs, (const S *)F.vx, (const S *)F.vy, (const S *)F.vz, (S *)F.vxt,
-                                     (S *)F.vyt, (S *)F.vzt, scp, F.dust, !F.dust, bid);
+                                     (S *)F.vyt, (S *)F.vzt, scp, F.dust, !F.dust, F.vbg, bid);
 }
 
 template <typename T, typename S>
@@ -119,8 +120,8 @@ __global__ void kb_bnd(const fb_disk_dev *ds, const int4 *items, int f, int vtem
   Dims m = dims_of(D);
   BndTab tb{D.bnd_tab, m.sy, m.sz};
   S *vx = (S *)(vtemp ? F.vxt : F.vx), *vy = (S *)(vtemp ? F.vyt : F.vy), *vz = (S *)(vtemp ? F.vzt : F.vz);
-  if (zside) b_bnd_z<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, bid);
-  else b_bnd_y<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, bid);
+  if (zside) b_bnd_z<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, F.vbg, bid);
+  else b_bnd_y<T, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), tb, (S *)F.rho, vx, vy, vz, scp, !vtemp, F.vbg, bid);
 }
 
 template <typename T, int N, typename S>
@@ -138,6 +139,7 @@ __global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? FB_COL_MINB32 : 1) kb
   const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;
   QSrc<T, S> src;
   src.vxt = (const S *)F.vxt; src.vyt = (const S *)F.vyt; src.vzt = (const S *)F.vzt; src.of = (T)0;
+  src.dl = (const T *)(DIR == 1 ? F.dlb_z : F.dlb_y);
   if (!m.is3d || DIR == 1) {
     src.rho = (const S *)F.rho;
     for (int q = 0; q < 6; q++) src.q[q] = nullptr;
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? FB_SX_MINB32 : 1) kb_swe
                         nj, nrings, (S *)(b ? F.rho_b : F.rho_a), (S *)(b ? F.mpx_b : F.mpx),
                         (S *)(b ? F.mmx_b : F.mmx), (S *)(b ? F.mpy_b : F.mpy), (S *)(b ? F.mmy_b : F.mmy),
                         (S *)(b ? F.mpz_b : F.mpz), (S *)(b ? F.mmz_b : F.mmz), (const S *)F.vxt, F.vxmed_t, F.nshift,
-                        scp, (unsigned long long *)D.dtmin + 1, bid);
+                        scp, (unsigned long long *)D.dtmin + 1, F.vbg, wait_limit(D), bid);
 }
 
 template <typename T, typename S>

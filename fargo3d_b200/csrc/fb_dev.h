@@ -37,6 +37,17 @@ typedef struct {
   int *nshift;
   void *rho0, *vx0, *vy0, *vz0;
   int dust;
+  /* FP32 disks: the azimuthal velocities (vx, vxt, vx0) are stored relative
+     to a per-ring background vbg ([sz][sy] doubles: the FP64 ring mean of the
+     first vx the caller gave), so a stored float carries the deviation from
+     the ring's rotation, not the rotation itself.  dlb_y / dlb_z hold the
+     neighbour differences of vbg * R along y / z (R the cylindrical radius,
+     differenced in double, stored in the disk's precision): the column sweeps
+     add them to the frame's OMEGAFRAME * R^2 differences.  Null (FP64 disks)
+     or zero (no vx given yet) means no background. */
+  double *vbg;
+  void *dlb_y, *dlb_z;
+  int has_bg;
 } fb_fluid_dev;
 
 /* Per-step scalars (host-computed in FP64 mode, device-computed in the
@@ -69,12 +80,13 @@ typedef struct {
   int nfluids;
   double *dtmin;          /* device scalar: CFL minimum (bits as u64 min) */
   fb_scalars *scal_dev;   /* device copy of the per-step scalars */
-  double *rowmin;         /* per-ring scratch */
+  double *ringsum;        /* per-ring scratch of the mass reduction: 2 x rings + 2 doubles */
   double *bnd_tab;        /* boundary factor tables (double) */
   int bnd_tab_n;
   double *ramps;          /* Stockholm ramps: [sy] radial, [sz] zmed, [sz] zmin */
   int tile_cx;            /* azimuthal sweep cells per thread (0: default) */
   int tile_ns;            /* column sweep segment length (0: default) */
+  long long wait_limit;   /* polls of a bounded wait (0: default 2^22; < 0: none) */
   /* collision rates between the fluids, alpha[p + o * nfluids] (ColRate,
      colrate.c:10-23): alpha[0 + f n] = alpha[f + 0 n] = 1/St of dust fluid f */
   double alpha[FB_MAXFLUIDS * FB_MAXFLUIDS];
@@ -90,6 +102,7 @@ typedef struct {
   int fb_launch_sweep_x_##SUF(const fb_disk_dev *d, int fluid, void *stream);       \
   int fb_launch_newvel_##SUF(const fb_disk_dev *d, int fluid, void *stream);        \
   int fb_launch_collisions_##SUF(const fb_disk_dev *d, void *stream);                 \
+  int fb_launch_mass_##SUF(const fb_disk_dev *d, int fluid, double *part, double *out, void *stream); \
   int fb_launch_disk_force_##SUF(const fb_disk_dev *d, double x, double y, double z, double rs, double *ring3, \
                                  double *out3, void *stream);
 
@@ -105,6 +118,14 @@ size_t fb_disk_internal_esz(struct fb_disk *d);
 int fb_internal_fail(int code, const char *what, int cuda_err);
 /* FP64 <-> FP32 copy of n values on the device (fb_kernels_f64.cu) */
 int fb_launch_convert(void *dst, const void *src, size_t n, int to_f32, void *stream);
+/* the same for values of whole rings of nx cells less (to FP32) or plus (to
+ * FP64) the per-ring offset off[ring0 + i / nx] */
+int fb_launch_convert_off(void *dst, const void *src, size_t n, int to_f32, const double *off, int nx,
+                          long long ring0, void *stream);
+/* out[r] = mean of the nx doubles of ring r, r < nrings (fixed summation order) */
+int fb_launch_ring_mean(double *out, const double *src, int nx, int nrings, void *stream);
+/* the background's neighbour differences dlb_y / dlb_z of fluid f (FP32 disks) */
+int fb_launch_bg_diffs(const fb_disk_dev *d, int fluid, void *stream);
 
 #ifdef __cplusplus
 }

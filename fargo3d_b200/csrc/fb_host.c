@@ -403,9 +403,11 @@ int fb_params_bytes(const fb_params *p, int precision, size_t *out) {
   rings = sy * sz;
   fields = is3d ? 15 + 7 : 11;
   b = (size_t)p->nfluids * (fields * nc * esz + 2 * rings * sizeof(double) + rings * sizeof(int) + 4 * rings * esz);
+  /* FP32: per-ring azimuthal background and its y / z differences */
+  if (precision != FB_FP64) b += (size_t)p->nfluids * rings * (sizeof(double) + 2 * esz);
   b += 2 * sizeof(double) * (6 * ((size_t)p->nx + 1) + 20 * (sy + 1) + 16 * (sz + 1));
   b += sizeof(double) * (18 + 6 * sz + 6 * sy + 6) + sizeof(double) * (sy + 2 * sz);
-  b += 64 + sizeof(fb_scalars) + 64 * 16;
+  b += 64 + sizeof(fb_scalars) + 64 * 16 + sizeof(double) * (2 * rings + 2);
   *out = b;
   return FB_OK;
 }
@@ -439,6 +441,15 @@ int fb_disk_set_tiles(fb_disk *D, int cx, int ns) {
   if (ns != 0 && ns != 4 && ns != 8 && ns != 16) return fail(FB_ERR_ARG, "column segment %d not in {4, 8, 16}", ns);
   D->d.tile_cx = cx;
   D->d.tile_ns = ns;
+  return FB_OK;
+}
+
+/* Polls of the bounded wait on the azimuthal sweep's staged ring loads
+ * before the disk is flagged (failure detection): 0 restores the default,
+ * a negative value polls not at all (the wait gives up at once; for tests). */
+int fb_disk_set_wait_limit(fb_disk *D, long long polls) {
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  D->d.wait_limit = polls;
   return FB_OK;
 }
 
@@ -597,9 +608,15 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
       fb_disk_destroy(D);
       return rc;
     }
+    if (precision == FB_FP32 &&   /* zero until the first vx arrives (fb_disk_set_state) */
+        ((rc = dalloc(D, (void **)&F->vbg, f2)) || (rc = dalloc(D, &F->dlb_y, e2)) || (rc = dalloc(D, &F->dlb_z, e2)))) {
+      fb_disk_destroy(D);
+      return rc;
+    }
     F->dust = f > 0;
   }
-  if ((rc = dalloc(D, (void **)&D->d.dtmin, 64)) || (rc = dalloc(D, (void **)&D->d.scal_dev, sizeof(fb_scalars)))) {
+  if ((rc = dalloc(D, (void **)&D->d.dtmin, 64)) || (rc = dalloc(D, (void **)&D->d.scal_dev, sizeof(fb_scalars))) ||
+      (rc = dalloc(D, (void **)&D->d.ringsum, sizeof(double) * (2 * (size_t)D->d.sy * D->d.sz + 2)))) {
     fb_disk_destroy(D);
     return rc;
   }
@@ -720,6 +737,35 @@ static int stage_move(fb_disk *D, double *st, double *host, void *field, size_t 
   return 0;
 }
 
+/* The azimuthal velocity of an FP32 fluid crosses as vx - vbg(ring), whole
+ * rings per chunk.  The first vx given sets the background: its rings' FP64
+ * means (then vbg * R's neighbour differences for the column sweeps). */
+static int stage_move_vx(fb_disk *D, int f, double *st, double *host, void *field, int to_f32) {
+  fb_fluid_dev *F = &D->d.fl[f];
+  const size_t nx = (size_t)D->d.nx, rings = (size_t)D->d.sy * D->d.sz, rpc = DSTAGE_N / nx;
+  const int first = to_f32 && !F->has_bg;
+  size_t r0;
+  if (rpc == 0 || !F->vbg) return 1;
+  for (r0 = 0; r0 < rings; r0 += rpc) {
+    const size_t nr = rings - r0 < rpc ? rings - r0 : rpc, c = nr * nx, o = r0 * nx;
+    if (to_f32) {
+      if (cudaMemcpyAsync(st, host + o, c * sizeof(double), cudaMemcpyHostToDevice, D->stream) != cudaSuccess ||
+          (first && fb_launch_ring_mean(F->vbg + r0, st, (int)nx, (int)nr, D->stream) != cudaSuccess) ||
+          fb_launch_convert_off((float *)field + o, st, c, 1, F->vbg, (int)nx, (long long)r0, D->stream) != cudaSuccess)
+        return 1;
+    } else {
+      if (fb_launch_convert_off(st, (float *)field + o, c, 0, F->vbg, (int)nx, (long long)r0, D->stream) != cudaSuccess ||
+          cudaMemcpyAsync(host + o, st, c * sizeof(double), cudaMemcpyDeviceToHost, D->stream) != cudaSuccess)
+        return 1;
+    }
+  }
+  if (first) {
+    if (fb_launch_bg_diffs(&D->d, f, D->stream) != cudaSuccess) return 1;
+    F->has_bg = 1;
+  }
+  return 0;
+}
+
 int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, const double *vy, const double *vz,
                       const double *cs) {
   fb_fluid_dev *F;
@@ -734,7 +780,8 @@ int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, co
     double *st = dstage_lock(D->device);
     if (!st) return fail(FB_ERR_CUDA, "device staging");
     for (q = 0; q < 5 && !rc; q++)
-      if (src[q] && dst[q] && stage_move(D, st, (double *)src[q], dst[q], n, 1))
+      if (src[q] && dst[q] &&
+          (q == 1 ? stage_move_vx(D, f, st, (double *)src[q], dst[q], 1) : stage_move(D, st, (double *)src[q], dst[q], n, 1)))
         rc = fail(FB_ERR_CUDA, "state upload");
     if (cudaStreamSynchronize(D->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state upload");
     stage_unlock();
@@ -761,7 +808,8 @@ int fb_disk_get_state(fb_disk *D, int f, double *rho, double *vx, double *vy, do
     double *st = dstage_lock(D->device);
     if (!st) return fail(FB_ERR_CUDA, "device staging");
     for (q = 0; q < 4 && !rc; q++)
-      if (dst[q] && src[q] && stage_move(D, st, dst[q], (void *)src[q], n, 0))
+      if (dst[q] && src[q] &&
+          (q == 1 ? stage_move_vx(D, f, st, dst[q], (void *)src[q], 0) : stage_move(D, st, dst[q], (void *)src[q], n, 0)))
         rc = fail(FB_ERR_CUDA, "state download");
     if (cudaStreamSynchronize(D->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state download");
     stage_unlock();
@@ -1032,6 +1080,37 @@ int fb_disk_device_fields(fb_disk *D, int f, void *ptrs[5], size_t *esz) {
   ptrs[0] = D->d.fl[f].rho; ptrs[1] = D->d.fl[f].vx; ptrs[2] = D->d.fl[f].vy;
   ptrs[3] = D->d.fl[f].vz; ptrs[4] = D->d.fl[f].cs;
   if (esz) *esz = D->esz;
+  return FB_OK;
+}
+
+/* Total mass of one fluid (ComputeMass, LowTasks.c:709-748): the sum of
+ * rho * Vol over the active cells, FP64 with compensation, on the device.
+ * Synchronous; a batch member's caller calls fb_batch_sync first. */
+int fb_disk_mass(fb_disk *D, int f, double *mass) {
+  double *part, *out;
+  if (!D || !mass || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
+  CU(cudaSetDevice(D->device));
+  part = D->d.ringsum;
+  out = part + 2 * (size_t)D->d.sy * D->d.sz;
+  LCH(LAUNCH(mass, &D->d, f, part, out, D->stream));
+  CU(cudaMemcpyAsync(mass, out, sizeof(double), cudaMemcpyDeviceToHost, D->stream));
+  CU(cudaStreamSynchronize(D->stream));
+  return FB_OK;
+}
+
+/* The per-ring azimuthal background of an FP32 fluid ((Nz+6 or 1) x (Ny+6)
+ * doubles; zeros for FP64 disks and before the first vx was given). */
+int fb_disk_get_background(fb_disk *D, int f, double *out) {
+  size_t n;
+  if (!D || !out || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
+  n = (size_t)D->d.sy * D->d.sz;
+  if (!D->d.fl[f].vbg) {
+    memset(out, 0, n * sizeof(double));
+    return FB_OK;
+  }
+  CU(cudaSetDevice(D->device));
+  CU(cudaMemcpyAsync(out, D->d.fl[f].vbg, n * sizeof(double), cudaMemcpyDeviceToHost, D->stream));
+  CU(cudaStreamSynchronize(D->stream));
   return FB_OK;
 }
 

@@ -135,10 +135,13 @@ __device__ __forceinline__ void b_rowsum(Dims m, Geo<double> gd, const S *__rest
 }
 // Order-free ring sums (FP32 storage): one warp per ring, lanes striding
 // over the ring with an FP64 accumulator, then a shuffle tree; 8 rings per
-// CTA of 256 threads, no shared memory and no barrier.
+// CTA of 256 threads, no shared memory and no barrier.  vbg: the ring's
+// background azimuthal velocity (FP32 disks store v - vbg), added back so
+// the mean is that of the full velocity.
 template <typename S>
 __device__ __forceinline__ void b_rowsum_warp(Dims m, Geo<double> gd, const S *__restrict__ v,
-                                              double *__restrict__ out, double xlen, uint3 bid) {
+                                              double *__restrict__ out, double xlen, const double *__restrict__ vbg,
+                                              uint3 bid) {
   const int ring = bid.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (ring >= m.sy * m.sz) return;
   const int j = ring % m.sy, k = ring / m.sy;
@@ -146,13 +149,19 @@ __device__ __forceinline__ void b_rowsum_warp(Dims m, Geo<double> gd, const S *_
   double acc = 0.0;
   for (int i = lane; i < m.nx; i += 32) acc += (double)row[i] * (ld(gd.xmin + i + 1) - ld(gd.xmin + i));
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) out[ring] = acc / xlen;
+  if (lane == 0) out[ring] = acc / xlen + (vbg ? vbg[ring] : 0.0);
 }
 
 template <typename S>
 __global__ void __launch_bounds__(256) k_rowsum_warp(Dims m, Geo<double> gd, const S *__restrict__ v,
-                                                      double *__restrict__ out, double xlen) {
-  b_rowsum_warp<S>(m, gd, v, out, xlen, blockIdx);
+                                                      double *__restrict__ out, double xlen,
+                                                      const double *__restrict__ vbg) {
+  b_rowsum_warp<S>(m, gd, v, out, xlen, vbg, blockIdx);
+}
+
+// The background of an FP32 fluid at ring (j, k) (0 without one).
+__device__ __forceinline__ double bg_at(const double *__restrict__ vbg, int ring) {
+  return vbg ? vbg[ring] : 0.0;
 }
 
 template <typename T, bool ORDERED, typename S = T, int R = 32>
@@ -249,8 +258,10 @@ __device__ __forceinline__ double cfl_ring(Dims m, Geo<T> g, const S *__restrict
                                            const S *__restrict__ vx, const S *__restrict__ vy,
                                            const S *__restrict__ vz, const double *__restrict__ vxmed,
                                            const fb_scalars *__restrict__ sc, double cfl_num, double mindx,
-                                           unsigned long long *__restrict__ dtmin, int j, int k) {
-  const double vm = vxmed[j + k * m.sy];
+                                           unsigned long long *__restrict__ dtmin, int j, int k,
+                                           const double *__restrict__ vbg) {
+  // FP32 disks hold vx less the ring's background: the mean less it too
+  const double vm = vxmed[j + k * m.sy] - bg_at(vbg, j + k * m.sy);
   const T nu = (T)sc->nu, alpha = (T)sc->alpha;
   double mn = 1e20;
   bool bad = false;
@@ -283,10 +294,11 @@ __device__ __forceinline__ void b_cfl(Dims m, Geo<T> g, const S *__restrict__ rh
                                              const S *__restrict__ vx, const S *__restrict__ vy,
                                              const S *__restrict__ vz, const double *__restrict__ vxmed,
                                              const fb_scalars *__restrict__ sc, double cfl_num,
-                                             double mindx, unsigned long long *__restrict__ dtmin, uint3 bid) {
+                                             double mindx, unsigned long long *__restrict__ dtmin,
+                                             const double *__restrict__ vbg, uint3 bid) {
   const int j = FB_NGH + bid.x;
   const int k = m.is3d ? FB_NGH + bid.y : 0;
-  cfl_commit(cfl_ring<T, S>(m, g, rho, cs, vx, vy, vz, vxmed, sc, cfl_num, mindx, dtmin, j, k), dtmin);
+  cfl_commit(cfl_ring<T, S>(m, g, rho, cs, vx, vy, vz, vxmed, sc, cfl_num, mindx, dtmin, j, k, vbg), dtmin);
 }
 
 template <typename T, typename S = T>
@@ -294,8 +306,9 @@ __global__ void __launch_bounds__(256) k_cfl(Dims m, Geo<T> g, const S *__restri
                                              const S *__restrict__ vx, const S *__restrict__ vy,
                                              const S *__restrict__ vz, const double *__restrict__ vxmed,
                                              const fb_scalars *__restrict__ sc, double cfl_num,
-                                             double mindx, unsigned long long *__restrict__ dtmin) {
-  b_cfl<T, S>(m, g, rho, cs, vx, vy, vz, vxmed, sc, cfl_num, mindx, dtmin, blockIdx);
+                                             double mindx, unsigned long long *__restrict__ dtmin,
+                                             const double *__restrict__ vbg) {
+  b_cfl<T, S>(m, g, rho, cs, vx, vy, vz, vxmed, sc, cfl_num, mindx, dtmin, vbg, blockIdx);
 }
 
 // ---------------------------------------------------------------------------
@@ -365,7 +378,7 @@ template <typename T, int TX, int TY, typename S = T>
 __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
     const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx,
     const S *__restrict__ vy, S *__restrict__ vxt, S *__restrict__ vyt,
-    const fb_scalars *__restrict__ scp, int dust, int viscous, uint3 bid) {
+    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg, uint3 bid) {
   constexpr int W = TX + 2, H = TY + 2;
   __shared__ T s_rho[H][W], s_cs[H][W], s_vx[H][W], s_vy[H][W], s_p[H][W];
   __shared__ double s_pot[H][W];
@@ -396,7 +409,9 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
       const T r = rho[l], c = cs[l];
       s_rho[lj][li] = r;
       s_cs[lj][li] = c;
-      s_vx[lj][li] = vx[l] - domega * ld(g.ymed + j);
+      // FP32 storage holds vx less the ring's background (added back here)
+      if (FAST) s_vx[lj][li] = ((T)vx[l] + (T)bg_at(vbg, j)) - domega * ld(g.ymed + j);
+      else s_vx[lj][li] = vx[l] - domega * ld(g.ymed + j);
       s_vy[lj][li] = vy[l];
       s_p[lj][li] = r * c * c;
       s_pot[lj][li] = FAST ? potential_fast(m, gd, sc, s_ind, i, j, 0) : potential_at(m, gd, sc, i, j, 0);
@@ -517,15 +532,15 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
     ax += -(T)2.0 * (T)dt * dxmed * (qx - qxm) / (r * ld(g.sxi + i) + rxm * ld(g.sxi + im)) * izx;
     ay += -(T)2.0 * (qy - qym) / (r * (yip - yi) + rym * (yi - yim)) * (T)dt;
   }
-  vxt[l] = ax;
+  vxt[l] = FAST ? ax - (T)bg_at(vbg, j) : ax;
   vyt[l] = ay;
 }
 template <typename T, int TX, int TY, typename S = T>
 __global__ void __launch_bounds__(TX *TY) k_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
     const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx,
     const S *__restrict__ vy, S *__restrict__ vxt, S *__restrict__ vyt,
-    const fb_scalars *__restrict__ scp, int dust, int viscous) {
-  b_sources_cyl<T, TX, TY, S>(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, blockIdx);
+    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg) {
+  b_sources_cyl<T, TX, TY, S>(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, vbg, blockIdx);
 }
 
 }  // namespace fb
@@ -555,7 +570,7 @@ struct BndTab {
 template <typename T, typename S = T>
 __device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
                         S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
-                        int do_rho, uint3 bid) {
+                        int do_rho, const double *__restrict__ vbg, uint3 bid) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   const int jj = bid.y % 3, s = bid.y / 3, k = bid.z;
   if (i >= m.nx) return;
@@ -566,13 +581,19 @@ __device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restri
   else { jgh = ny + nghy + jj; jact = ny + nghy - 1 - jj; jlacts = jact; jnull = ny + nghy; }
   const long long lgh = m.l(i, jgh, k), lact = m.l(i, jact, k);
   const T yact = ld(g.ymed + jact), ygh = ld(g.ymed + jgh);
+  // FP32 storage: vx less the ring backgrounds of the active and ghost rows
+  constexpr bool BG = sizeof(S) < sizeof(T);
+  const T vact = BG ? (T)vx[lact] + (T)bg_at(vbg, jact + k * m.sy) : (T)vx[lact];
+  const T bgh = BG ? (T)bg_at(vbg, jgh + k * m.sy) : (T)0;
   if (!m.is3d) {
     if (do_rho) rho[lgh] = rho[lact] * (T)tb.rhof(s, jj);
-    vx[lgh] = (vx[lact] + yact * of) * (T)tb.sqf(s, jj) - ygh * of;
+    if (BG) vx[lgh] = (vact + yact * of) * (T)tb.sqf(s, jj) - ygh * of - bgh;
+    else vx[lgh] = (vx[lact] + yact * of) * (T)tb.sqf(s, jj) - ygh * of;
   } else {
     const T sz = ld(g.sin_zmed + k);
     if (do_rho) rho[lgh] = rho[lact] * (T)tb.rhof(s, jj) * (T)tb.rhoe(s, jj, k);
-    vx[lgh] = (vx[lact] + of * yact * sz) * (T)tb.sqf(s, jj) * (T)tb.cf(s, jj) - ygh * of * sz;
+    if (BG) vx[lgh] = (vact + of * yact * sz) * (T)tb.sqf(s, jj) * (T)tb.cf(s, jj) - ygh * of * sz - bgh;
+    else vx[lgh] = (vx[lact] + of * yact * sz) * (T)tb.sqf(s, jj) * (T)tb.cf(s, jj) - ygh * of * sz;
   }
   // Vy: ANTISYMMETRIC, staggered in y (|-a|0|a|)
   if (s == 0) vy[lgh] = -vy[m.l(i, jlacts, k)];
@@ -584,15 +605,15 @@ __device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restri
 template <typename T, typename S = T>
 __global__ void k_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
                         S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
-                        int do_rho) {
-  b_bnd_y<T, S>(m, g, tb, rho, vx, vy, vz, scp, do_rho, blockIdx);
+                        int do_rho, const double *__restrict__ vbg) {
+  b_bnd_y<T, S>(m, g, tb, rho, vx, vy, vz, scp, do_rho, vbg, blockIdx);
 }
 
 // Colatitude sides (3D): one thread per (i, j, ghost layer kk, side s).
 template <typename T, typename S = T>
 __device__ __forceinline__ void b_bnd_z(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
                         S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
-                        int do_rho, uint3 bid) {
+                        int do_rho, const double *__restrict__ vbg, uint3 bid) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   const int j = bid.y, kk = bid.z % 3, s = bid.z / 3;
   if (i >= m.nx) return;
@@ -604,7 +625,13 @@ __device__ __forceinline__ void b_bnd_z(Dims m, Geo<T> g, BndTab tb, S *__restri
   const long long lgh = m.l(i, j, kgh), lact = m.l(i, j, kact);
   const T ym = ld(g.ymed + j);
   if (do_rho) rho[lgh] = rho[lact] * (T)tb.zrho(s, kk, j);
-  vx[lgh] = (vx[lact] + of * ym * ld(g.sin_zmed + kact)) * (T)tb.zw(s, kk) - ym * of * ld(g.sin_zmed + kgh);
+  if (sizeof(S) < sizeof(T)) {  // FP32 storage: vx less the ring backgrounds
+    const T vact = (T)vx[lact] + (T)bg_at(vbg, j + kact * m.sy);
+    vx[lgh] = (vact + of * ym * ld(g.sin_zmed + kact)) * (T)tb.zw(s, kk) - ym * of * ld(g.sin_zmed + kgh) -
+              (T)bg_at(vbg, j + kgh * m.sy);
+  } else {
+    vx[lgh] = (vx[lact] + of * ym * ld(g.sin_zmed + kact)) * (T)tb.zw(s, kk) - ym * of * ld(g.sin_zmed + kgh);
+  }
   vy[lgh] = vy[lact];
   if (s == 0) vz[lgh] = -vz[m.l(i, j, klacts)];
   else if (kk < nghz - 1) vz[m.l(i, j, nz + nghz + 1 + kk)] = -vz[m.l(i, j, klacts)];
@@ -613,8 +640,8 @@ __device__ __forceinline__ void b_bnd_z(Dims m, Geo<T> g, BndTab tb, S *__restri
 template <typename T, typename S = T>
 __global__ void k_bnd_z(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
                         S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
-                        int do_rho) {
-  b_bnd_z<T, S>(m, g, tb, rho, vx, vy, vz, scp, do_rho, blockIdx);
+                        int do_rho, const double *__restrict__ vbg) {
+  b_bnd_z<T, S>(m, g, tb, rho, vx, vy, vz, scp, do_rho, vbg, blockIdx);
 }
 
 // ---------------------------------------------------------------------------
@@ -681,6 +708,9 @@ struct QSrc {
   const S *q[6];   // when from buffers: mpx, mmx, mpy, mmy, mpz, mmz
   int from_v;
   T of;
+  // FP32 storage: neighbour differences along the sweep of the background's
+  // vbg * R per ring (fb_fluid_dev dlb_y / dlb_z), or null
+  const T *dl;
 };
 
 // REL: the azimuthal momenta relative to the frame's rotation (the
@@ -762,11 +792,18 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, in
     const T flux = cg.surf(vel[u] * rs[u], c) - cg.surf(vel[u + 1] * rs[u + 1], c + 1);
     rnew[u] = r[u + 2] + cg.finish(flux, dt, c);
   }
-  // OMEGAFRAME * (R^2(c) - R^2(c-1))
+  // OMEGAFRAME * (R^2(c) - R^2(c-1)), plus (vbg R)(c) - (vbg R)(c-1) where
+  // the stored azimuthal velocities are relative to a ring background: the
+  // difference of the offset l(c) = R (OMEGAFRAME R + vbg) that the relative
+  // momenta leave out
+  auto dlb = [&](int c) -> T {
+    if (!src.dl) return (T)0;
+    return ld(src.dl + ((DIR == 0) ? c + k * m.sy : j + c * m.sy));
+  };
   auto dr2 = [&](int c) -> T {
-    if (!m.sph) return src.of * ld(g.dr2_j + c);
-    if (DIR == 0) return src.of * (ld(g.dr2_j + c) * ld(g.s2_k + k));
-    return src.of * (ld(g.r2_j + j) * ld(g.ds2_k + c));
+    if (!m.sph) return src.of * ld(g.dr2_j + c) + dlb(c);
+    if (DIR == 0) return src.of * (ld(g.dr2_j + c) * ld(g.s2_k + k)) + dlb(c);
+    return src.of * (ld(g.r2_j + j) * ld(g.ds2_k + c)) + dlb(c);
   };
   S *qo[6] = {q_out0, q_out1, q_out2, q_out3, q_out4, q_out5};
 #pragma unroll
@@ -942,7 +979,7 @@ template <typename T, int TX, int TY, typename S = T>
 __device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
     const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx, const S *__restrict__ vy,
     const S *__restrict__ vz, S *__restrict__ vxt, S *__restrict__ vyt, S *__restrict__ vzt,
-    const fb_scalars *__restrict__ scp, int dust, int viscous, uint3 bid) {
+    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg, uint3 bid) {
   constexpr int W = TX + 2, H = TY + 2;
   __shared__ T s_rho[3][H][W], s_cs[3][H][W], s_vx[3][H][W], s_vy[3][H][W], s_vz[3][H][W];
   __shared__ double s_pot[2][H][W];   // layers k-1, k
@@ -968,7 +1005,10 @@ __device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
       const T r = rho[l], c = cs[l];
       s_rho[lk][lj][li] = r;
       s_cs[lk][lj][li] = c;
-      s_vx[lk][lj][li] = vx[l] - domega * ld(g.ymed + j) * ld(g.sin_zmed + k);
+      if (sizeof(S) < sizeof(T))   // FP32 storage: vx less the ring's background
+        s_vx[lk][lj][li] = ((T)vx[l] + (T)bg_at(vbg, j + k * m.sy)) - domega * ld(g.ymed + j) * ld(g.sin_zmed + k);
+      else
+        s_vx[lk][lj][li] = vx[l] - domega * ld(g.ymed + j) * ld(g.sin_zmed + k);
       s_vy[lk][lj][li] = vy[l];
       s_vz[lk][lj][li] = vz[l];
       if (lk < 2) s_pot[lk][lj][li] = FAST ? potential_fast(m, gd, sc, s_ind, i, j, k) : potential_at(m, gd, sc, i, j, k);
@@ -1121,7 +1161,7 @@ __device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
     const T dzmed = zm - zmm, dzrho1 = zip - zi, dzrho2 = zi - zim;
     az += -(T)2.0 * dzmed * (qz - qzm) / (r * dzrho1 + rzm * dzrho2) * (T)dt / (ym * (zm - zmm));
   }
-  vxt[l] = ax;
+  vxt[l] = sizeof(S) < sizeof(T) ? ax - (T)bg_at(vbg, j + k * m.sy) : ax;
   vyt[l] = ay;
   vzt[l] = az;
 }
@@ -1129,8 +1169,8 @@ template <typename T, int TX, int TY, typename S = T>
 __global__ void __launch_bounds__(TX *TY) k_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
     const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx, const S *__restrict__ vy,
     const S *__restrict__ vz, S *__restrict__ vxt, S *__restrict__ vyt, S *__restrict__ vzt,
-    const fb_scalars *__restrict__ scp, int dust, int viscous) {
-  b_sources_sph<T, TX, TY, S>(m, g, gd, rho, cs, vx, vy, vz, vxt, vyt, vzt, scp, dust, viscous, blockIdx);
+    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg) {
+  b_sources_sph<T, TX, TY, S>(m, g, gd, rho, cs, vx, vy, vz, vxt, vyt, vzt, scp, dust, viscous, vbg, blockIdx);
 }
 
 }  // namespace fb
@@ -1216,7 +1256,8 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
                                            int klo, int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,
                                            S *q5, const S *__restrict__ vxt, const double *__restrict__ vxmed_t,
                                            int *__restrict__ nshift_out, const fb_scalars *__restrict__ scp,
-                                           unsigned long long *__restrict__ errflag, uint3 bid) {
+                                           unsigned long long *__restrict__ errflag, const double *__restrict__ vbg,
+                                           long long wait_limit, uint3 bid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long mbar;
   T *sm = reinterpret_cast<T *>(smem_raw);
@@ -1274,17 +1315,23 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
         }
       }
     }
-    // bounded wait: past the limit the disk is flagged (its next step stops
-    // it), the copies in flight get a second bounded wait, and the CTA leaves
+    // Bounded wait (wait_limit polls).  The decision is the block's: if any
+    // thread gave up, the disk is flagged (its next step reports it; a batch
+    // freezes it), every thread waits again -- boundedly -- for the copies in
+    // flight, so the CTA does not leave while the copy engine still writes
+    // its shared memory, and the block then returns without computing or
+    // writing anything.  Past the second limit the block returns regardless.
     uint32_t done = 0;
-    for (long it = 0; it < (1l << 22) && !done; it++)
+    for (long long it = 0; it < wait_limit && !done; it++)
       asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
                    : "=r"(done) : "r"(bar), "r"(0) : "memory");
-    if (!done) {
+    if (__syncthreads_or(!done)) {
       if (threadIdx.x == 0) atomicOr(errflag, 2ull);
-      for (long it = 0; it < (1l << 22) && !done; it++)
+      uint32_t drained = 0;
+      for (long it = 0; it < (1l << 22) && !drained; it++)
         asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-                     : "=r"(done) : "r"(bar), "r"(0) : "memory");
+                     : "=r"(drained) : "r"(bar), "r"(0) : "memory");
+      __syncthreads();
       return;
     }
   } else {
@@ -1303,6 +1350,8 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
   __syncthreads();
   const int sl0 = slot < rpc ? slot : 0;
   const double vm = active ? vxmed_t[j + k * m.sy] : 0.0;
+  // the residual velocity of the stored (background-relative, FP32 disks) vxt
+  const double vm_rel = vm - (active ? bg_at(vbg, j + k * m.sy) : 0.0);
   auto wrap = [&](int i) { i += (i < 0) ? nx : 0; i -= (i >= nx) ? nx : 0; return i; };
   // FP32: the azimuthal spacing is uniform (FARGO's shift requires it), so a
   // ring's zone size is one value, formed once in FP64, instead of a table
@@ -1329,7 +1378,7 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
       T v[C + 1];
       if (pass == 0) {
 #pragma unroll
-        for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nxp + P(wrap(c0 + f))] - vm);  // residual
+        for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nxp + P(wrap(c0 + f))] - vm_rel);  // residual
       } else {
 #pragma unroll
         for (int f = 0; f <= C; f++) {  // uniform fractional velocity (compute_residual.c:68-73), FP64
@@ -1461,6 +1510,8 @@ __device__ __forceinline__ void b_collisions(const fb_disk_dev &D, Dims m, Geo<d
       }
       const S *v = (const S *)(dir == 0 ? D.fl[o].vxt : (dir == 1 ? D.fl[o].vyt : D.fl[o].vzt));
       b[o] = (T)v[l];
+      // FP32 storage: the drag acts on the full azimuthal velocities
+      if (sizeof(S) < sizeof(T) && dir == 0) b[o] += (T)bg_at(D.fl[o].vbg, j + k * m.sy);
     }
 #pragma unroll
     for (int ir = 0; ir < N - 1; ir++) {
@@ -1500,7 +1551,8 @@ __device__ __forceinline__ void b_collisions(const fb_disk_dev &D, Dims m, Geo<d
 #pragma unroll
     for (int o = 0; o < N; o++) {
       S *v = (S *)(dir == 0 ? D.fl[o].vxt : (dir == 1 ? D.fl[o].vyt : D.fl[o].vzt));
-      v[l] = (S)b[o];
+      if (sizeof(S) < sizeof(T) && dir == 0) v[l] = (S)(b[o] - (T)bg_at(D.fl[o].vbg, j + k * m.sy));
+      else v[l] = (S)b[o];
     }
   }
 }
@@ -1584,6 +1636,57 @@ static __global__ void k_disk_force_fold(const fb_disk_dev D, double x, double y
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mass of one fluid, ComputeMass (LowTasks.c:709-748): the sum over the active
+// cells of rho * Vol(i, j, k), Vol = Syk(k) * Sxi(i) / InvVj(j) (define.h:229),
+// in FP64 with compensation (Neumaier), so its rounding error does not grow
+// with the cell count and a change of the total at round-off level is
+// visible.  One warp per active ring writes the ring's (sum, compensation);
+// one CTA folds the rings in a fixed order.
+__device__ __forceinline__ void neumaier_add(double &s, double &c, double v) {
+  const double t = s + v;
+  if (fabs(s) >= fabs(v)) c += (s - t) + v;
+  else c += (v - t) + s;
+  s = t;
+}
+// (s, c) += (s2, c2) with the rounding error of s + s2 kept
+__device__ __forceinline__ void neumaier_merge(double &s, double &c, double s2, double c2) {
+  neumaier_add(s, c, s2);
+  c += c2;
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_mass_rings(Dims m, Geo<double> gd, const S *__restrict__ rho,
+                                                    double *__restrict__ part) {
+  const int r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (r >= m.ny * (m.is3d ? m.nz : 1)) return;
+  const int j = FB_NGH + r % m.ny, k = m.is3d ? FB_NGH + r / m.ny : 0;
+  const double syk = ld(gd.syk + k), ivj = ld(gd.invvj + j);
+  double s = 0.0, c = 0.0;
+  for (int i = lane; i < m.nx; i += 32) neumaier_add(s, c, (double)rho[m.l(i, j, k)] * (syk * ld(gd.sxi + i) / ivj));
+  for (int o = 16; o > 0; o >>= 1) {
+    const double s2 = __shfl_xor_sync(0xffffffffu, s, o), c2 = __shfl_xor_sync(0xffffffffu, c, o);
+    // both lanes of a pair fold in the same order (lower lane first)
+    if (lane & o) { double t = s2, tc = c2; neumaier_merge(t, tc, s, c); s = t; c = tc; }
+    else neumaier_merge(s, c, s2, c2);
+  }
+  if (lane == 0) { part[2 * r] = s; part[2 * r + 1] = c; }
+}
+
+__global__ void __launch_bounds__(256) k_mass_fold(const double *__restrict__ part, int n, double *__restrict__ out) {
+  __shared__ double ss[256], cc[256];
+  double s = 0.0, c = 0.0;
+  for (int r = threadIdx.x; r < n; r += 256) neumaier_merge(s, c, part[2 * r], part[2 * r + 1]);
+  ss[threadIdx.x] = s;
+  cc[threadIdx.x] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double S = 0.0, Cc = 0.0;
+    for (int t = 0; t < 256; t++) neumaier_merge(S, Cc, ss[t], cc[t]);
+    *out = S + Cc;
+  }
+}
+
 // shared memory of b_sweep_x2 for a ring of nx cells (rpc rings per CTA)
 __host__ __device__ inline size_t sweep_x2_smem(int nx, int C, int nt, int nq, size_t esz) {
   const int rpc = nt / (nx / C);
@@ -1606,6 +1709,10 @@ inline int disk_cx(const fb_disk_dev &d) { return d.tile_cx ? d.tile_cx : sweep_
 inline int disk_ns(const fb_disk_dev &d) { return d.tile_ns ? d.tile_ns : 8; }
 inline bool valid_cx(int nx, int c) { return (c == 1 || c == 2 || c == 4 || c == 8 || c == 16) && nx % c == 0 && nx / c <= 256; }
 inline bool valid_ns(int ns) { return ns == 4 || ns == 8 || ns == 16; }
+// polls of the staged-load wait before a disk is flagged (fb_disk_set_wait_limit)
+__host__ __device__ inline long long wait_limit(const fb_disk_dev &d) {
+  return d.wait_limit > 0 ? d.wait_limit : (d.wait_limit < 0 ? 0 : (1ll << 22));
+}
 
 template <typename T, int C, typename S = T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_sweep_x2(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
@@ -1613,9 +1720,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_sweep_x2(Dims m
                                                   S *q5, const S *__restrict__ vxt,
                                                   const double *__restrict__ vxmed_t, int *__restrict__ nshift_out,
                                                   const fb_scalars *__restrict__ scp,
-                                                  unsigned long long *__restrict__ errflag) {
+                                                  unsigned long long *__restrict__ errflag,
+                                                  const double *__restrict__ vbg, long long wait_limit) {
   b_sweep_x2<T, C, 256, S>(m, g, gd, nq, jlo, klo, nj, nrings, rho, q0, q1, q2, q3, q4, q5, vxt, vxmed_t, nshift_out,
-                        scp, errflag, blockIdx);
+                        scp, errflag, vbg, wait_limit, blockIdx);
 }
 
 }  // namespace fb

@@ -12,6 +12,7 @@ static inline QSrc<T, S> qsrc_from_v(const fb_fluid_dev &F, T of) {
   for (int q = 0; q < 6; q++) s.q[q] = nullptr;
   s.from_v = 1;
   s.of = of;
+  s.dl = nullptr;
   return s;
 }
 
@@ -24,7 +25,7 @@ static int launch_rowsum(const fb_disk_dev *d, int f, int which, cudaStream_t st
   const S *v = (const S *)(which == 0 ? F.vx : F.vxt);
   double *out = which == 0 ? F.vxmed : F.vxmed_t;
   if (d->precision != FB_FP64) {  // order-free: one warp per ring
-    k_rowsum_warp<S><<<(nring + 7) / 8, 256, 0, st>>>(m, gd, v, out, d->xlen);
+    k_rowsum_warp<S><<<(nring + 7) / 8, 256, 0, st>>>(m, gd, v, out, d->xlen, F.vbg);
     return (int)cudaGetLastError();
   }
   if (nring < 32 * 148) {  // few rings: 8 per CTA
@@ -47,7 +48,7 @@ static int launch_cfl(const fb_disk_dev *d, int f, cudaStream_t st) {
   dim3 grid(m.ny, m.is3d ? m.nz : 1);
   k_cfl<T, S><<<grid, 256, 0, st>>>(m, g, (const S *)F.rho, (const S *)F.cs, (const S *)F.vx, (const S *)F.vy,
                                   (const S *)F.vz, F.vxmed, d->scal_dev, d->cfl, d->mindx,
-                                  (unsigned long long *)d->dtmin);
+                                  (unsigned long long *)d->dtmin, F.vbg);
   return (int)cudaGetLastError();
 }
 
@@ -62,13 +63,13 @@ static int launch_sources(const fb_disk_dev *d, int f, cudaStream_t st) {
     constexpr int TX = 32, TY = 8;
     dim3 grid((m.nx + TX - 1) / TX, (m.ny + TY - 1) / TY);
     k_sources_cyl<T, TX, TY, S><<<grid, dim3(TX, TY), 0, st>>>(m, g, gd, (const S *)F.rho, (const S *)F.cs,
-        (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, d->scal_dev, F.dust, viscous);
+        (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, d->scal_dev, F.dust, viscous, F.vbg);
   } else {
     constexpr int TX = 32, TY = 4;
     dim3 grid((m.nx + TX - 1) / TX, (m.ny + TY - 1) / TY, m.nz);
     k_sources_sph<T, TX, TY, S><<<grid, dim3(TX, TY), 0, st>>>(m, g, gd, (const S *)F.rho, (const S *)F.cs,
         (const S *)F.vx, (const S *)F.vy, (const S *)F.vz, (S *)F.vxt, (S *)F.vyt, (S *)F.vzt, d->scal_dev,
-        F.dust, viscous);
+        F.dust, viscous, F.vbg);
   }
   return (int)cudaGetLastError();
 }
@@ -84,10 +85,10 @@ static int launch_bnd(const fb_disk_dev *d, int f, int vtemp, cudaStream_t st) {
   const int bx = 128;
   if (m.is3d) {
     dim3 gz((m.nx + bx - 1) / bx, m.sy, 6);
-    k_bnd_z<T, S><<<gz, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp);
+    k_bnd_z<T, S><<<gz, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp, F.vbg);
   }
   dim3 gy((m.nx + bx - 1) / bx, 6, m.sz);
-  k_bnd_y<T, S><<<gy, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp);
+  k_bnd_y<T, S><<<gy, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp, F.vbg);
   return (int)cudaGetLastError();
 }
 
@@ -106,6 +107,7 @@ static int launch_sweep_cols_n(const fb_disk_dev *d, int f, cudaStream_t st) {
   if (!m.is3d) {
     nq = 4;
     QSrc<T, S> src = qsrc_from_v<T, S>(F, (T)0);
+    src.dl = (const T *)F.dlb_y;
     rho_out = (S *)F.rho_a;
     q[0] = (S *)F.mpx; q[1] = (S *)F.mmx; q[2] = (S *)F.mpy; q[3] = (S *)F.mmy; q[4] = q[5] = nullptr;
     dim3 grid((m.nx + bx - 1) / bx, 1, (yhi - ylo + NS) / NS);
@@ -116,6 +118,7 @@ static int launch_sweep_cols_n(const fb_disk_dev *d, int f, cudaStream_t st) {
     const int zlo = FB_NGH - 1, zhi = m.nz + FB_NGH - 1;
     // Z sweep from V_temp into set A, rows 0 .. sy-2
     QSrc<T, S> src = qsrc_from_v<T, S>(F, (T)0);
+    src.dl = (const T *)F.dlb_z;
     dim3 gz((m.nx + bx - 1) / bx, m.sy - 1, (zhi - zlo + NS) / NS);
     k_sweep_col<T, 1, NS, S><<<gz, bx, 0, st>>>(m, g, src, nq, zlo, zhi, 0, (S *)F.rho_a, (S *)F.mpx, (S *)F.mmx,
                                              (S *)F.mpy, (S *)F.mmy, (S *)F.mpz, (S *)F.mmz, d->scal_dev);
@@ -124,7 +127,7 @@ static int launch_sweep_cols_n(const fb_disk_dev *d, int f, cudaStream_t st) {
     sa.rho = (const S *)F.rho_a; sa.vxt = (const S *)F.vxt; sa.vyt = (const S *)F.vyt; sa.vzt = (const S *)F.vzt;
     sa.q[0] = (const S *)F.mpx; sa.q[1] = (const S *)F.mmx; sa.q[2] = (const S *)F.mpy;
     sa.q[3] = (const S *)F.mmy; sa.q[4] = (const S *)F.mpz; sa.q[5] = (const S *)F.mmz;
-    sa.from_v = 0; sa.of = (T)0;
+    sa.from_v = 0; sa.of = (T)0; sa.dl = (const T *)F.dlb_y;
     dim3 gy((m.nx + bx - 1) / bx, zhi - zlo + 1, (yhi - ylo + NS) / NS);
     rho_out = (S *)F.rho_b;
     q[0] = (S *)F.mpx_b; q[1] = (S *)F.mmx_b; q[2] = (S *)F.mpy_b; q[3] = (S *)F.mmy_b; q[4] = (S *)F.mpz_b;
@@ -174,7 +177,7 @@ static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
     }                                                                                                      \
     k_sweep_x2<T, CC, S><<<gx, 256, smem, st>>>(m, g, gd, nq, ylo, klo, nj, nrings, rho_out, q[0], q[1], q[2], \
                                              q[3], q[4], q[5], (const S *)F.vxt, F.vxmed_t, F.nshift,      \
-                                             d->scal_dev, (unsigned long long *)d->dtmin + 1);                                                 \
+                                             d->scal_dev, (unsigned long long *)d->dtmin + 1, F.vbg, wait_limit(*d));                         \
   }
   switch (C) {
     case 16: FB_SX(16) break;
@@ -234,6 +237,17 @@ static int launch_disk_force(const fb_disk_dev *d, double x, double y, double z,
   return (int)cudaGetLastError();
 }
 
+// compensated mass of one fluid into out (device double); part: 2 x active
+// rings doubles of scratch
+template <typename S>
+static int launch_mass(const fb_disk_dev *d, int f, double *part, double *out, cudaStream_t st) {
+  Dims m = dims_of(*d);
+  const int nr = m.ny * (m.is3d ? m.nz : 1);
+  k_mass_rings<S><<<(nr + 7) / 8, 256, 0, st>>>(m, geo_of<double>(d->geomd), (const S *)d->fl[f].rho, part);
+  k_mass_fold<<<1, 256, 0, st>>>(part, nr, out);
+  return (int)cudaGetLastError();
+}
+
 }  // namespace fb
 
 #define FB_CAT2(a, b) a##_##b
@@ -263,6 +277,9 @@ int FB_CAT(fb_launch_newvel, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
 }
 int FB_CAT(fb_launch_collisions, FB_SUF)(const fb_disk_dev *d, void *s) {
   return fb::launch_collisions<FB_REAL, FB_STORE>(d, (cudaStream_t)s);
+}
+int FB_CAT(fb_launch_mass, FB_SUF)(const fb_disk_dev *d, int fluid, double *part, double *out, void *s) {
+  return fb::launch_mass<FB_STORE>(d, fluid, part, out, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_disk_force, FB_SUF)(const fb_disk_dev *d, double x, double y, double z, double rs,
                                           double *ring3, double *out3, void *s) {

@@ -94,6 +94,21 @@ class Disk:
         _abi.check(_abi.lib().fb_disk_device_fields(self._h, fluid, ptrs, C.byref(esz)))
         return [p for p in ptrs], esz.value
 
+    def mass(self, fluid: int = 0) -> float:
+        """Total mass of a fluid (compensated FP64 sum of rho * Vol over the
+        active cells, on the device)."""
+        m = C.c_double()
+        _abi.check(_abi.lib().fb_disk_mass(self._h, fluid, C.byref(m)))
+        return m.value
+
+    def background(self, fluid: int = 0):
+        """The per-ring azimuthal background an FP32 disk stores vx relative
+        to, shape (Nz+6 or 1, Ny+6); zeros for FP64 disks."""
+        nz, ny, _ = self.shape
+        o = np.zeros((nz, ny))
+        _abi.check(_abi.lib().fb_disk_get_background(self._h, fluid, _ptr(o)))
+        return o
+
     @property
     def stream(self) -> int:
         return _abi.lib().fb_disk_stream(self._h)

@@ -80,6 +80,13 @@ int fb_disk_step(fb_disk *d, double dt_interval, double *dt_out);
 /* [0] PhysicalTime [1] OMEGAFRAME [2] last dt [3..6] planet 0 x, y, vx, vy [7] Domega */
 int fb_disk_get_scalars(fb_disk *d, double out8[8]);
 
+/* Total mass of one fluid, ComputeMass (LowTasks.c:709-748): the sum over the
+ * active cells of rho * Vol(i, j, k), computed on the device in FP64 with
+ * compensated (Neumaier) summation, so a change of the total at round-off
+ * level stays visible.  Synchronous (the reference returns it to the host
+ * too); batch members: call fb_batch_sync first. */
+int fb_disk_mass(fb_disk *d, int fluid, double *mass);
+
 /* FARGO3D's output files (output.c): merged field files
  * <dir>/<fluid><field><n>.dat for field = dens, energy (the isothermal sound
  * speed), vx, vy[, vz] -- active cells, raw doubles, x fastest
@@ -104,8 +111,18 @@ int fb_disk_get_planets(fb_disk *d, int n, double *x, double *y, double *z, doub
                         double *mass, double *omegaframe);
 
 /* Device pointers of one fluid's state (rho, vx, vy, vz, cs) and the element
- * size, for callers that keep their inputs on the device. */
+ * size, for callers that keep their inputs on the device.  FP32 disks hold vx
+ * less the fluid's per-ring background (fb_disk_get_background). */
 int fb_disk_device_fields(fb_disk *d, int fluid, void *ptrs5[5], size_t *elem_size);
+
+/* FP32 disks store each fluid's azimuthal velocity relative to a per-ring
+ * background vbg(j, k): the FP64 ring means of the first vx the caller set.  A
+ * float then carries the deviation from the ring's rotation (the planet's wake,
+ * the slow viscous drift) instead of the rotation itself, so its rounding is
+ * that of the deviation; fb_disk_set_state / get_state convert both ways.  No
+ * counterpart in the reference (whose -DFLOAT build stores vx itself in FP32,
+ * types_def.h:2-6).  out: (Nz+6 or 1) x (Ny+6) doubles, zero for FP64 disks. */
+int fb_disk_get_background(fb_disk *d, int fluid, double *out);
 
 /* Stream the disk's kernels run on (a cudaStream_t). */
 void *fb_disk_stream(fb_disk *d);
@@ -168,6 +185,15 @@ int fb_batch_poll(fb_batch *b, int *status, double *phys_time, long long *steps)
  * autotuner (fargo3d_b200/autotune.py) picks them per (Nx, Ny, Nz,
  * precision).  A batch member's choice takes effect at the next run. */
 int fb_disk_set_tiles(fb_disk *d, int sweep_x_cells, int col_segment);
+/* Failure detection of the azimuthal sweep's staged ring loads (no
+ * counterpart in the reference, whose kernels never wait): a CTA polls the
+ * copies' completion at most `polls` times (0: the default 2^22; negative:
+ * not at all, the wait gives up at once).  A CTA that gives up waits,
+ * boundedly again, for its copies to land, writes nothing and flags the
+ * disk; fb_disk_step reports FB_ERR_NONFINITE at the next step (the flag is
+ * read with that step's CFL minimum), a batch freezes the member.  A batch
+ * member takes the value its disk has when it is activated. */
+int fb_disk_set_wait_limit(fb_disk *d, long long polls);
 int fb_disk_get_tiles(fb_disk *d, int *sweep_x_cells, int *col_segment);
 int fb_batch_set_tiles(fb_batch *b, int slot, int sweep_x_cells, int col_segment);
 
@@ -218,17 +244,24 @@ int fb_server_destroy(fb_server *s);
  * scratch is a fixed file-scope device array: meshes with more than
  * FB_NOALLOC_MAX_RINGS rings ((Ny+6) x (Nz+6 or 1)) are rejected with
  * FB_ERR_TOO_LARGE.  The first call on each device looks the array up and must
- * come before any stream capture; calls that overlap on the GPU race. */
+ * come before any stream capture; calls that overlap on the GPU race.
+ * Fields may be pitched as FARGO3D's cudaMallocPitch Fields are (Pitch_gpu /
+ * Stride_gpu, allocate.c:169-206): pitch and stride in elements, 0 for a
+ * dense [nz+6|1][ny+6][nx] array.  A state with a non-finite limit or a
+ * non-positive density yields *dt_out = NaN; a zero limit yields 0 (the
+ * reference's null time step). */
 #define FB_NOALLOC_MAX_RINGS 65536
 typedef struct {
   int nx, ny, nz;              /* active zones; nz <= 1: 2D                      */
   int spherical, alpha_visc;
-  const double *rho, *cs, *vx, *vy, *vz;  /* device fields, [nz+6|1][ny+6][nx] */
+  const double *rho, *cs, *vx, *vy, *vz;  /* device fields, [nz+6|1][ny+6][pitch] */
   const double *xmin, *ymin, *zmin;       /* device mesh edges (Xmin, Ymin, Zmin) */
   const double *sin_zmed;                 /* device sin(Zmed(k)) (spherical only) */
   double cfl, nu, alpha;
   double mindx;                /* min_i (Xmin[i+1] - Xmin[i])                     */
   double xlen;                 /* XMAX - XMIN                                     */
+  int pitch;                   /* elements between rows (Pitch_gpu); 0: nx       */
+  long long stride;            /* elements between layers (Stride_gpu); 0: pitch x (ny+6) */
 } fb_cfl_static_args;
 int fb_cfl_dt_static(const fb_cfl_static_args *args, double *dt_out, void *stream);
 

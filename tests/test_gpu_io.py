@@ -82,8 +82,14 @@ def test_fp32_state_transfer_rounds_like_a_host_cast():
     d = Disk(cfg, "fp32")
     d.set_state(rho, vx, vy, None, cs)
     got = d.state()
-    for k, v in (("rho", rho), ("vx", vx), ("vy", vy)):
+    for k, v in (("rho", rho), ("vy", vy)):
         assert np.array_equal(got[k], v.astype(np.float32).astype(np.float64)), k
+    # vx is stored less its ring's background (the FP64 ring mean of the
+    # first vx given): the float is the deviation's cast, read back plus it
+    bg = d.background()[:, :, None]
+    assert bg.shape[:2] == cfg.shape[:2]
+    assert np.allclose(bg[0, :, 0], vx.mean(axis=2)[0], rtol=1e-12, atol=0.0)
+    assert np.array_equal(got["vx"], (vx - bg).astype(np.float32).astype(np.float64) + bg)
     assert got["vz"].shape == cfg.shape and not got["vz"].any()
     out = {k: torch.empty(cfg.shape, dtype=torch.float64).pin_memory().numpy() for k in ("rho", "vx", "vy")}
     got2 = d.state(out=out)
