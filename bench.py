@@ -33,10 +33,14 @@ roofline    the dominant launch group of a step against the measured HBM copy
 cpu_baseline  the reference's own C sources (oracle/_ref, built from the
             reference tree) timed on this host on a bounded sample
 
-Under torchrun each rank advances its own disks (independent disks: weak
-scaling, no collective in the data path).  `--impl reference` times the
-reference's CPU implementation of the same workload on rank 0 only, using
-every host core for independent disks.
+Multi-GPU: `--gpus N` without a torchrun environment starts N ranks itself
+(torch.distributed.run on 127.0.0.1).  The batched workload is then ONE list
+of 64 x N disks split over the ranks by the LPT rule (fargo3d_b200/shard.py):
+about 64 disks per GPU (weak scaling), no collective in the data path; the
+single-disk workloads run one replica per rank.  `--impl reference` times the
+reference's CPU implementation (its own C sources with its stock -O3) of the
+same workload on rank 0 only, every host core running independent disks, for
+the same step count as the GPU arm.
 """
 from __future__ import annotations
 
@@ -64,16 +68,35 @@ LAUNCH_WORDS = {
     "3d": {"rowsum": 1, "cfl": 5, "sources": 8, "bnd_vtemp": 0, "rowsum_vtemp": 1,
            "sweep_cols": 26, "sweep_x": 15, "newvel": 11, "bnd": 0, "scalars": 0},
 }
-# DRAM bytes (read + write) per launch from one ncu capture of the batched
-# FP32 step (profiles/batched64_fp32_launches_and_top_kernels.md, --set full
-# on 3 eager steps); None where no capture of the workload exists
-TRAFFIC_BYTES = {("batched", "fp32"): {"sweep_x": (191.7184 + 331.205376) * 1e6,
-                                       "sources": (130.313216 + 44.268544) * 1e6,
-                                       "sweep_cols": (98.627328 + 123.73964) * 1e6,
-                                       "cfl": (127.243008 + 3.932928) * 1e6,
-                                       "newvel": (159.164928 + 64.728832) * 1e6}}
 KERNELS_PER_GROUP = {"2d": {"sweep_cols": 1, "bnd": 1, "bnd_vtemp": 1},
                      "3d": {"sweep_cols": 2, "bnd": 2, "bnd_vtemp": 2}}
+
+
+def build_hash() -> str:
+    """Digest of the library's sources: a DRAM-traffic figure applies to the
+    build it was captured on only."""
+    import hashlib
+    h = hashlib.sha256()
+    for d in (os.path.join(ROOT, "fargo3d_b200", "csrc"), os.path.join(ROOT, "include")):
+        for f in sorted(os.listdir(d)):
+            with open(os.path.join(d, f), "rb") as fh:
+                h.update(f.encode() + b"\0" + fh.read())
+    return h.hexdigest()[:16]
+
+
+def traffic_bytes(workload: str, precision: str, group: str):
+    """DRAM bytes (read + write) per launch of a launch group from the last
+    ncu capture (profiles/traffic.json), or None unless that capture was
+    taken on this very build and workload."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as fh:
+            t = json.load(fh)
+    except (OSError, ValueError):
+        return None
+    if t.get("build") != build_hash() or t.get("workload") != "%s:%s" % (workload, precision):
+        return None
+    return t.get("bytes_per_launch", {}).get(group)
 
 
 def peaks():
@@ -85,8 +108,11 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def workload(name: str, rank: int = 0):
+def workload(name: str, rank: int = 0, world: int = 1):
+    """This rank's disks and the workload's description.  Batched: rank's LPT
+    share of one global list of 64 x world disks (seeded once, seed 0)."""
     from fargo3d_b200 import config_batched, config_fargo2d, config_p3disof
+    from fargo3d_b200.shard import shard_disks
     if name == "fargo2d":
         return [config_fargo2d(384, 128, seed=rank)], "fargo2d 384x128 (2D cylindrical, 1 planet, nu=1e-5)"
     if name == "p3disof":
@@ -99,8 +125,9 @@ def workload(name: str, rank: int = 0):
         from fargo3d_b200 import serving_requests
         return [r.cfg for r in serving_requests(64, seed=rank)], ("serving requests, sizes {256x64, 512x128, "
                                                                   "1024x256, 2048x512} weighted {.4,.3,.2,.1}")
-    return config_batched(64, seed=rank), ("64 independent 2D disks, N_phi x N_r in {128..1024} x {64..512}, "
-                                           "alpha viscosity, 1 planet each")
+    return shard_disks(config_batched(64 * world, seed=0), rank, world), (
+        "%d independent 2D disks (%d per GPU), N_phi x N_r in {128..1024} x {64..512}, alpha viscosity, "
+        "1 planet each" % (64 * world, 64))
 
 
 class ClockSampler:
@@ -243,12 +270,92 @@ def run_serving(n_requests: int, rate: float, orbits: float, device: int, seed: 
             "span_s": span}
 
 
+def run_serving_fp64_sequential(n_requests: int, rate: float, orbits: float, device: int, seed: int = 0):
+    """The same request stream served by the plain FP64 path one request at a
+    time: each request runs alone (fb_disk_step, FP64) until its end time;
+    requests queue in arrival order behind the one running.  Service times
+    are measured (wall clock around each request's steps, state uploaded
+    before), the queue is then replayed on the measured times:
+    finish_k = max(arrival_k, finish_{k-1}) + service_k."""
+    from fargo3d_b200 import Disk, initial_state, serving_requests
+    reqs = serving_requests(n_requests, rate=rate, orbits=orbits, seed=seed)
+    service, work = [], 0
+    for r in reqs:
+        d = Disk(r.cfg, "fp64", device=device)
+        d.set_state(*initial_state(r.cfg))
+        d.initialize()
+        t0 = time.perf_counter()
+        steps = 0
+        while d.scalars()[0] < r.t_end * (1.0 - 1e-12):
+            d.step(r.t_end)
+            steps += 1
+        service.append(time.perf_counter() - t0)
+        work += steps * r.cfg.active_cells
+        d.close()
+    fin, lat = 0.0, []
+    for r, sv in zip(reqs, service):
+        fin = max(r.arrival, fin) + sv
+        lat.append(fin - r.arrival)
+    lat = np.array(lat)
+    return {"value": work / (fin - reqs[0].arrival), "unit": "cell-updates/s",
+            "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3), "p99": float(np.percentile(lat, 99) * 1e3),
+                           "max": float(lat.max() * 1e3)},
+            "orbits_per_request": orbits, "requests": len(reqs),
+            "how": "plain FP64 path (fb_disk_step), one request at a time in arrival order, measured service "
+                   "times replayed through the FIFO queue"}
+
+
+def fp32_errors(device: int):
+    """Per-field error of the FP32 path against the FP64 path after each
+    configuration's own step count, native CFL steps: the 64 batched disks
+    (1000 steps; FP64 batched path as the reference, it follows the CPU oracle
+    to round-off), the 3D spherical disk 512x256x48 (500 steps) and the
+    multifluid disk 768x256 x 5 fluids (1000 steps; plain paths).  Relative
+    L1 and L-infinity over the active cells."""
+    from fargo3d_b200 import Batch, Disk, config_batched, config_multifluid, config_p3disof
+
+    def err(a, b, k, is3d):
+        sl = (slice(3, -3) if is3d else slice(None), slice(3, -3), slice(None))
+        x, y = a[k][sl], b[k][sl]
+        den = np.sum(np.abs(y))
+        return {"l1": float(np.sum(np.abs(x - y)) / den) if den > 0 else 0.0,
+                "linf": float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300))}
+
+    out = {}
+    cfgs = config_batched(64)
+    st = {}
+    for prec in ("fp64", "fp32"):
+        b = Batch(cfgs, prec, device=device)
+        b.load_initial_states()
+        b.run(1000)
+        st[prec] = [b.state(i) for i in range(len(cfgs))]
+        b.close()
+    per = {k: [err(st["fp32"][i], st["fp64"][i], k, False) for i in range(len(cfgs))] for k in ("rho", "vx", "vy")}
+    out["batched_64_disks_1000_steps"] = {
+        k: {"l1_max": max(e["l1"] for e in v), "l1_median": float(np.median([e["l1"] for e in v])),
+            "linf_max": max(e["linf"] for e in v)} for k, v in per.items()}
+    out["batched_64_disks_1000_steps"]["disks_over_1e-5_l1_rho"] = sum(1 for e in per["rho"] if e["l1"] > 1e-5)
+    for name, cfg, n in (("p3disof_512x256x48_500_steps", config_p3disof(512, 256, 48), 500),
+                         ("multifluid_768x256x5_1000_steps", config_multifluid(768, 256), 1000)):
+        res = {}
+        for prec in ("fp64", "fp32"):
+            d = Disk(cfg, prec, device=device)
+            d.load_initial_state()
+            d.run(n)
+            res[prec] = [d.state(f) for f in range(cfg.nfluids)]
+            d.close()
+        keys = ("rho", "vx", "vy", "vz") if cfg.is3d else ("rho", "vx", "vy")
+        out[name] = {("fluid%d_" % f if cfg.nfluids > 1 else "") + k: err(res["fp32"][f], res["fp64"][f], k, cfg.is3d)
+                     for f in range(cfg.nfluids) for k in keys}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from fargo3d_b200 import Batch, Disk, initial_state
     from fargo3d_b200 import _abi
     torch.cuda.set_device(local_rank)
-    cfgs, wname = workload(args.workload, rank)
+    cfgs, wname = workload(args.workload, rank, world)
     batched = args.workload == "batched"
     precision = "fp32" if batched and args.precision_default else args.precision
     dim = "3d" if cfgs[0].is3d else "2d"
@@ -291,7 +398,14 @@ def run_ours(args, rank, world, local_rank):
         from fargo3d_b200.shard import max_over_ranks
         ms = max_over_ranks(ms, device="cuda")   # the job's time is its slowest rank's
         tdist.barrier()
-    value = cells * args.steps * world / (ms / 1e3)
+    # the whole job's cells: every rank's share of the global list (batched)
+    # or one replica per rank
+    if batched:
+        from fargo3d_b200 import config_batched
+        total_cells = sum(c.active_cells for c in config_batched(64 * world, seed=0))
+    else:
+        total_cells = cells * world
+    value = total_cells * args.steps / (ms / 1e3)
     # per-launch-group timing of one extra step (dominant kernel, roofline)
     if batched:
         prof, count = read_profile(L, L.fb_batch_profile_step, runner._h, 1e30)
@@ -335,6 +449,9 @@ def run_ours(args, rank, world, local_rank):
         outs = [r2.state(f, out=results[0][f]) for f in range(nf)]
     t_e2e = time.perf_counter() - t0
     r2.close()
+    if dist:
+        from fargo3d_b200.shard import max_over_ranks
+        t_e2e = max_over_ranks(t_e2e, device="cuda")
     nstored = sum(int(np.prod(c.shape)) for c in cfgs) * nf
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
@@ -342,15 +459,17 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32", "data": "synthetic",
         "config": {"workload": wname, "precision": precision, "disks_per_gpu": len(cfgs),
                    "active_cells_per_gpu": cells,
+                   "disk_seeds": [c.seed for c in cfgs] if batched else [cfgs[0].seed],
                    "parallelism": "independent disks per GPU (no collective)" if world > 1 else "one GPU",
                    "mode": "batched launches + CUDA graph" if batched else "plain, one disk",
                    "l2": "state (%d MB) larger than L2 (126 MB); no flush needed" % (nstored * esz * 5 // 2 ** 20)},
-        "e2e": {"value": cells * args.steps * world / t_e2e, "unit": "cell-updates/s",
+        "e2e": {"value": total_cells * args.steps / t_e2e, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": (5 if dim == "3d" else 4) * nstored * 8 / args.steps,
                 "d2h_bytes_per_step": len(keys) * nstored * 8 / args.steps + (0 if batched else 16)},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
-                     "traffic": TRAFFIC_BYTES.get((args.workload, precision), {}).get(dom),
+                     "traffic": traffic_bytes(args.workload, precision, dom),
+                     "build": build_hash(),
                      "alg_bytes_per_launch": dom_bytes, "launch_ms": prof[dom],
                      "step_alg_frac": (ALG_WORDS[dim] + (ALG_WORDS[dim] - 1) * (nf - 1)) * esz * cells
                                       * args.steps / (ms / 1e3) / 1e9 / hbm},
@@ -369,17 +488,22 @@ def run_ours(args, rank, world, local_rank):
 
 # --------------------------------------------------------------------------
 def _ref_disk_worker(job):
-    """One disk advanced by the reference's own sources (oracle/_ref)."""
+    """One disk advanced by the reference's own sources (oracle/_ref, built
+    with the reference's stock -O3; the parity build if that is missing)."""
     cfg, steps = job
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from fargo3d_b200 import initial_state
-    try:
-        d = pyoracle.Disk(cfg, "ref")
-        kind = "reference"
-    except FileNotFoundError:
+    d, kind = None, "port"
+    for k in ("ref_o3", "ref"):
+        try:
+            d = pyoracle.Disk(cfg, k)
+            kind = "reference" if k == "ref_o3" else "reference (-O2 parity build)"
+            break
+        except FileNotFoundError:
+            continue
+    if d is None:
         d = pyoracle.Disk(cfg, "oracle")
-        kind = "port"
     for f in range(cfg.nfluids):
         d.set_state(*initial_state(cfg, f), fluid=f)
     d.initialize()
@@ -412,7 +536,8 @@ def cpu_reference(cfgs, steps):
         # makespan of the stepping itself (process start-up excluded)
         wall = max(r[2] for r in res) - min(r[1] for r in res)
     work = sum(r[0] for r in res)
-    kind = "reference" if all(r[3] == "reference" for r in res) else "port"
+    kinds = sorted(set(r[3] for r in res))
+    kind = kinds[0] if len(kinds) == 1 else "mixed: " + ", ".join(kinds)
     return work / wall, kind, cores, wall
 
 
@@ -427,6 +552,26 @@ def cpu_model():
     return "unknown"
 
 
+def cpu_steps_for(cfgs, steps, cores):
+    """Steps of the CPU sample: the GPU arm's count, capped so the sample is
+    about 30 s of host work (at ~3 M cell-updates/s per core)."""
+    work = sum(c.active_cells * c.nfluids for c in cfgs)
+    cap = max(1, int(30.0 * 3.0e6 * max(1, min(cores, len(cfgs))) / max(work, 1)))
+    return max(1, min(steps, cap))
+
+
+def relaunch_with_ranks(n: int) -> int:
+    """`--gpus N` outside torchrun: start N ranks of this same command."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(n),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -439,30 +584,34 @@ def main():
     ap.add_argument("--orbits", type=float, default=0.25, help="serving: orbits per request")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg of the default run")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 error leg of the default run")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
-    ap.add_argument("--cpu-steps", type=int, default=0, help="reference steps per disk (0: auto)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg (profiling runs)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_with_ranks(args.gpus))
     args.precision_default = args.precision is None
     if args.precision is None:
         args.precision = "fp32" if args.workload == "batched" else "fp64"
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
-    cfgs, wname = workload(args.workload, 0)
-    auto = {"batched": 6, "p3disof": 2, "fargo2d": 300, "multifluid": 20, "serving": 6}[args.workload]
-    cpu_steps = args.cpu_steps or auto
     if args.impl == "reference":
         if rank != 0:
             return
-        steps = max(1, min(args.steps, cpu_steps))
-        v, kind, cores, wall = cpu_reference(cfgs, steps)
+        # the GPU arm's workload (for N > 1 its first 64 disks: a bounded
+        # sample of the same distribution), the GPU arm's step count
+        gcfgs, wname = workload(args.workload, 0, 1)
+        cores = max(1, min(len(gcfgs), os.cpu_count() or 1))
+        steps = cpu_steps_for(gcfgs, args.steps, cores)
+        v, kind, cores, wall = cpu_reference(gcfgs, steps)
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": world,
-                "steps": steps, "warmup": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": wname, "precision": "fp64 (the reference CPU build)"},
+                "steps": steps, "warmup": 0, "ms_per_step": wall / steps * 1e3, "higher_is_better": True,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": wname, "precision": "fp64 (the reference CPU build, stock -O3)"},
                 "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": kind,
-                                 "sample": "%d hydro steps of every disk, %d single-threaded processes, %.1f s (%s)"
-                                           % (steps, cores, wall, cpu_model())},
+                                 "sample": "%d hydro steps of each of %d disks, %d single-threaded processes, "
+                                           "%.1f s (%s)" % (steps, len(gcfgs), cores, wall, cpu_model())},
                 "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -470,6 +619,7 @@ def main():
         if rank != 0:
             return
         sv = run_serving(args.requests, args.rate, args.orbits, local_rank)
+        sv["fp64_one_at_a_time"] = run_serving_fp64_sequential(args.requests, args.rate, args.orbits, local_rank)
         line = {"metric": METRIC, "value": sv["value"], "unit": "cell-updates/s", "n_gpus": 1,
                 "steps": sv["requests"], "warmup": 4, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -486,15 +636,23 @@ def main():
     line = run_ours(args, rank, world, local_rank)
     if rank == 0 and world == 1 and args.workload == "batched" and not args.no_serving:
         line["serving"] = run_serving(args.requests, args.rate, args.orbits, local_rank)
-    if rank == 0 and not args.no_cpu:
-        v, kind, cores, wall = cpu_reference(cfgs, cpu_steps)
+        line["serving"]["fp64_one_at_a_time"] = run_serving_fp64_sequential(args.requests, args.rate, args.orbits,
+                                                                            local_rank)
+    if rank == 0 and world == 1 and args.workload == "batched" and not args.no_accuracy:
+        line["fp32_error"] = fp32_errors(local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cfgs, _ = workload(args.workload, 0, 1)
+        cores = max(1, min(len(cfgs), os.cpu_count() or 1))
+        steps = cpu_steps_for(cfgs, args.steps, cores)
+        v, kind, cores, wall = cpu_reference(cfgs, steps)
         line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": kind,
-                                "sample": "%d hydro steps of every disk, %d single-threaded processes, %.1f s (%s)"
-                                          % (cpu_steps, cores, wall, cpu_model())}
+                                "sample": "%d hydro steps of each of %d disks, %d single-threaded processes, "
+                                          "%.1f s (%s)" % (steps, len(cfgs), cores, wall, cpu_model())}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as tdist
+        tdist.barrier()
         tdist.destroy_process_group()
 
 

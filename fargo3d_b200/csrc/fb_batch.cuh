@@ -80,6 +80,20 @@ __global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 
   // 128 cells keep all 256 busy); min and OR do not depend on the order
   int r = 0, i = threadIdx.x;
   while (i >= m.nx) { i -= m.nx; r++; }
+  if constexpr (sizeof(T) == 4 && sizeof(S) == 4) {
+    if (!m.is3d) {   // FP32 2D: per-ring reciprocals, no division per cell
+#pragma unroll 2
+      for (; r < nr;) {
+        const int j = j0 + r;
+        mn = fmin(mn, (double)cfl_cell32(m, g, (const float *)F.rho, (const float *)F.cs, (const float *)F.vx,
+                                         (const float *)F.vy, F.vxmed[j] - bg_at(F.vbg, j), nu, alpha, (float)D.cfl,
+                                         i, j, bad));
+        i += blockDim.x;
+        while (i >= m.nx) { i -= m.nx; r++; }
+      }
+      r = nr;
+    }
+  }
 #pragma unroll 2
   for (; r < nr;) {
     const int j = j0 + r;
@@ -104,6 +118,14 @@ __global__ void __launch_bounds__(SRC2_TX *SRC2_TY, sizeof(S) == 4 ? FB_SRC_MINB
   b_sources_cyl<T, SRC2_TX, SRC2_TY, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), (const S *)F.rho,
                                      (const S *)F.cs, (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, scp,
                                      F.dust, !F.dust, F.vbg, bid);
+}
+
+// FP32 storage, 2D: FP32 arithmetic, column-marching warps (fb_sources32.cuh)
+static __global__ void __launch_bounds__(S32_WARPS * 32, FB_S32_MINB) kb_sources_cyl32(const fb_disk_dev *ds, const int4 *items, int f) {
+  FB_TILE
+  b_sources_cyl32(dims_of(D), geo_of<float>(D.geom), geo_of<double>(D.geomd), (const float *)F.rho,
+                  (const float *)F.cs, (const float *)F.vx, (const float *)F.vy, (float *)F.vxt, (float *)F.vyt, scp,
+                  F.dust, !F.dust, F.vbg, (const float *)F.shear_bg, bid);
 }
 
 template <typename T, typename S>
@@ -258,8 +280,9 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
       case ST_ROWSUM: g = dim3(B->precision == FB_FP64 ? (sy * sz + 31) / 32 : (sy * sz + 7) / 8); break;
       case ST_CFL: g = dim3((ny + CFL_R - 1) / CFL_R, D.is3d ? nz : 1); break;
       case ST_SOURCES:
-        g = D.is3d ? dim3((nx + SRC3_TX - 1) / SRC3_TX, (ny + SRC3_TY - 1) / SRC3_TY, nz)
-                   : dim3((nx + SRC2_TX - 1) / SRC2_TX, (ny + SRC2_TY - 1) / SRC2_TY);
+        if (D.is3d) g = dim3((nx + SRC3_TX - 1) / SRC3_TX, (ny + SRC3_TY - 1) / SRC3_TY, nz);
+        else if (B->precision == FB_FP32) g = dim3((nx + S32_COLS - 1) / S32_COLS, (ny + S32_NS - 1) / S32_NS);
+        else g = dim3((nx + SRC2_TX - 1) / SRC2_TX, (ny + SRC2_TY - 1) / SRC2_TY);
         break;
       case ST_BND_Z: g = D.is3d ? dim3((nx + BND_BX - 1) / BND_BX, sy, 6) : dim3(0); break;
       case ST_BND_Y: g = dim3((nx + BND_BX - 1) / BND_BX, 6, sz); break;
@@ -345,6 +368,7 @@ static int launch_step(fb_batch *B, double DT) {
   pmark(st, "scalars");
   for (int f = 0; f < nf; f++) {
     if (B->is3d) kb_sources_sph<T, S><<<grid(ST_SOURCES), dim3(SRC3_TX, SRC3_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
+    else if (sizeof(S) == 4) kb_sources_cyl32<<<grid(ST_SOURCES), S32_WARPS * 32, 0, st>>>(ds, B->items[ST_SOURCES], f);
     else kb_sources_cyl<T, S><<<grid(ST_SOURCES), dim3(SRC2_TX, SRC2_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
     pmark(st, "sources");
     if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 1, 1);

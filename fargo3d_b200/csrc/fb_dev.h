@@ -47,6 +47,10 @@ typedef struct {
      or zero (no vx given yet) means no background. */
   double *vbg;
   void *dlb_y, *dlb_z;
+  /* the background's r-phi shear of face j (2D cylindrical sources):
+     (vbg(j) - vbg(j-1)) / (Ymed(j) - Ymed(j-1)) - (vbg(j) + vbg(j-1)) / (2 Ymin(j)),
+     formed in double, stored in the disk's precision */
+  void *shear_bg;
   int has_bg;
 } fb_fluid_dev;
 

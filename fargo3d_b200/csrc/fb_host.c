@@ -404,7 +404,7 @@ int fb_params_bytes(const fb_params *p, int precision, size_t *out) {
   fields = is3d ? 15 + 7 : 11;
   b = (size_t)p->nfluids * (fields * nc * esz + 2 * rings * sizeof(double) + rings * sizeof(int) + 4 * rings * esz);
   /* FP32: per-ring azimuthal background and its y / z differences */
-  if (precision != FB_FP64) b += (size_t)p->nfluids * rings * (sizeof(double) + 2 * esz);
+  if (precision != FB_FP64) b += (size_t)p->nfluids * rings * (sizeof(double) + 3 * esz);
   b += 2 * sizeof(double) * (6 * ((size_t)p->nx + 1) + 20 * (sy + 1) + 16 * (sz + 1));
   b += sizeof(double) * (18 + 6 * sz + 6 * sy + 6) + sizeof(double) * (sy + 2 * sz);
   b += 64 + sizeof(fb_scalars) + 64 * 16 + sizeof(double) * (2 * rings + 2);
@@ -609,7 +609,8 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
       return rc;
     }
     if (precision == FB_FP32 &&   /* zero until the first vx arrives (fb_disk_set_state) */
-        ((rc = dalloc(D, (void **)&F->vbg, f2)) || (rc = dalloc(D, &F->dlb_y, e2)) || (rc = dalloc(D, &F->dlb_z, e2)))) {
+        ((rc = dalloc(D, (void **)&F->vbg, f2)) || (rc = dalloc(D, &F->dlb_y, e2)) || (rc = dalloc(D, &F->dlb_z, e2)) ||
+         (rc = dalloc(D, &F->shear_bg, e2)))) {
       fb_disk_destroy(D);
       return rc;
     }

@@ -246,6 +246,32 @@ __device__ __forceinline__ T cfl_cell(const Dims &m, const Geo<T> &g, const S *_
   return dtc;
 }
 
+// The same limit for FP32 2D disks (uniform azimuthal spacing): the zone
+// sizes enter as per-ring reciprocals, the maxima of quotients as maxima of
+// products, and the square root and division at the end as one reciprocal
+// square root -- algebraically cfl.c's expression, rounded differently.
+__device__ __forceinline__ float cfl_cell32(const Dims &m, const Geo<float> &g, const float *__restrict__ rho,
+                                            const float *__restrict__ cs, const float *__restrict__ vx,
+                                            const float *__restrict__ vy, double vm, float nu, float alpha,
+                                            float cfl_num, int i, int j, bool &bad) {
+  const long long l = m.l(i, j, 0);
+  const long long lxp = (i < m.nx - 1) ? l + 1 : l - (m.nx - 1);
+  const float izx = ld(g.invdiffxmed + 0) * ld(g.inv_ymed + j), izy = 1.0f / ld(g.sxj + j);
+  const float vxl = vx[l], vxp = vx[lxp], vyl = vy[l], vyp = vy[l + m.pitch], c = cs[l];
+  const float vmf = (float)vm;
+  const float visc = m.alpha ? alpha * c * c * ld(g.visc_j + j) : nu;
+  const float ss = fabsf(c);
+  const float mx7 = fmaxf(izx, izy);
+  const float c1 = ss * mx7;
+  const float c2 = fmaxf(fabsf(vxl - vmf), fabsf(vxp - vmf)) * izx;
+  const float c3 = fmaxf(fabsf(vyl), fabsf(vyp)) * izy;
+  const float c5 = fmaxf(fabsf(vxp - vxl) * izx, fabsf(vyp - vyl) * izy) * (4.0f * (float)FB_CVNR);
+  const float c7 = 4.0f * visc * (mx7 * mx7);
+  const float dtc = cfl_num * rsqrtf(c1 * c1 + c2 * c2 + c3 * c3 + c5 * c5 + c7 * c7);
+  bad |= !(dtc == dtc) || !(rho[l] > 0.0f);
+  return dtc;
+}
+
 // Shear limit of ring j (cfl_b.c:20-31).
 template <typename T>
 __device__ __forceinline__ double cfl_shear(const Geo<T> &g, const double *__restrict__ vxmed, double cfl_num,
@@ -1251,6 +1277,49 @@ __device__ __forceinline__ void chunk_iface(const T *w, const T *v, const Z &zon
   }
 }
 
+// The same interfaces for FP32 rings, whose azimuthal zones are one size z:
+// the van Leer slope's zone factors cancel into the Courant number v dt / z
+// (dtz = dt / z), leaving one division (the harmonic mean) per cell, and the
+// PPA's xi = v dt / z is one product.  Algebraically vanleer_x_a/_b and
+// fargo_ppa_a..d; rounded differently.
+template <int C>
+__device__ __forceinline__ void chunk_iface32(const float *w, const float *v, float dtz, bool ppa, float *qs) {
+  if (!ppa) {
+    float sl[C + 2];  // cells c0-1 .. c0+C: 2 dq+ dq- / (dq- + dq+) of the unscaled differences
+#pragma unroll
+    for (int u = 0; u < C + 2; u++) {
+      const float dqm = w[u + 2] - w[u + 1], dqp = w[u + 3] - w[u + 2];
+      sl[u] = (dqp * dqm <= 0.0f) ? 0.0f : (2.0f * dqp * dqm) / (dqm + dqp);
+    }
+#pragma unroll
+    for (int f = 0; f <= C; f++) {
+      const float cr = v[f] * dtz;
+      if (v[f] > 0.0f) qs[f] = w[f + 2] + 0.5f * (1.0f - cr) * sl[f];
+      else qs[f] = w[f + 3] - 0.5f * (1.0f + cr) * sl[f + 1];
+    }
+  } else {
+    float sl[C + 4];  // cells c0-2 .. c0+C+1
+#pragma unroll
+    for (int u = 0; u < C + 4; u++) sl[u] = mc_slope(w[u], w[u + 1], w[u + 2]);
+#pragma unroll
+    for (int f = 0; f <= C; f++) {
+      float L, R, s;
+      if (v[f] > 0.0f) {
+        ppa_lr(w[f + 1], w[f + 2], w[f + 3], sl[f], sl[f + 1], sl[f + 2], L, R);
+        const float ksi = v[f] * dtz;
+        s = R + ksi * (w[f + 2] - R);
+        s += ksi * (1.0f - ksi) * (2.0f * w[f + 2] - R - L);
+      } else {
+        ppa_lr(w[f + 2], w[f + 3], w[f + 4], sl[f + 1], sl[f + 2], sl[f + 3], L, R);
+        const float ksi = -v[f] * dtz;
+        s = L + ksi * (w[f + 3] - L);
+        s += ksi * (1.0f - ksi) * (2.0f * w[f + 3] - R - L);
+      }
+      qs[f] = s;
+    }
+  }
+}
+
 template <typename T, int C, int NT, typename S = T>
 __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const Geo<double> &gd, int nq, int jlo,
                                            int klo, int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,
@@ -1379,6 +1448,14 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
       if (pass == 0) {
 #pragma unroll
         for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nxp + P(wrap(c0 + f))] - vm_rel);  // residual
+      } else if constexpr (sizeof(T) == 4) {
+        // uniform fractional velocity (compute_residual.c:68-73), FP64; the
+        // FP32 path's azimuthal spacing is uniform, so it is one value per ring
+        const double zx = (double)zsx(m, gd, 0, j, k);
+        const double ntilde = vm * dtd / zx;
+        const T vf = (T)((ntilde - floor(ntilde + 0.5)) * zx / dtd);
+#pragma unroll
+        for (int f = 0; f <= C; f++) v[f] = vf;
       } else {
 #pragma unroll
         for (int f = 0; f <= C; f++) {  // uniform fractional velocity (compute_residual.c:68-73), FP64
@@ -1415,14 +1492,28 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
       };
       T wr[C + 6], rs[C + 1], out[C];
       window(src, wr);
-      chunk_iface<T, C>(wr, v, zone, dt, pass == 1, rs);
+      // FP32: one reciprocal of each window density, shared by the momenta
+      T irw[C + 6];
+      if constexpr (sizeof(T) == 4) {
+        chunk_iface32<C>((const float *)wr, (const float *)v, (float)(dt / zring), pass == 1, (float *)rs);
+#pragma unroll
+        for (int u = 0; u < C + 6; u++) irw[u] = (T)1.0 / wr[u];
+      } else {
+        chunk_iface<T, C>(wr, v, zone, dt, pass == 1, rs);
+      }
       for (int q = 0; q < nq; q++) {
         const T *sq = src + (1 + q) * nxp;
         T raw[C + 6], wq[C + 6], qs[C + 1];
         window(sq, raw);
+        if constexpr (sizeof(T) == 4) {
 #pragma unroll
-        for (int u = 0; u < C + 6; u++) wq[u] = raw[u] / wr[u];  // DivideByRho
-        chunk_iface<T, C>(wq, v, zone, dt, pass == 1, qs);
+          for (int u = 0; u < C + 6; u++) wq[u] = raw[u] * irw[u];  // DivideByRho
+          chunk_iface32<C>((const float *)wq, (const float *)v, (float)(dt / zring), pass == 1, (float *)qs);
+        } else {
+#pragma unroll
+          for (int u = 0; u < C + 6; u++) wq[u] = raw[u] / wr[u];  // DivideByRho
+          chunk_iface<T, C>(wq, v, zone, dt, pass == 1, qs);
+        }
 #pragma unroll
         for (int u = 0; u < C; u++) {
           const T fl = v[u] * qs[u] * rs[u] - v[u + 1] * qs[u + 1] * rs[u + 1];
@@ -1439,15 +1530,21 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
     }
     __syncthreads();
   }
-  // AdvectSHIFT (advect_shift.c:49-54): integer shift nround of cell 0
+  // AdvectSHIFT (advect_shift.c:49-54): integer shift nround of cell 0, one
+  // value per ring (formed by the ring's first thread)
+  __shared__ int s_nsh[NT];
+  if (active && lt == 0) {
+    const double ntilde0 = vm * dtd / (double)zsx(m, gd, 0, j, k);
+    const int nsh = (int)floor(ntilde0 + 0.5);
+    s_nsh[slot] = nsh;
+    if (nshift_out) nshift_out[j + k * m.sy] = nsh;
+  }
+  __syncthreads();
   for (int e = threadIdx.x; e < rpc * nx; e += NT) {
     const int s = e / nx, i = e - s * nx, rr = bid.x * rpc + s;
     if (rr >= nrings) continue;
     const int jj = jlo + rr % nj, kk = m.is3d ? klo + rr / nj : 0;
-    const double vms = vxmed_t[jj + kk * m.sy];
-    const double ntilde0 = vms * dtd / (double)zsx(m, gd, 0, jj, kk);
-    const int nsh = (int)floor(ntilde0 + 0.5);
-    if (i == 0 && nshift_out) nshift_out[jj + kk * m.sy] = nsh;
+    const int nsh = s_nsh[s];
     int it = (i - nsh) % nx;
     if (it < 0) it += nx;
     const T *b = bufA + (size_t)s * nf * nxp;
@@ -1673,7 +1770,7 @@ __global__ void __launch_bounds__(256) k_mass_rings(Dims m, Geo<double> gd, cons
   if (lane == 0) { part[2 * r] = s; part[2 * r + 1] = c; }
 }
 
-__global__ void __launch_bounds__(256) k_mass_fold(const double *__restrict__ part, int n, double *__restrict__ out) {
+static __global__ void __launch_bounds__(256) k_mass_fold(const double *__restrict__ part, int n, double *__restrict__ out) {
   __shared__ double ss[256], cc[256];
   double s = 0.0, c = 0.0;
   for (int r = threadIdx.x; r < n; r += 256) neumaier_merge(s, c, part[2 * r], part[2 * r + 1]);
@@ -1727,3 +1824,5 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_sweep_x2(Dims m
 }
 
 }  // namespace fb
+
+#include "fb_sources32.cuh"

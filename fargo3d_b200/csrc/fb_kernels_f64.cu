@@ -78,9 +78,11 @@ extern "C" int fb_launch_ring_mean(double *out, const double *src, int nx, int n
 // Neighbour differences of l(j, k) = vbg(j, k) R(j, k) along y and z (R the
 // cylindrical radius: Ymed, or Ymed sin(Zmed) on spherical meshes), taken in
 // double and stored in the disk's FP32 precision; 0 at the first row / layer.
+// Also the background's r-phi shear of face j for the 2D sources:
+// (vbg(j) - vbg(j-1)) / (Ymed(j) - Ymed(j-1)) - (vbg(j) + vbg(j-1)) / (2 Ymin(j)).
 __global__ void k_bg_diffs(const double *__restrict__ vbg, const double *__restrict__ ymed,
-                           const double *__restrict__ szmed, int sy, int sz, int sph, float *__restrict__ dly,
-                           float *__restrict__ dlz) {
+                           const double *__restrict__ ymin, const double *__restrict__ szmed, int sy, int sz,
+                           int sph, float *__restrict__ dly, float *__restrict__ dlz, float *__restrict__ shb) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= sy * sz) return;
   const int j = r % sy, k = r / sy;
@@ -88,14 +90,16 @@ __global__ void k_bg_diffs(const double *__restrict__ vbg, const double *__restr
   const double l0 = ell(j, k);
   dly[r] = j > 0 ? (float)(l0 - ell(j - 1, k)) : 0.0f;
   dlz[r] = k > 0 ? (float)(l0 - ell(j, k - 1)) : 0.0f;
+  shb[r] = j > 0 ? (float)((vbg[r] - vbg[r - 1]) / (ymed[j] - ymed[j - 1]) - 0.5 * (vbg[r] + vbg[r - 1]) / ymin[j])
+                 : 0.0f;
 }
 
 extern "C" int fb_launch_bg_diffs(const fb_disk_dev *d, int fluid, void *stream) {
   const fb_fluid_dev &F = d->fl[fluid];
-  if (!F.vbg || !F.dlb_y || !F.dlb_z) return 0;
+  if (!F.vbg || !F.dlb_y || !F.dlb_z || !F.shear_bg) return 0;
   const int n = d->sy * d->sz;
   k_bg_diffs<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
-      F.vbg, (const double *)d->geomd.ymed, (const double *)d->geomd.sin_zmed, d->sy, d->sz, d->spherical,
-      (float *)F.dlb_y, (float *)F.dlb_z);
+      F.vbg, (const double *)d->geomd.ymed, (const double *)d->geomd.ymin, (const double *)d->geomd.sin_zmed, d->sy,
+      d->sz, d->spherical, (float *)F.dlb_y, (float *)F.dlb_z, (float *)F.shear_bg);
   return (int)cudaGetLastError();
 }

@@ -59,7 +59,12 @@ static int launch_sources(const fb_disk_dev *d, int f, cudaStream_t st) {
   Geo<T> g = geo_of<T>(sizeof(T) == 8 ? d->geomd : d->geom);
   Geo<double> gd = geo_of<double>(d->geomd);
   const int viscous = !F.dust;
-  if (!m.is3d) {
+  if (!m.is3d && sizeof(S) == 4) {   // FP32 storage: FP32 arithmetic, column-marching warps
+    dim3 grid((m.nx + S32_COLS - 1) / S32_COLS, (m.ny + S32_NS - 1) / S32_NS);
+    k_sources_cyl32<<<grid, S32_WARPS * 32, 0, st>>>(m, geo_of<float>(d->geom), gd, (const float *)F.rho,
+        (const float *)F.cs, (const float *)F.vx, (const float *)F.vy, (float *)F.vxt, (float *)F.vyt, d->scal_dev,
+        F.dust, viscous, F.vbg, (const float *)F.shear_bg);
+  } else if (!m.is3d) {
     constexpr int TX = 32, TY = 8;
     dim3 grid((m.nx + TX - 1) / TX, (m.ny + TY - 1) / TY);
     k_sources_cyl<T, TX, TY, S><<<grid, dim3(TX, TY), 0, st>>>(m, g, gd, (const S *)F.rho, (const S *)F.cs,

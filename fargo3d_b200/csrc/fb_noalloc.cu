@@ -134,13 +134,13 @@ extern "C" int fb_cfl_dt_static(const fb_cfl_static_args *a, double *dt_out, voi
   if (is3d && (!a->vz || !a->zmin || (a->spherical && !a->sin_zmed)))
     return fb_internal_fail(FB_ERR_ARG, "fb_cfl_dt_static: null 3D field or mesh pointer", 0);
   const int sy = a->ny + 6;
+  const long long nring = (long long)sy * (is3d ? a->nz + 6 : 1);
+  if (nring > FB_NOALLOC_MAX_RINGS)
+    return fb_internal_fail(FB_ERR_TOO_LARGE, "fb_cfl_dt_static: more rings than FB_NOALLOC_MAX_RINGS", 0);
   const long long pitch = a->pitch > 0 ? a->pitch : a->nx;
   const long long stride = a->stride > 0 ? a->stride : pitch * sy;
   if (pitch < a->nx || (is3d && stride < pitch * sy))
     return fb_internal_fail(FB_ERR_ARG, "fb_cfl_dt_static: pitch below Nx or stride below pitch x (Ny+6)", 0);
-  const long long nring = (long long)sy * (is3d ? a->nz + 6 : 1);
-  if (nring > FB_NOALLOC_MAX_RINGS)
-    return fb_internal_fail(FB_ERR_TOO_LARGE, "fb_cfl_dt_static: more rings than FB_NOALLOC_MAX_RINGS", 0);
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return fb_internal_fail(FB_ERR_CUDA, "fb_cfl_dt_static: cudaGetDevice", (int)e);
   if (dev < 0 || dev >= FB_NOALLOC_MAX_DEVICES) return fb_internal_fail(FB_ERR_CUDA, "fb_cfl_dt_static: device index", 0);
   {

@@ -1,0 +1,206 @@
+// fb_sources32.cuh -- the source stage of FP32 2D cylindrical disks
+// (algogas.c:30-120: ComputePressureFieldIso, the planets' potential,
+// CorrectVtheta, SubStep1_x/y, visctensor_cyl + addviscosity_cyl, SubStep2_a/b)
+// in FP32 arithmetic, without shared memory or CTA barriers.
+//
+// Layout of the work: a warp owns 32 consecutive columns (azimuthal cells) of
+// a ring and marches down NS rows (radii), keeping the rows j-1, j, j+1 of its
+// column in registers; the neighbours i-1 / i+1 come from the adjacent lanes
+// by shuffle.  Lanes 0 and 31 are halo lanes: they compute what their
+// neighbours need but write nothing, so a warp writes 30 columns.  Every
+// quantity (pressure, planet potential, the three viscous stresses) is formed
+// once per cell and row, none is staged or recomputed for a tile halo.
+//
+// Why FP32 is safe here: FP32 disks store v_phi relative to a per-ring
+// background vbg (fb_fluid_dev), so no large velocity enters the arithmetic.
+// What remains large is the background's own radial balance -- centrifugal
+// (B^2 / r) against the star's gravity, with B = vbg + r OMEGAFRAME on the
+// face -- two O(1) terms whose difference is O(h^2).  That difference is
+// formed per row in FP64 (K_j below) and only the perturbation terms,
+// (2 B + d) d / r with d the small relative velocity, the planets' potential
+// and the pressure gradient, are formed in FP32.  Likewise the background's
+// r-phi shear enters tau_r_phi as one per-row constant (fb_fluid_dev shear_bg,
+// formed in FP64).  The planets' potential is the only potential evaluated
+// per cell: the star's -GM/r cancels in the x differences and is part of
+// K_j in the y difference.
+#pragma once
+#include "fb_kernels.cuh"
+
+namespace fb {
+
+constexpr int S32_WARPS = 4;                       // warps per CTA
+constexpr int S32_OUT = 30;                        // columns written per warp (lanes 1..30)
+constexpr int S32_COLS = S32_WARPS * S32_OUT;      // columns per CTA
+constexpr int S32_NS = 16;                         // rows per CTA
+// resident CTAs per SM the kernel is compiled for (register cap 64 at 8)
+#ifndef FB_S32_MINB
+#define FB_S32_MINB 8
+#endif
+
+// one row of a column: density, sound speed, relative azimuthal velocity
+// (CorrectVtheta applied), radial velocity, pressure, planets' potential
+struct Cell32 {
+  float r, c, u, vy, p, pot;
+};
+
+__device__ __forceinline__ float lane_m(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }    // column i-1
+__device__ __forceinline__ float lane_p(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }  // column i+1
+
+// planets' potential (potential.c:51-208 without the star's term), FP32
+__device__ __forceinline__ float pot_planets32(const fb_scalars *__restrict__ sc, float XC, float YC) {
+  float pot = 0.0f;
+  const int np = sc->nplanets;
+  for (int n = 0; n < np; n++) {
+    const float xp = (float)sc->px[n], yp = (float)sc->py[n], zp = (float)sc->pz[n];
+    const float dx = XC - xp, dy = YC - yp;
+    const float dist = dx * dx + dy * dy + zp * zp;
+    if (sc->indirect_term) pot += (float)(sc->pmass[n] / sc->pdist3[n]) * (XC * xp + YC * yp);
+    pot -= (float)sc->pmass[n] * rsqrtf(dist + (float)sc->psmooth2[n]);
+  }
+  return pot;
+}
+
+__device__ __forceinline__ Cell32 load_cell32(const Dims &m, const Geo<float> &g, const float *__restrict__ rho,
+                                              const float *__restrict__ cs, const float *__restrict__ vx,
+                                              const float *__restrict__ vy, const fb_scalars *__restrict__ sc,
+                                              float domega, int i, int j) {
+  const long long l = m.l(i, j, 0);
+  Cell32 o;
+  o.r = rho[l];
+  o.c = cs[l];
+  const float ym = ld(g.ymed + j);
+  o.u = vx[l] - domega * ym;     // CorrectVtheta (correct_vtheta.c:55-60)
+  o.vy = vy[l];
+  o.p = o.r * o.c * o.c;         // ComputePressureFieldIso
+  o.pot = pot_planets32(sc, ym * ld(g.cos_xmed + i), ym * ld(g.sin_xmed + i));
+  return o;
+}
+
+// tau_phi_phi and tau_r_r of row j at column i (visctensor_cyl.c): R is row
+// j, vyp the radial velocity of row j + 1, uxp the relative azimuthal
+// velocity of column i + 1 (all lanes call it: it shuffles)
+__device__ __forceinline__ void stress_diag32(const Geo<float> &g, const Cell32 &R, float vyp, int alpha_visc,
+                                              float nu, float alpha, float sxi0, int j, float &txx, float &tyy) {
+  const float uxp = lane_p(R.u);
+  const float visc = alpha_visc ? alpha * R.c * R.c * ld(g.visc_j + j) : nu;
+  const float dux = uxp - R.u;
+  const float syj = ld(g.syj + j), syjp = ld(g.syj + j + 1), sxj = ld(g.sxj + j);
+  float div_v = dux * sxj + (vyp * syjp * sxi0 - R.vy * syj * sxi0);
+  div_v *= (2.0f / 3.0f) * ld(g.invvj + j) / sxi0;
+  const float izx = ld(g.invdiffxmed + 0) * ld(g.inv_ymed + j);
+  txx = visc * R.r * (2.0f * dux * izx - div_v) + visc * R.r * (vyp + R.vy) * ld(g.inv_ymed + j);
+  tyy = visc * R.r * (2.0f * (vyp - R.vy) / sxj - div_v);
+}
+
+// tau_r_phi at the corner (i - 1/2, j - 1/2) from rows j (R) and j - 1 (Rm);
+// the background's shear of this face is shb (shuffles)
+__device__ __forceinline__ float stress_rphi32(const Geo<float> &g, const Cell32 &R, const Cell32 &Rm, int alpha_visc,
+                                               float nu, float alpha, float shb, int j) {
+  const float rxm = lane_m(R.r), rxym = lane_m(Rm.r), cxm = lane_m(R.c), cxym = lane_m(Rm.c), vyxm = lane_m(R.vy);
+  float viscm = nu;
+  if (alpha_visc) {
+    const float s = R.c + cxm + Rm.c + cxym;
+    viscm = alpha * 0.0625f * s * s * ld(g.viscm_j + j);
+  }
+  const float iyi = ld(g.inv_ymin + j);
+  return viscm * 0.25f * (R.r + rxm + Rm.r + rxym) *
+         ((R.vy - vyxm) * ld(g.invdiffxmed + 0) * iyi + (R.u - Rm.u) * ld(g.inv_dymed + j) -
+          0.5f * (R.u + Rm.u) * iyi + shb);
+}
+
+__device__ __forceinline__ void b_sources_cyl32(const Dims m, const Geo<float> g, const Geo<double> gd,
+    const float *__restrict__ rho, const float *__restrict__ cs, const float *__restrict__ vx,
+    const float *__restrict__ vy, float *__restrict__ vxt, float *__restrict__ vyt,
+    const fb_scalars *__restrict__ sc, int dust, int viscous, const double *__restrict__ vbg,
+    const float *__restrict__ shear_bg, uint3 bid) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int iu = (int)(bid.x * S32_WARPS + w) * S32_OUT - 1 + lane;   // unwrapped column of this lane
+  const int i = ((iu % m.nx) + m.nx) % m.nx;
+  const bool writes = lane >= 1 && lane <= S32_OUT && iu < m.nx;
+  const int j0 = FB_NGH + (int)bid.y * S32_NS, j1 = min(j0 + S32_NS, m.ny + FB_NGH);
+  if (j0 >= j1) return;
+  const double dtd = sc->dt, of = sc->omegaframe;
+  const float dt = (float)dtd, domega = (float)sc->domega, nu = (float)sc->nu, alpha = (float)sc->alpha;
+  const float sxi0 = ld(g.sxi + 0), idx0 = ld(g.invdiffxmed + 0);
+  const float c2 = (float)FB_CVNR;
+  // rows j0 - 1 and j0; the stresses of row j0 - 1 and the corner of row j0
+  Cell32 A = load_cell32(m, g, rho, cs, vx, vy, sc, domega, i, j0 - 1);
+  Cell32 C0 = load_cell32(m, g, rho, cs, vx, vy, sc, domega, i, j0);
+  float txx_m = 0.f, tyy_m = 0.f, tyx_c = 0.f;
+  if (viscous) {
+    stress_diag32(g, A, C0.vy, m.alpha, nu, alpha, sxi0, j0 - 1, txx_m, tyy_m);
+    tyx_c = stress_rphi32(g, C0, A, m.alpha, nu, alpha, ld(shear_bg + j0), j0);
+  }
+  for (int j = j0; j < j1; j++) {
+    const Cell32 P = load_cell32(m, g, rho, cs, vx, vy, sc, domega, i, j + 1);
+    float txx_c = 0.f, tyy_c = 0.f, tyx_p = 0.f;
+    if (viscous) {
+      stress_diag32(g, C0, P.vy, m.alpha, nu, alpha, sxi0, j, txx_c, tyy_c);
+      tyx_p = stress_rphi32(g, P, C0, m.alpha, nu, alpha, ld(shear_bg + j + 1), j + 1);
+    }
+    // neighbours by shuffle (every lane takes part)
+    const float rxm = lane_m(C0.r), pxm = lane_m(C0.p), potxm = lane_m(C0.pot);
+    const float uxm = lane_m(C0.u), uxp = lane_p(C0.u), umxp = lane_p(A.u);
+    const float txx_xm = lane_m(txx_c), tyx_xp = lane_p(tyx_c);
+    // the background's balance on face j: K = B^2 / r - d(Phi_star)/dr,
+    // B = (vbg(j) + vbg(j-1)) / 2 + Ymin(j) OMEGAFRAME, in FP64
+    const double Bd = 0.5 * (bg_at(vbg, j) + bg_at(vbg, j - 1)) + ld(gd.ymin + j) * of;
+    const float K = (float)(Bd * Bd * ld(gd.inv_ymin + j) -
+                            (ld(gd.pot_star + j) - ld(gd.pot_star + j - 1)) * ld(gd.inv_dymed + j));
+    const float B = (float)Bd;
+    if (writes) {
+      const float r = C0.r, rym = A.r;
+      const float izx = idx0 * ld(g.inv_ymed + j);
+      const float ym = ld(g.ymed + j), ymm = ld(g.ymed + j - 1), yi = ld(g.ymin + j), yip = ld(g.ymin + j + 1);
+      const float iyi = ld(g.inv_ymin + j), idym = ld(g.inv_dymed + j);
+      const float irx = 1.0f / (r + rxm);   // 1 / (rho + rho_{i-1}) (uniform azimuthal spacing)
+      const float ideny = 1.0f / (r * ld(g.sxj + j) + rym * ld(g.sxj + j - 1));
+      // SubStep1_x (substep1_x.c:107-117)
+      float ax = C0.u;
+      if (!dust) ax -= 2.0f * dt * irx * (C0.p - pxm) * izx;
+      ax -= (C0.pot - potxm) * dt * izx;
+      // SubStep1_y (substep1_y.c:146-192, cylindrical)
+      float ay = C0.vy;
+      if (!dust) ay -= 2.0f * dt * ideny * (C0.p - A.p);
+      const float d = 0.25f * (C0.u + uxp + A.u + umxp);
+      ay += (K + (2.0f * B + d) * d * iyi - (C0.pot - A.pot) * idym) * dt;
+      if (viscous) {
+        // addviscosity_cyl (addviscosity_cyl.c:106-124)
+        ax += 2.0f * (txx_c - txx_xm) * izx * irx * dt;
+        ax += 2.0f * (yip * yip * tyx_p - yi * yi * tyx_c) / ((yip - yi) * ym * ym * (rxm + r)) * dt;
+        ay += 2.0f * (ym * tyy_c - ymm * tyy_m) / ((ym - ymm) * (r + rym) * yi) * dt;
+        ay += 2.0f * (tyx_xp - tyx_c) / (sxi0 * yi * (r + rym)) * dt;
+        ay -= (txx_c + txx_m) / (yi * (r + rym)) * dt;
+      }
+      // SubStep2_a / SubStep2_b (substep2_a.c:107-129, substep2_b.c:150-175)
+      float dv = uxp - C0.u;
+      const float qx = dv < 0.0f ? c2 * c2 * r * dv * dv : 0.0f;
+      dv = C0.u - uxm;
+      const float qxm = dv < 0.0f ? c2 * c2 * rxm * dv * dv : 0.0f;
+      dv = P.vy - C0.vy;
+      const float qy = dv < 0.0f ? c2 * c2 * r * dv * dv : 0.0f;
+      dv = C0.vy - A.vy;
+      const float qym = dv < 0.0f ? c2 * c2 * rym * dv * dv : 0.0f;
+      ax += -2.0f * dt * (qx - qxm) * irx * izx;
+      ay += -2.0f * (qy - qym) * ideny * dt;
+      const long long l = m.l(i, j, 0);
+      vxt[l] = ax;   // relative to the background, as the state
+      vyt[l] = ay;
+    }
+    A = C0;
+    C0 = P;
+    txx_m = txx_c;
+    tyy_m = tyy_c;
+    tyx_c = tyx_p;
+  }
+}
+
+static __global__ void __launch_bounds__(S32_WARPS * 32, FB_S32_MINB) k_sources_cyl32(Dims m, Geo<float> g, Geo<double> gd,
+    const float *__restrict__ rho, const float *__restrict__ cs, const float *__restrict__ vx,
+    const float *__restrict__ vy, float *__restrict__ vxt, float *__restrict__ vyt,
+    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg,
+    const float *__restrict__ shear_bg) {
+  b_sources_cyl32(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, vbg, shear_bg, blockIdx);
+}
+
+}  // namespace fb

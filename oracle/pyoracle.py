@@ -63,20 +63,21 @@ def make_params(cfg) -> FoParams:
     return p
 
 
-def build():
-    """Compile the oracle restatement (and, when the reference tree is
-    present, the reference's own sources)."""
+def build(ref: str | None = None):
+    """Compile the oracle restatement and, when the reference tree is given
+    (`ref`, or FARGO_REFERENCE in the environment), the reference's own
+    sources; without one, the previously built oracle/_ref libraries stay."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    ref = os.environ.get("FARGO_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "src")):
+    ref = ref or os.environ.get("FARGO_REFERENCE")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
         subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref], check=True)
 
 
-def build_dropin():
+def build_dropin(ref: str | None = None):
     """The drop-in variants of the reference build (needs libfargo_b200.so
-    and the reference tree)."""
-    ref = os.environ.get("FARGO_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "src")):
+    and the reference tree, as for build())."""
+    ref = ref or os.environ.get("FARGO_REFERENCE")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
         subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref, "dropin"], check=True)
 
 
@@ -105,16 +106,21 @@ class Disk:
     _libs = {}
 
     def __init__(self, cfg, kind: str = "oracle"):
+        """kind: 'oracle' (the C restatement), 'ref' (the reference's sources
+        as the parity tests build them), 'ref_o3' (the same sources with the
+        reference's stock -O3, for timing) or 'dropin'."""
         self.cfg, self.kind = cfg, kind
         if kind == "oracle":
             path = os.path.join(HERE, "_build", "libfargo_oracle.so")
         elif kind == "dropin":
             path = os.path.join(HERE, "_ref", "libfargo_ref_dropin_%s.so" % ref_variant(cfg))
+        elif kind == "ref_o3":
+            path = os.path.join(HERE, "_ref", "libfargo_ref_%s_o3.so" % ref_variant(cfg))
         else:
             path = os.path.join(HERE, "_ref", "libfargo_ref_%s.so" % ref_variant(cfg))
         if not os.path.exists(path):
             raise FileNotFoundError(path)
-        if kind in ("ref", "dropin"):
+        if kind in ("ref", "ref_o3", "dropin"):
             # Each reference library holds one disk in its globals (and in
             # function-level statics such as potential.c's alreadycalculated):
             # load a fresh private copy per Disk.  dlopen identifies a library
