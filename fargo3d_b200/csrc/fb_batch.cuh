@@ -214,6 +214,15 @@ __global__ void __launch_bounds__(NV_BX) kb_newvel(const fb_disk_dev *ds, const 
   }
 }
 
+// FP32 2D: column-marching rows (fb_sources32.cuh); 128 columns x NV32_R rows a tile
+static __global__ void __launch_bounds__(128) kb_newvel_cyl32(const fb_disk_dev *ds, const int4 *items, int f) {
+  FB_TILE
+  b_newvel_cyl32(dims_of(D), geo_of<float>(D.geom), (const float *)F.rho_a, (const float *)F.mpx,
+                 (const float *)F.mmx, (const float *)F.mpy, (const float *)F.mmy, (float *)F.rho, (float *)F.vx,
+                 (float *)F.vy, (const float *)F.rho0, (const float *)F.vx0, (const float *)F.vy0, D.ramps,
+                 D.stockholm, scp, bid);
+}
+
 // The scalar work of the step for every disk, one thread per disk; then the
 // CFL minimum is reset for the next step.  dtmin[1] carries the kernels'
 // non-finite flag.  A disk with an end time uses it as its DT interval, so
@@ -305,7 +314,10 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
         g = dim3((nr + rpc - 1) / rpc);
         break;
       }
-      case ST_NEWVEL: g = dim3((nx + NV_BX - 1) / NV_BX, (ny + NV_R - 1) / NV_R, D.is3d ? nz : 1); break;
+      case ST_NEWVEL:
+        if (!D.is3d && B->precision == FB_FP32) g = dim3((nx + 127) / 128, (ny + NV32_R - 1) / NV32_R);
+        else g = dim3((nx + NV_BX - 1) / NV_BX, (ny + NV_R - 1) / NV_R, D.is3d ? nz : 1);
+        break;
     }
     for (unsigned z = 0; z < g.z; z++)
       for (unsigned y = 0; y < g.y; y++)
@@ -417,7 +429,8 @@ static int launch_step(fb_batch *B, double DT) {
     pmark(st, "sweep_x");
   }
   for (int f = 0; f < nf; f++) {
-    kb_newvel<TN, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
+    if (!B->is3d && sizeof(S) == 4) kb_newvel_cyl32<<<grid(ST_NEWVEL), 128, 0, st>>>(ds, B->items[ST_NEWVEL], f);
+    else kb_newvel<TN, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
     pmark(st, "newvel");
     if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 0, 1);
     kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 0, 0);

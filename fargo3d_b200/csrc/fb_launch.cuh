@@ -206,6 +206,13 @@ static int launch_newvel(const fb_disk_dev *d, int f, cudaStream_t st) {
   const S *mpy = (const S *)(b ? F.mpy_b : F.mpy), *mmy = (const S *)(b ? F.mmy_b : F.mmy);
   const S *mpz = (const S *)(b ? F.mpz_b : F.mpz), *mmz = (const S *)(b ? F.mmz_b : F.mmz);
   const int bx = 128;
+  if (!m.is3d && sizeof(S) == 4) {   // FP32 2D: column-marching rows
+    dim3 g2((m.nx + bx - 1) / bx, (m.ny + NV32_R - 1) / NV32_R);
+    k_newvel_cyl32<<<g2, bx, 0, st>>>(m, geo_of<float>(d->geom), (const float *)rt, (const float *)mpx,
+        (const float *)mmx, (const float *)mpy, (const float *)mmy, (float *)F.rho, (float *)F.vx, (float *)F.vy,
+        (const float *)F.rho0, (const float *)F.vx0, (const float *)F.vy0, d->ramps, d->stockholm, d->scal_dev);
+    return (int)cudaGetLastError();
+  }
   dim3 grid((m.nx + bx - 1) / bx, m.ny, m.is3d ? m.nz : 1);
   k_newvel<T, S><<<grid, bx, 0, st>>>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, (S *)F.rho, (S *)F.vx, (S *)F.vy,
                                    (S *)F.vz, (const S *)F.rho0, (const S *)F.vx0, (const S *)F.vy0,

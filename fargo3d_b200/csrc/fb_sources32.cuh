@@ -195,12 +195,79 @@ __device__ __forceinline__ void b_sources_cyl32(const Dims m, const Geo<float> g
   }
 }
 
+// ---------------------------------------------------------------------------
+// NewVelocity_x/y (newvel_x.c:81, newvel_y.c:70) and StockholmBoundary
+// (stockholm.c:129-185) of FP32 2D disks.  A lane owns a column and marches
+// over NV32_R rows: row j-1's transported density and upper-face radial
+// momentum, which newvel_y reads for row j, are the previous iteration's own
+// loads; the column i-1 values newvel_x reads come from the adjacent lane
+// (lane 0 loads them).  The azimuthal spacing is uniform, so Sxi cancels from
+// the x average; the momenta are relative to the frame and the ring
+// background, and the velocity they give is the stored (relative) vx.  Each
+// component is one correctly rounded division (see b_newvel).
+constexpr int NV32_R = 8;
+
+__device__ __forceinline__ void b_newvel_cyl32(const Dims m, const Geo<float> g, const float *__restrict__ rt,
+    const float *__restrict__ mpx, const float *__restrict__ mmx, const float *__restrict__ mpy,
+    const float *__restrict__ mmy, float *__restrict__ rho, float *__restrict__ vx, float *__restrict__ vy,
+    const float *__restrict__ rho0, const float *__restrict__ vx0, const float *__restrict__ vy0,
+    const double *__restrict__ ramps, int stockholm, const fb_scalars *__restrict__ sc, uint3 bid) {
+  const int lane = threadIdx.x & 31;
+  const int i = (int)bid.x * blockDim.x + threadIdx.x;
+  const int j0 = FB_NGH + (int)bid.y * NV32_R, j1 = min(j0 + NV32_R, m.ny + FB_NGH);
+  const bool act = i < m.nx;
+  const int im = i > 0 ? i - 1 : m.nx - 1;
+  const int ic = act ? i : m.nx - 1;   // lanes past the ring load a valid cell and write nothing
+  const float dt = (float)sc->dt, dof = (float)(sc->omegaframe - sc->omegaframe0);
+  // row j0 - 1: its density and upper-face radial momentum
+  float r_m = rt[m.l(ic, j0 - 1, 0)], mpy_m = mpy[m.l(ic, j0 - 1, 0)];
+  for (int j = j0; j < j1; j++) {
+    const long long l = m.l(ic, j, 0);
+    const float r = rt[l], mm_x = mmx[l], mp_x = mpx[l], mm_y = mmy[l], mp_y = mpy[l];
+    float rxm = lane_m(r), mpxm = lane_m(mp_x);
+    if (lane == 0 || i == 0) {   // column i-1 outside this warp (or the wrap)
+      const long long lxm = m.l(im, j, 0);
+      rxm = rt[lxm];
+      mpxm = mpx[lxm];
+    }
+    const float ivj = ld(g.invvj + j), ivjm = ld(g.invvj + j - 1), rc = ld(g.ymed + j);
+    float nvx = __fdiv_rn(mm_x + mpxm, (r + rxm) * rc);
+    float nvy = __fdiv_rn(mm_y * ivjm + mpy_m * ivj, r * ivjm + r_m * ivj);
+    float nr = r;
+    if (stockholm) {
+      const float ramp = (float)ramps[j];
+      if (ramp > 0.0f) {
+        const float taud = ld(g.tau_j + j) / ramp;
+        const float vx0t = vx0[j] - dof * rc;
+        nr = (nr * taud + rho0[j] * dt) / (dt + taud);
+        nvx = (nvx * taud + vx0t * dt) / (dt + taud);
+        nvy = (nvy * taud + vy0[j] * dt) / (dt + taud);
+      }
+    }
+    if (act) {
+      rho[l] = nr;
+      vx[l] = nvx;
+      vy[l] = nvy;
+    }
+    r_m = r;
+    mpy_m = mp_y;
+  }
+}
+
 static __global__ void __launch_bounds__(S32_WARPS * 32, FB_S32_MINB) k_sources_cyl32(Dims m, Geo<float> g, Geo<double> gd,
     const float *__restrict__ rho, const float *__restrict__ cs, const float *__restrict__ vx,
     const float *__restrict__ vy, float *__restrict__ vxt, float *__restrict__ vyt,
     const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg,
     const float *__restrict__ shear_bg) {
   b_sources_cyl32(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, vbg, shear_bg, blockIdx);
+}
+
+static __global__ void __launch_bounds__(128) k_newvel_cyl32(Dims m, Geo<float> g, const float *__restrict__ rt,
+    const float *__restrict__ mpx, const float *__restrict__ mmx, const float *__restrict__ mpy,
+    const float *__restrict__ mmy, float *__restrict__ rho, float *__restrict__ vx, float *__restrict__ vy,
+    const float *__restrict__ rho0, const float *__restrict__ vx0, const float *__restrict__ vy0,
+    const double *__restrict__ ramps, int stockholm, const fb_scalars *__restrict__ scp) {
+  b_newvel_cyl32(m, g, rt, mpx, mmx, mpy, mmy, rho, vx, vy, rho0, vx0, vy0, ramps, stockholm, scp, blockIdx);
 }
 
 }  // namespace fb
