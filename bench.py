@@ -560,6 +560,25 @@ def cpu_steps_for(cfgs, steps, cores):
     return max(1, min(steps, cap))
 
 
+def print_plan(args, rank: int, world: int):
+    """Each rank's share of the workload, gathered on rank 0 over the same
+    rank set-up as a run (gloo: it needs no GPU)."""
+    cfgs, wname = workload(args.workload, rank, world)
+    mine = {"rank": rank, "disks": len(cfgs), "cells": sum(c.active_cells for c in cfgs),
+            "seeds": [c.seed for c in cfgs]}
+    allp = [mine]
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        tdist.init_process_group("gloo", timeout=timedelta(seconds=60))
+        allp = [None] * world
+        tdist.all_gather_object(allp, mine)
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"plan": True, "n_gpus": world, "workload": wname, "ranks": allp}), flush=True)
+
+
 def relaunch_with_ranks(n: int) -> int:
     """`--gpus N` outside torchrun: start N ranks of this same command."""
     import socket
@@ -587,6 +606,8 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 error leg of the default run")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg (profiling runs)")
+    ap.add_argument("--plan", action="store_true",
+                    help="print every rank's share of the workload and exit (no GPU work; gloo when N > 1)")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         sys.exit(relaunch_with_ranks(args.gpus))
@@ -596,6 +617,9 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.plan:
+        print_plan(args, rank, world)
+        return
     if args.impl == "reference":
         if rank != 0:
             return

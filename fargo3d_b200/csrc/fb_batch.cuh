@@ -112,6 +112,14 @@ __global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 
   cfl_commit(mn, dtmin);
 }
 
+// FP32 2D: 128 columns x CFL32_R rows a tile (fb_sources32.cuh)
+static __global__ void __launch_bounds__(128) kb_cfl_cyl32(const fb_disk_dev *ds, const int4 *items, int f) {
+  FB_TILE
+  b_cfl_cyl32(dims_of(D), geo_of<float>(D.geom), (const float *)F.rho, (const float *)F.cs, (const float *)F.vx,
+              (const float *)F.vy, F.vxmed, F.vbg, (float)scp->nu, (float)scp->alpha, D.cfl, D.mindx,
+              (unsigned long long *)D.dtmin, bid);
+}
+
 template <typename T, typename S>
 __global__ void __launch_bounds__(SRC2_TX *SRC2_TY, sizeof(S) == 4 ? FB_SRC_MINB : 1) kb_sources_cyl(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
@@ -172,7 +180,11 @@ __global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? FB_COL_MINB32 : 1) kb
     src.q[3] = (const S *)F.mmy; src.q[4] = (const S *)F.mpz; src.q[5] = (const S *)F.mmz;
     src.from_v = 0;
   }
-  if (!m.is3d) {
+  if (!m.is3d && sizeof(S) == 4 && sizeof(T) == 4) {   // FP32 2D (fb_sources32.cuh)
+    b_sweep_col32<COL_NS>(m, geo_of<float>(D.geom), (const float *)F.rho, (const float *)F.vxt, (const float *)F.vyt,
+                          (const float *)F.dlb_y, ylo, yhi, (float *)F.rho_a, (float *)F.mpx, (float *)F.mmx,
+                          (float *)F.mpy, (float *)F.mmy, scp, bid);
+  } else if (!m.is3d) {
     b_sweep_col<T, 0, COL_NS, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), src, 4, ylo, yhi, 0, (S *)F.rho_a, (S *)F.mpx, (S *)F.mmx,
                               (S *)F.mpy, (S *)F.mmy, nullptr, nullptr, scp, bid);
   } else if (DIR == 1) {
@@ -287,7 +299,10 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
     dim3 g(1, 1, 1);
     switch (st) {
       case ST_ROWSUM: g = dim3(B->precision == FB_FP64 ? (sy * sz + 31) / 32 : (sy * sz + 7) / 8); break;
-      case ST_CFL: g = dim3((ny + CFL_R - 1) / CFL_R, D.is3d ? nz : 1); break;
+      case ST_CFL:
+        if (!D.is3d && B->precision == FB_FP32) g = dim3((nx + 127) / 128, (ny + CFL32_R - 1) / CFL32_R);
+        else g = dim3((ny + CFL_R - 1) / CFL_R, D.is3d ? nz : 1);
+        break;
       case ST_SOURCES:
         if (D.is3d) g = dim3((nx + SRC3_TX - 1) / SRC3_TX, (ny + SRC3_TY - 1) / SRC3_TY, nz);
         else if (B->precision == FB_FP32) g = dim3((nx + S32_COLS - 1) / S32_COLS, (ny + S32_NS - 1) / S32_NS);
@@ -374,7 +389,10 @@ static int launch_step(fb_batch *B, double DT) {
     else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
   }
   pmark(st, "rowsum");
-  for (int f = 0; f < nf; f++) kb_cfl<TF, S><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
+  for (int f = 0; f < nf; f++) {
+    if (!B->is3d && sizeof(S) == 4) kb_cfl_cyl32<<<grid(ST_CFL), 128, 0, st>>>(ds, B->items[ST_CFL], f);
+    else kb_cfl<TF, S><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
+  }
   pmark(st, "cfl");
   kb_scalars<<<(B->n + 63) / 64, 64, 0, st>>>(ds, B->d_psys, B->n, DT);
   pmark(st, "scalars");

@@ -1320,6 +1320,45 @@ __device__ __forceinline__ void chunk_iface32(const float *w, const float *v, fl
   }
 }
 
+// The PPA interfaces of an FP32 ring, whose fractional velocity vf is one
+// value for the whole ring (compute_residual.c:68-73 with uniform spacing):
+// every face has the same upwind side, so the raw interface values
+// (fargo_ppa_b: a + (a+ - a)/2 - (s+ - s)/6, shared by a cell's right and its
+// neighbour's left edge) are formed once per face, the monotonised edges
+// (fargo_ppa_c) once per upwind cell, and the Courant number xi = |vf| dt / z
+// once per ring (fargo_ppa_d).
+template <int C, int D>
+__device__ __forceinline__ void ppa_uniform32_dir(const float *w, float ksi, float *qs) {
+  float sl[C + 4];                          // MC slopes of window cells 1 .. C+4
+#pragma unroll
+  for (int u = 0; u < C + 4; u++) sl[u] = mc_slope(w[u], w[u + 1], w[u + 2]);
+  float e[C + 3];                           // raw edge between window cells k and k+1, k = 1 .. C+3
+#pragma unroll
+  for (int k = 1; k < C + 4; k++)
+    e[k - 1] = w[k] + 0.5f * (w[k + 1] - w[k]) - (1.0f / 6.0f) * (sl[k] - sl[k - 1]);
+  const float kk = ksi * (1.0f - ksi);
+#pragma unroll
+  for (int f = 0; f <= C; f++) {
+    constexpr int d = D;
+    const int k = f + 2 + d;                // upwind window cell of face f
+    const float a0 = w[k];
+    float L = e[k - 2], R = e[k - 1];       // edges k-1|k and k|k+1
+    if ((R - a0) * (a0 - L) < 0.0f) { L = a0; R = a0; }
+    const float diff = R - L;
+    const float cord = a0 - 0.5f * (L + R);
+    if (6.0f * diff * cord > diff * diff) L = 3.0f * a0 - 2.0f * R;
+    if (-diff * diff > 6.0f * diff * cord) R = 3.0f * a0 - 2.0f * L;
+    const float edge = d ? L : R;
+    qs[f] = edge + ksi * (a0 - edge) + kk * (2.0f * a0 - R - L);
+  }
+}
+template <int C>
+__device__ __forceinline__ void chunk_ppa_uniform32(const float *w, float vf, float dtz, float *qs) {
+  const float ksi = fabsf(vf) * dtz;
+  if (vf > 0.0f) ppa_uniform32_dir<C, 0>(w, ksi, qs);   // upwind: the cell before each face
+  else ppa_uniform32_dir<C, 1>(w, ksi, qs);             // the cell after it
+}
+
 template <typename T, int C, int NT, typename S = T>
 __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const Geo<double> &gd, int nq, int jlo,
                                            int klo, int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,
@@ -1495,7 +1534,8 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
       // FP32: one reciprocal of each window density, shared by the momenta
       T irw[C + 6];
       if constexpr (sizeof(T) == 4) {
-        chunk_iface32<C>((const float *)wr, (const float *)v, (float)(dt / zring), pass == 1, (float *)rs);
+        if (pass == 1) chunk_ppa_uniform32<C>((const float *)wr, (float)v[0], (float)(dt / zring), (float *)rs);
+        else chunk_iface32<C>((const float *)wr, (const float *)v, (float)(dt / zring), false, (float *)rs);
 #pragma unroll
         for (int u = 0; u < C + 6; u++) irw[u] = (T)1.0 / wr[u];
       } else {
@@ -1508,7 +1548,8 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
         if constexpr (sizeof(T) == 4) {
 #pragma unroll
           for (int u = 0; u < C + 6; u++) wq[u] = raw[u] * irw[u];  // DivideByRho
-          chunk_iface32<C>((const float *)wq, (const float *)v, (float)(dt / zring), pass == 1, (float *)qs);
+          if (pass == 1) chunk_ppa_uniform32<C>((const float *)wq, (float)v[0], (float)(dt / zring), (float *)qs);
+          else chunk_iface32<C>((const float *)wq, (const float *)v, (float)(dt / zring), false, (float *)qs);
         } else {
 #pragma unroll
           for (int u = 0; u < C + 6; u++) wq[u] = raw[u] / wr[u];  // DivideByRho

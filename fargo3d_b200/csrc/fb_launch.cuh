@@ -109,6 +109,13 @@ static int launch_sweep_cols_n(const fb_disk_dev *d, int f, cudaStream_t st) {
   S *q[6];
   int nq;
   (void)gd;
+  if (!m.is3d && sizeof(S) == 4 && sizeof(T) == 4) {   // FP32 2D (fb_sources32.cuh)
+    dim3 grid((m.nx + bx - 1) / bx, 1, (yhi - ylo + NS) / NS);
+    k_sweep_col32<NS><<<grid, bx, 0, st>>>(m, geo_of<float>(d->geom), (const float *)F.rho, (const float *)F.vxt,
+        (const float *)F.vyt, (const float *)F.dlb_y, ylo, yhi, (float *)F.rho_a, (float *)F.mpx, (float *)F.mmx,
+        (float *)F.mpy, (float *)F.mmy, d->scal_dev);
+    return (int)cudaGetLastError();
+  }
   if (!m.is3d) {
     nq = 4;
     QSrc<T, S> src = qsrc_from_v<T, S>(F, (T)0);

@@ -46,23 +46,42 @@ struct Cell32 {
 __device__ __forceinline__ float lane_m(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }    // column i-1
 __device__ __forceinline__ float lane_p(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }  // column i+1
 
-// planets' potential (potential.c:51-208 without the star's term), FP32
-__device__ __forceinline__ float pot_planets32(const fb_scalars *__restrict__ sc, float XC, float YC) {
-  float pot = 0.0f;
+// The planets of one step in FP32, formed once per CTA: position, mass,
+// smoothing^2 + z^2 and the indirect-term factor m / d^3 (0 without it).
+struct Planet32 {
+  float x, y, m, s2z, ind;
+};
+__device__ __forceinline__ int planets32_load(const fb_scalars *__restrict__ sc, Planet32 *sp) {
   const int np = sc->nplanets;
+  if ((int)threadIdx.x < np) {
+    const int n = threadIdx.x;
+    Planet32 p;
+    p.x = (float)sc->px[n];
+    p.y = (float)sc->py[n];
+    p.m = (float)sc->pmass[n];
+    p.s2z = (float)(sc->psmooth2[n] + sc->pz[n] * sc->pz[n]);
+    p.ind = sc->indirect_term ? (float)(sc->pmass[n] / sc->pdist3[n]) : 0.0f;
+    sp[n] = p;
+  }
+  __syncthreads();
+  return np;
+}
+
+// planets' potential (potential.c:51-208 without the star's term), FP32
+__device__ __forceinline__ float pot_planets32(const Planet32 *sp, int np, float XC, float YC) {
+  float pot = 0.0f;
   for (int n = 0; n < np; n++) {
-    const float xp = (float)sc->px[n], yp = (float)sc->py[n], zp = (float)sc->pz[n];
-    const float dx = XC - xp, dy = YC - yp;
-    const float dist = dx * dx + dy * dy + zp * zp;
-    if (sc->indirect_term) pot += (float)(sc->pmass[n] / sc->pdist3[n]) * (XC * xp + YC * yp);
-    pot -= (float)sc->pmass[n] * rsqrtf(dist + (float)sc->psmooth2[n]);
+    const Planet32 p = sp[n];
+    const float dx = XC - p.x, dy = YC - p.y;
+    pot += p.ind * (XC * p.x + YC * p.y);
+    pot -= p.m * rsqrtf(dx * dx + dy * dy + p.s2z);
   }
   return pot;
 }
 
 __device__ __forceinline__ Cell32 load_cell32(const Dims &m, const Geo<float> &g, const float *__restrict__ rho,
                                               const float *__restrict__ cs, const float *__restrict__ vx,
-                                              const float *__restrict__ vy, const fb_scalars *__restrict__ sc,
+                                              const float *__restrict__ vy, const Planet32 *sp, int np,
                                               float domega, int i, int j) {
   const long long l = m.l(i, j, 0);
   Cell32 o;
@@ -72,7 +91,7 @@ __device__ __forceinline__ Cell32 load_cell32(const Dims &m, const Geo<float> &g
   o.u = vx[l] - domega * ym;     // CorrectVtheta (correct_vtheta.c:55-60)
   o.vy = vy[l];
   o.p = o.r * o.c * o.c;         // ComputePressureFieldIso
-  o.pot = pot_planets32(sc, ym * ld(g.cos_xmed + i), ym * ld(g.sin_xmed + i));
+  o.pot = pot_planets32(sp, np, ym * ld(g.cos_xmed + i), ym * ld(g.sin_xmed + i));
   return o;
 }
 
@@ -113,6 +132,8 @@ __device__ __forceinline__ void b_sources_cyl32(const Dims m, const Geo<float> g
     const float *__restrict__ vy, float *__restrict__ vxt, float *__restrict__ vyt,
     const fb_scalars *__restrict__ sc, int dust, int viscous, const double *__restrict__ vbg,
     const float *__restrict__ shear_bg, uint3 bid) {
+  __shared__ Planet32 s_pl[FB_MAXPLANETS];
+  const int np = planets32_load(sc, s_pl);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int iu = (int)(bid.x * S32_WARPS + w) * S32_OUT - 1 + lane;   // unwrapped column of this lane
   const int i = ((iu % m.nx) + m.nx) % m.nx;
@@ -124,15 +145,15 @@ __device__ __forceinline__ void b_sources_cyl32(const Dims m, const Geo<float> g
   const float sxi0 = ld(g.sxi + 0), idx0 = ld(g.invdiffxmed + 0);
   const float c2 = (float)FB_CVNR;
   // rows j0 - 1 and j0; the stresses of row j0 - 1 and the corner of row j0
-  Cell32 A = load_cell32(m, g, rho, cs, vx, vy, sc, domega, i, j0 - 1);
-  Cell32 C0 = load_cell32(m, g, rho, cs, vx, vy, sc, domega, i, j0);
+  Cell32 A = load_cell32(m, g, rho, cs, vx, vy, s_pl, np, domega, i, j0 - 1);
+  Cell32 C0 = load_cell32(m, g, rho, cs, vx, vy, s_pl, np, domega, i, j0);
   float txx_m = 0.f, tyy_m = 0.f, tyx_c = 0.f;
   if (viscous) {
     stress_diag32(g, A, C0.vy, m.alpha, nu, alpha, sxi0, j0 - 1, txx_m, tyy_m);
     tyx_c = stress_rphi32(g, C0, A, m.alpha, nu, alpha, ld(shear_bg + j0), j0);
   }
   for (int j = j0; j < j1; j++) {
-    const Cell32 P = load_cell32(m, g, rho, cs, vx, vy, sc, domega, i, j + 1);
+    const Cell32 P = load_cell32(m, g, rho, cs, vx, vy, s_pl, np, domega, i, j + 1);
     float txx_c = 0.f, tyy_c = 0.f, tyx_p = 0.f;
     if (viscous) {
       stress_diag32(g, C0, P.vy, m.alpha, nu, alpha, sxi0, j, txx_c, tyy_c);
@@ -268,6 +289,189 @@ static __global__ void __launch_bounds__(128) k_newvel_cyl32(Dims m, Geo<float> 
     const float *__restrict__ rho0, const float *__restrict__ vx0, const float *__restrict__ vy0,
     const double *__restrict__ ramps, int stockholm, const fb_scalars *__restrict__ scp) {
   b_newvel_cyl32(m, g, rt, mpx, mmx, mpy, mmy, rho, vx, vy, rho0, vx0, vy0, ramps, stockholm, scp, blockIdx);
+}
+
+// ---------------------------------------------------------------------------
+// The radial sweep of FP32 2D disks (TransportY, transport.c:24-46, for the
+// density and the four momenta; vanleer_y_a/_b, divrho, update_y,
+// update_density_y): b_sweep_col's work with every per-row factor formed once
+// per thread -- the zone sizes and their reciprocals, the face areas and the
+// cell updates for the uniform azimuthal spacing -- and the specific momenta
+// taken directly as v R or v (DivideByRho of rho v R is v R), so the only
+// division per cell and quantity is the limiter's harmonic mean.  Table
+// indices are clamped like the field rows (cells past chi + 2 never reach an
+// output).  The azimuthal momenta are frame- and background-relative as in
+// b_sweep_col.
+template <int NS>
+__device__ __forceinline__ void b_sweep_col32(const Dims m, const Geo<float> g, const float *__restrict__ rho,
+    const float *__restrict__ vxt, const float *__restrict__ vyt, const float *__restrict__ dlb, int clo, int chi,
+    float *__restrict__ rho_out, float *__restrict__ o_mpx, float *__restrict__ o_mmx, float *__restrict__ o_mpy,
+    float *__restrict__ o_mmy, const fb_scalars *__restrict__ scp, uint3 bid) {
+  const int i = (int)bid.x * blockDim.x + threadIdx.x;
+  if (i >= m.nx) return;
+  const int c0 = clo + (int)bid.z * NS;
+  if (c0 > chi) return;
+  const float dt = (float)scp->dt, of = (float)scp->omegaframe;
+  const int cmax = chi + 2;
+  const int ixp = i < m.nx - 1 ? i + 1 : 0;
+  const float sxi0 = ld(g.sxi + 0), isxi0 = 1.0f / sxi0;
+  float r[NS + 4], izn[NS + 4], vel[NS + 1];
+  // zone_size_y = Ymin(j+1) - Ymin(j) of window cell w (a broadcast table load)
+  auto zn = [&](int w) -> float { return ld(g.sxj + min(c0 - 2 + w, cmax)); };
+#pragma unroll
+  for (int w = 0; w < NS + 4; w++) {
+    r[w] = rho[m.l(i, min(c0 - 2 + w, cmax), 0)];
+    izn[w] = 1.0f / zn(w);
+  }
+#pragma unroll
+  for (int f = 0; f < NS + 1; f++) vel[f] = vyt[m.l(i, min(c0 + f, cmax - 1), 0)];
+  // van Leer interface values of a window a[] (cells c0-2 .. c0+NS+1) at the
+  // faces c0 .. c0+NS; off[] (when given) are the neighbour differences of
+  // the offset the window leaves out
+  auto iface = [&](const float *a, const float *off, float *qs) {
+    float slope[NS + 2];
+#pragma unroll
+    for (int s2 = 0; s2 < NS + 2; s2++) {
+      float dqm = a[s2 + 1] - a[s2], dqp = a[s2 + 2] - a[s2 + 1];
+      if (off) { dqm += off[s2]; dqp += off[s2 + 1]; }
+      dqm *= izn[s2 + 1];
+      dqp *= izn[s2 + 2];
+      slope[s2] = (dqp * dqm <= 0.0f) ? 0.0f : 2.0f * dqp * dqm / (dqm + dqp);
+    }
+#pragma unroll
+    for (int f = 0; f < NS + 1; f++) {
+      if (vel[f] > 0.0f) qs[f] = a[f + 1] + 0.5f * (zn(f + 1) - vel[f] * dt) * slope[f];
+      else qs[f] = a[f + 2] - 0.5f * (zn(f + 2) + vel[f] * dt) * slope[f + 1];
+    }
+  };
+  // face area factor (Surf_y over v rho*) at face c0 + f, and the cell
+  // update dt / Vol at cell c0 + u (broadcast table loads)
+  auto sf = [&](int f) -> float { return ld(g.syj + min(c0 + f, cmax)) * sxi0; };
+  auto fin = [&](int u) -> float { return dt * ld(g.invvj + min(c0 + u, cmax)) * isxi0; };
+  float rs[NS + 1];
+  iface(r, nullptr, rs);
+  // OMEGAFRAME (R^2(c) - R^2(c-1)) + (vbg R)(c) - (vbg R)(c-1)
+  auto dr2 = [&](int c) -> float { return of * ld(g.dr2_j + c) + (dlb ? ld(dlb + c) : 0.0f); };
+  float off[NS + 3];
+#pragma unroll
+  for (int w = 0; w < NS + 3; w++) {
+    const int c = c0 - 1 + w;
+    off[w] = c <= cmax ? dr2(c) : 0.0f;
+  }
+  float *qo[4] = {o_mpx, o_mmx, o_mpy, o_mmy};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    float a[NS + 4], qs[NS + 1];
+#pragma unroll
+    for (int w = 0; w < NS + 4; w++) {
+      const int c = min(c0 - 2 + w, cmax);
+      const long long l = m.l(i, c, 0);
+      // momenta_x.c:76-85 (relative), momenta_y.c:65-66, over rho
+      if (q == 0) a[w] = vxt[m.l(ixp, c, 0)] * ld(g.ymed + c);
+      else if (q == 1) a[w] = vxt[l] * ld(g.ymed + c);
+      else if (q == 2) a[w] = vyt[l + m.pitch];
+      else a[w] = vyt[l];
+    }
+    iface(a, q < 2 ? off : nullptr, qs);
+#pragma unroll
+    for (int u = 0; u < NS; u++) {
+      const int c = c0 + u;
+      if (c <= chi) {
+        float qin = qs[u], qout = qs[u + 1];
+        if (q < 2) {
+          if (vel[u] > 0.0f) qin -= off[u + 1];            // upwind cell c-1
+          if (!(vel[u + 1] > 0.0f)) qout += off[u + 2];    // upwind cell c+1
+        }
+        const float flux = vel[u] * qin * rs[u] * sf(u) - vel[u + 1] * qout * rs[u + 1] * sf(u + 1);
+        qo[q][m.l(i, c, 0)] = a[u + 2] * r[u + 2] + flux * fin(u);
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < NS; u++) {
+    const int c = c0 + u;
+    if (c <= chi) {
+      const float flux = vel[u] * rs[u] * sf(u) - vel[u + 1] * rs[u + 1] * sf(u + 1);
+      rho_out[m.l(i, c, 0)] = r[u + 2] + flux * fin(u);
+    }
+  }
+}
+
+template <int NS>
+static __global__ void __launch_bounds__(128, 4) k_sweep_col32(Dims m, Geo<float> g, const float *__restrict__ rho,
+    const float *__restrict__ vxt, const float *__restrict__ vyt, const float *__restrict__ dlb, int clo, int chi,
+    float *__restrict__ rho_out, float *__restrict__ o_mpx, float *__restrict__ o_mmx, float *__restrict__ o_mpy,
+    float *__restrict__ o_mmy, const fb_scalars *__restrict__ scp) {
+  b_sweep_col32<NS>(m, g, rho, vxt, vyt, dlb, clo, chi, rho_out, o_mpx, o_mmx, o_mpy, o_mmy, scp, blockIdx);
+}
+
+// ---------------------------------------------------------------------------
+// CFL time step of FP32 2D disks (cfl.c:135-258, cfl_b.c:14-39): the limits
+// of cfl_cell32 for a tile of 128 columns x CFL32_R rows, a lane per column
+// marching over the rows with every load of the tile issued up front (the
+// kernel is a stream of four fields; it is bound by how many loads are in
+// flight), the x neighbour's vx by shuffle, the next row's vy reused.  The
+// tile's minimum (with the shear limits of its rows) is folded into the
+// disk's as in b_cfl; non-finite limits and non-positive densities set the
+// disk's flag word.
+constexpr int CFL32_R = 8;
+
+__device__ __forceinline__ void b_cfl_cyl32(const Dims m, const Geo<float> g, const float *__restrict__ rho,
+    const float *__restrict__ cs, const float *__restrict__ vx, const float *__restrict__ vy,
+    const double *__restrict__ vxmed, const double *__restrict__ vbg, float nu, float alpha, double cfl_num,
+    double mindx, unsigned long long *__restrict__ dtmin, uint3 bid) {
+  const int lane = threadIdx.x & 31;
+  const int i = (int)bid.x * blockDim.x + threadIdx.x;
+  const int j0 = FB_NGH + (int)bid.y * CFL32_R;
+  const int nr = min(CFL32_R, m.ny + FB_NGH - j0);
+  const bool act = i < m.nx;
+  const int ic = act ? i : m.nx - 1;
+  const int ixp = ic < m.nx - 1 ? ic + 1 : 0;
+  float r[CFL32_R], c[CFL32_R], u[CFL32_R], v[CFL32_R + 1], uxp_edge[CFL32_R];
+#pragma unroll
+  for (int q = 0; q < CFL32_R; q++) {
+    const int j = j0 + min(q, nr - 1);
+    const long long l = m.l(ic, j, 0);
+    r[q] = rho[l];
+    c[q] = cs[l];
+    u[q] = vx[l];
+    v[q] = vy[l];
+    uxp_edge[q] = (lane == 31 || ic == m.nx - 1) ? vx[m.l(ixp, j, 0)] : 0.0f;
+  }
+  v[CFL32_R] = vy[m.l(ic, j0 + nr, 0)];
+  const float cflf = (float)cfl_num;
+  const float izx0 = ld(g.invdiffxmed + 0);
+  float mn = 1e20f;
+  bool bad = false;
+#pragma unroll
+  for (int q = 0; q < CFL32_R; q++) {
+    const int j = j0 + min(q, nr - 1);
+    float uxp = lane_p(u[q]);
+    if (lane == 31 || ic == m.nx - 1) uxp = uxp_edge[q];
+    const float vyp = q + 1 < nr ? v[q + 1] : v[CFL32_R];
+    const float vmf = (float)(vxmed[j] - bg_at(vbg, j));
+    const float izx = izx0 * ld(g.inv_ymed + j), izy = 1.0f / ld(g.sxj + j);
+    const float visc = m.alpha ? alpha * c[q] * c[q] * ld(g.visc_j + j) : nu;
+    const float mx7 = fmaxf(izx, izy);
+    const float c1 = fabsf(c[q]) * mx7;
+    const float c2 = fmaxf(fabsf(u[q] - vmf), fabsf(uxp - vmf)) * izx;
+    const float c3 = fmaxf(fabsf(v[q]), fabsf(vyp)) * izy;
+    const float c5 = fmaxf(fabsf(uxp - u[q]) * izx, fabsf(vyp - v[q]) * izy) * (4.0f * (float)FB_CVNR);
+    const float c7 = 4.0f * visc * (mx7 * mx7);
+    const float dtc = cflf * rsqrtf(c1 * c1 + c2 * c2 + c3 * c3 + c5 * c5 + c7 * c7);
+    if (act && q < nr) {
+      bad |= !(dtc == dtc) || !(r[q] > 0.0f);
+      mn = fminf(mn, dtc);
+    }
+  }
+  double mnd = (double)mn;
+  if ((int)threadIdx.x < nr) {   // the shear limits of the tile's rows (a MIN: repeats are harmless)
+    const int j = j0 + threadIdx.x;
+    const double shear = cfl_shear(g, vxmed, cfl_num, mindx, j, j);
+    if (shear < mnd) mnd = shear;
+  }
+  if (bad) atomicOr(dtmin + 1, 1ull);
+  cfl_commit(mnd, dtmin);
 }
 
 }  // namespace fb

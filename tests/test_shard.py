@@ -65,3 +65,29 @@ def test_shards_over_two_gloo_ranks():
     total = sum(r[2] for r in res)
     assert all(r[3] == total for r in res)                               # SUM seen by both
     assert all(r[4] == 2.0 for r in res)                                 # MAX over ranks
+
+
+def test_bench_gpus_2_shards_one_global_list():
+    """`bench.py --gpus 2` starts two ranks itself (torch.distributed.run on
+    127.0.0.1), each takes its LPT share of one global list of 128 disks, and
+    rank 0 reports n_gpus = 2 (--plan: the rank set-up without GPU work)."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(k, None)
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--plan"],
+                         capture_output=True, text=True, timeout=300, env=env, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = [l for l in out.stdout.splitlines() if l.startswith("{")][-1]
+    plan = json.loads(line)
+    assert plan["n_gpus"] == 2 and len(plan["ranks"]) == 2
+    seeds = sorted(s for r in plan["ranks"] for s in r["seeds"])
+    assert seeds == list(range(128))
+    from fargo3d_b200 import config_batched
+    total = sum(c.active_cells for c in config_batched(128, seed=0))
+    loads = [r["cells"] for r in plan["ranks"]]
+    assert sum(loads) == total
+    assert max(loads) <= total / 2 + max(c.active_cells for c in config_batched(128, seed=0))
