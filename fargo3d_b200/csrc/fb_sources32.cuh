@@ -240,33 +240,53 @@ __device__ __forceinline__ void b_newvel_cyl32(const Dims m, const Geo<float> g,
   const int im = i > 0 ? i - 1 : m.nx - 1;
   const int ic = act ? i : m.nx - 1;   // lanes past the ring load a valid cell and write nothing
   const float dt = (float)sc->dt, dof = (float)(sc->omegaframe - sc->omegaframe0);
+  // every load of the tile first (rows past j1 repeat the last row and are
+  // not written): the kernel is bound by the loads in flight
+  const int nr = j1 - j0;
+  const bool edge = lane == 0 || i == 0;   // column i-1 outside this warp (or the wrap)
+  float a_r[NV32_R], a_mmx[NV32_R], a_mpx[NV32_R], a_mmy[NV32_R], a_mpy[NV32_R], e_r[NV32_R], e_mpx[NV32_R];
+#pragma unroll
+  for (int q = 0; q < NV32_R; q++) {
+    const int j = j0 + min(q, nr - 1);
+    const long long l = m.l(ic, j, 0);
+    a_r[q] = rt[l]; a_mmx[q] = mmx[l]; a_mpx[q] = mpx[l]; a_mmy[q] = mmy[l]; a_mpy[q] = mpy[l];
+    if (edge) {
+      const long long lxm = m.l(im, j, 0);
+      e_r[q] = rt[lxm];
+      e_mpx[q] = mpx[lxm];
+    } else {
+      e_r[q] = 0.0f;
+      e_mpx[q] = 0.0f;
+    }
+  }
   // row j0 - 1: its density and upper-face radial momentum
   float r_m = rt[m.l(ic, j0 - 1, 0)], mpy_m = mpy[m.l(ic, j0 - 1, 0)];
-  for (int j = j0; j < j1; j++) {
+#pragma unroll
+  for (int q = 0; q < NV32_R; q++) {
+    const int j = j0 + min(q, nr - 1);
     const long long l = m.l(ic, j, 0);
-    const float r = rt[l], mm_x = mmx[l], mp_x = mpx[l], mm_y = mmy[l], mp_y = mpy[l];
+    const float r = a_r[q], mm_x = a_mmx[q], mp_x = a_mpx[q], mm_y = a_mmy[q], mp_y = a_mpy[q];
     float rxm = lane_m(r), mpxm = lane_m(mp_x);
-    if (lane == 0 || i == 0) {   // column i-1 outside this warp (or the wrap)
-      const long long lxm = m.l(im, j, 0);
-      rxm = rt[lxm];
-      mpxm = mpx[lxm];
+    if (edge) {
+      rxm = e_r[q];
+      mpxm = e_mpx[q];
     }
     const float ivj = ld(g.invvj + j), ivjm = ld(g.invvj + j - 1), rc = ld(g.ymed + j);
     float nvx = __fdiv_rn(mm_x + mpxm, (r + rxm) * rc);
     float nvy = __fdiv_rn(mm_y * ivjm + mpy_m * ivj, r * ivjm + r_m * ivj);
-    float nr = r;
+    float nrho = r;
     if (stockholm) {
       const float ramp = (float)ramps[j];
       if (ramp > 0.0f) {
         const float taud = ld(g.tau_j + j) / ramp;
         const float vx0t = vx0[j] - dof * rc;
-        nr = (nr * taud + rho0[j] * dt) / (dt + taud);
+        nrho = (nrho * taud + rho0[j] * dt) / (dt + taud);
         nvx = (nvx * taud + vx0t * dt) / (dt + taud);
         nvy = (nvy * taud + vy0[j] * dt) / (dt + taud);
       }
     }
-    if (act) {
-      rho[l] = nr;
+    if (act && q < nr) {
+      rho[l] = nrho;
       vx[l] = nvx;
       vy[l] = nvy;
     }
