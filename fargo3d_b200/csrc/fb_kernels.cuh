@@ -1500,8 +1500,16 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
     if (active) {
       T v[C + 1];
       if (pass == 0) {
+        if constexpr (sizeof(T) == 4) {
+          // the residual of FP32 rings in FP32: vm_rel is the small mean of
+          // the background-relative velocity
+          const float vr = (float)vm_rel;
 #pragma unroll
-        for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nxp + P(wrap(c0 + f))] - vm_rel);  // residual
+          for (int f = 0; f <= C; f++) v[f] = svx[sl0 * nxp + P(wrap(c0 + f))] - vr;
+        } else {
+#pragma unroll
+          for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nxp + P(wrap(c0 + f))] - vm_rel);  // residual
+        }
       } else if constexpr (sizeof(T) == 4) {
         // uniform fractional velocity (compute_residual.c:68-73), FP64; the
         // FP32 path's azimuthal spacing is uniform, so it is one value per ring
@@ -1596,6 +1604,26 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
     if (nshift_out) nshift_out[j + k * m.sy] = nsh;
   }
   __syncthreads();
+  if constexpr (sizeof(T) == 4 && sizeof(S) == 4 && C == 4) {
+    // FP32 rings of 4 cells per thread: each thread writes its own cells,
+    // one float4 per field (the ring rows are 16-byte aligned: nx % 4 == 0)
+    if (active) {
+      const int nsh = s_nsh[slot];
+      int it0 = (c0 - nsh) % nx;
+      if (it0 < 0) it0 += nx;
+      int its[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) its[u] = (it0 + u < nx) ? it0 + u : it0 + u - nx;
+      const T *b = bufA + (size_t)slot * nf * nxp;
+      const long long l = m.l(c0, j, k);
+      reinterpret_cast<float4 *>(rho + l)[0] = make_float4(b[its[0]], b[its[1]], b[its[2]], b[its[3]]);
+      for (int q = 0; q < nq; q++) {
+        const T *bq = b + (1 + q) * nxp;
+        reinterpret_cast<float4 *>(qg[q] + l)[0] = make_float4(bq[its[0]], bq[its[1]], bq[its[2]], bq[its[3]]);
+      }
+    }
+    return;
+  }
   for (int e = threadIdx.x; e < rpc * nx; e += NT) {
     const int s = e / nx, i = e - s * nx, rr = bid.x * rpc + s;
     if (rr >= nrings) continue;

@@ -195,6 +195,18 @@ class Disk:
         self._call("get_geometry", _ptr(xa), _ptr(ya), _ptr(za))
         return xa, ya, za
 
+    def write_outputs(self, outdir: str, n: int, fluid: int = 0):
+        """The reference's own output writers ('ref' kinds): fluid's merged
+        <outdir>/<name><field><n>.dat files (WriteMerging) and, for fluid 0,
+        the planet files' next line (WritePlanetSystemFile)."""
+        if self.kind not in ("ref", "ref_o3"):
+            raise NotImplementedError("only the reference-source libraries write FARGO3D outputs")
+        self.lib.ref_write_outputs.restype = C.c_int
+        self.lib.ref_write_outputs.argtypes = [C.c_int, C.c_char_p, C.c_int]
+        rc = self.lib.ref_write_outputs(fluid, outdir.encode(), n)
+        if rc != 0:
+            raise RuntimeError("ref_write_outputs failed: %d" % rc)
+
     def mass(self, fluid: int = 0) -> float:
         if self.kind != "oracle":
             raise NotImplementedError

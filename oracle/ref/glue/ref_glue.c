@@ -514,6 +514,34 @@ void ref_get_scalars(double *o) {
   o[5] = Sys->nb ? Sys->vx[0] : 0; o[6] = Sys->nb ? Sys->vy[0] : 0; o[7] = Domega;
 }
 
+/* output.c is compiled in for its merged writer: the writers it can select
+ * that this build leaves out, and its monitoring hook, are no-ops here. */
+void MakeDir(char *s) { (void)s; }
+void Summary(int n) { (void)n; }
+void WriteVTK(Field *f, int n) { (void)f; (void)n; }
+void WriteVTKMerging(Field *f, int n) { (void)f; (void)n; }
+
+/* Fluid f's output files written by the reference's own writers: the merged
+ * field files <outdir>/<fluid><field><n>.dat (WriteMerging, output.c:283-315)
+ * of dens, energy, vx, vy[, vz], and, with fluid 0, the next line of every
+ * planet<k>.dat (WritePlanetSystemFile, output.c:181-196).  One process:
+ * CPU_Master, no offset (split.c with one rank). */
+int ref_write_outputs(int f, const char *outdir, int n) {
+  if (f < 0 || f >= NFLUIDS) return -1;
+  CPU_Master = YES; CPU_Rank = 0; CPU_Number = 1; Y0 = 0; Z0 = 0;
+  snprintf(OUTPUTDIR, sizeof OUTPUTDIR, "%s/", outdir);
+  WriteMerging(Fluids[f]->Density, n);
+  WriteMerging(Fluids[f]->Energy, n);
+  WriteMerging(Fluids[f]->Vx, n);
+  WriteMerging(Fluids[f]->Vy, n);
+#ifdef Z
+  WriteMerging(Fluids[f]->Vz, n);
+#endif
+  if (f == 0) WritePlanetSystemFile(n, NO);
+  strcpy(OUTPUTDIR, "./");
+  return 0;
+}
+
 void ref_get_geometry(double *xa, double *ya, double *za) {
   if (xa) memcpy(xa, Xmin, sizeof(real) * (Nx + 2 * NGHX + 1));
   if (ya) memcpy(ya, Ymin, sizeof(real) * (Ny + 2 * NGHY + 1));

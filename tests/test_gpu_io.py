@@ -99,3 +99,49 @@ def test_fp32_state_transfer_rounds_like_a_host_cast():
     with pytest.raises(ValueError):
         d.state(out={"rho": np.empty(10)})
     d.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["cyl2d", "sph3d"])
+def test_dat_files_equal_the_references_own_writer(which, tmp_path):
+    """The same initial state advanced 10 FP64 steps by the library and by the
+    reference's own C sources, each written by its own writer: the library's
+    fb_disk_write_dat / fb_disk_write_planets and the reference's WriteMerging
+    (output.c:283-315) / WritePlanetSystemFile (output.c:181-196), compiled
+    from the reference tree into oracle/_ref.  The merged field files are
+    byte-identical, the planet lines too; the library reads the reference's
+    files back into the same state (the restart path)."""
+    import pyoracle
+    from fargo3d_b200 import Disk, config_fargo2d, config_p3disof, initial_state
+    cfg = config_fargo2d(48, 20, seed=91) if which == "cyl2d" else config_p3disof(16, 12, 6, seed=92)
+    init = initial_state(cfg)
+    ours, theirs = tmp_path / "ours", tmp_path / "theirs"
+    ours.mkdir()
+    theirs.mkdir()
+    d = Disk(cfg, "fp64")
+    d.set_state(*init)
+    d.initialize()
+    d.run(10)
+    d.write_dat(str(ours), 3)
+    r = pyoracle.Disk(cfg, "ref")
+    r.set_state(*init)
+    r.initialize()
+    for _ in range(10):
+        r.step()
+    r.write_outputs(str(theirs), 3)
+    names = ["gasdens3.dat", "gasenergy3.dat", "gasvx3.dat", "gasvy3.dat"] + (["gasvz3.dat"] if cfg.is3d else [])
+    for nme in names:
+        a, b = (ours / nme).read_bytes(), (theirs / nme).read_bytes()
+        assert len(a) == 8 * cfg.active_cells and a == b, nme
+    assert (ours / "planet0.dat").read_text() == (theirs / "planet0.dat").read_text()
+    # the restart path: the reference's files into a fresh disk
+    d2 = Disk(cfg, "fp64")
+    d2.set_state(*init)
+    d2.read_dat(str(theirs), 3)
+    got, want = d2.state(), r.state()
+    sl = (slice(3, -3) if cfg.is3d else slice(None), slice(3, -3), slice(None))
+    for k in ("rho", "vx", "vy") + (("vz",) if cfg.is3d else ()):
+        assert np.array_equal(got[k][sl], want[k][sl]), k
+    d2.close()
+    d.close()
+    r.close()
