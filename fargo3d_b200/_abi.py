@@ -35,6 +35,7 @@ class FbParams(C.Structure):
         ("eccentricity", C.c_double), ("inclination", C.c_double),
         ("nfluids", C.c_int), ("invstokes", C.c_double * FB_MAXFLUIDS),
         ("stockholm", C.c_int),
+        ("adiabatic", C.c_int), ("gamma", C.c_double), ("dust_diffusion", C.c_int),
     ]
 
 
@@ -60,6 +61,9 @@ def params_of(cfg) -> FbParams:
     for i, v in enumerate(cfg.invstokes):
         p.invstokes[i] = v
     p.stockholm = int(cfg.stockholm)
+    p.adiabatic = int(cfg.adiabatic)
+    p.gamma = float(cfg.gamma)
+    p.dust_diffusion = int(cfg.dust_diffusion)
     return p
 
 
@@ -90,6 +94,7 @@ def lib():
     L.fb_disk_get_background.argtypes = [C.c_void_p, C.c_int, _D]
     L.fb_disk_set_wait_limit.argtypes = [C.c_void_p, C.c_longlong]
     L.fb_disk_mass.argtypes = [C.c_void_p, C.c_int, _D]
+    L.fb_disk_get_energy.argtypes = [C.c_void_p, C.c_int, _D]
     L.fb_disk_stream.restype = C.c_void_p
     L.fb_disk_stream.argtypes = [C.c_void_p]
     L.fb_params_bytes.argtypes = [C.POINTER(FbParams), C.c_int, C.POINTER(C.c_size_t)]

@@ -124,6 +124,8 @@ int fb_batch_create_slots(int capacity, int precision, int device, int is3d, int
 int fb_batch_add(fb_batch *B, const fb_params *p, double t_end, int *slot) {
   if (!B || !p || !slot) return FB_ERR_ARG;
   if ((p->nz > 1) != (B->is3d != 0) || p->nfluids != B->nfluids) return FB_ERR_ARG;
+  if (p->adiabatic || p->dust_diffusion)   // the batched stages have neither
+    return fb_internal_fail(FB_ERR_ARG, "adiabatic disks and dust diffusion run on the one-disk path (fb_disk_step)", 0);
   for (int n = 0; n < p->nplanets; n++)
     if (p->pl_feeldisk[n])  // the batch's device-side planetary step has no disk force
       return fb_internal_fail(FB_ERR_ARG, "planets that feel the disk run on the one-disk path (fb_disk_step)", 0);

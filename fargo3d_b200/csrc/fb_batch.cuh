@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(SRC2_TX *SRC2_TY, sizeof(S) == 4 ? FB_SRC_MINB
   FB_TILE
   b_sources_cyl<T, SRC2_TX, SRC2_TY, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), (const S *)F.rho,
                                      (const S *)F.cs, (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, scp,
-                                     F.dust, !F.dust, F.vbg, bid);
+                                     F.dust, !F.dust, F.vbg, (S *)nullptr, bid);
 }
 
 // FP32 storage, 2D: FP32 arithmetic, column-marching warps (fb_sources32.cuh)

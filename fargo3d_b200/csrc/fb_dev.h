@@ -52,6 +52,9 @@ typedef struct {
      formed in double, stored in the disk's precision */
   void *shear_bg;
   int has_bg;
+  /* adiabatic disks: the energy after SubStep2_b (et, read by SubStep3) and
+     the transported energy (e_a, copied to the Energy field after transport) */
+  void *et, *e_a;
 } fb_fluid_dev;
 
 /* Per-step scalars (host-computed in FP64 mode, device-computed in the
@@ -78,6 +81,9 @@ typedef struct {
   double cfl, mindx;
   int stockholm;
   double aspectratio, sigmaslope, flaringindex;
+  int adiabatic;          /* ADIABATIC: fl[].cs holds the internal energy */
+  int dust_diffusion;     /* DUSTDIFFUSION of the dust fluids */
+  double gamma;           /* GAMMA */
   fb_geom_dev geom;       /* precision of the disk */
   fb_geom_dev geomd;      /* always double */
   fb_fluid_dev fl[FB_MAXFLUIDS];
@@ -106,6 +112,8 @@ typedef struct {
   int fb_launch_sweep_x_##SUF(const fb_disk_dev *d, int fluid, void *stream);       \
   int fb_launch_newvel_##SUF(const fb_disk_dev *d, int fluid, void *stream);        \
   int fb_launch_collisions_##SUF(const fb_disk_dev *d, void *stream);                 \
+  int fb_launch_substep3_##SUF(const fb_disk_dev *d, int fluid, void *stream);        \
+  int fb_launch_dust_diffusion_##SUF(const fb_disk_dev *d, int fluid, void *stream);  \
   int fb_launch_mass_##SUF(const fb_disk_dev *d, int fluid, double *part, double *out, void *stream); \
   int fb_launch_disk_force_##SUF(const fb_disk_dev *d, double x, double y, double z, double rs, double *ring3, \
                                  double *out3, void *stream);

@@ -401,7 +401,7 @@ int fb_params_bytes(const fb_params *p, int precision, size_t *out) {
   sz = is3d ? (size_t)p->nz + 2 * NG : 1;
   nc = (size_t)p->nx * sy * sz;
   rings = sy * sz;
-  fields = is3d ? 15 + 7 : 11;
+  fields = (is3d ? 15 + 7 : 11) + (p->adiabatic ? 2 : 0);
   b = (size_t)p->nfluids * (fields * nc * esz + 2 * rings * sizeof(double) + rings * sizeof(int) + 4 * rings * esz);
   /* FP32: per-ring azimuthal background and its y / z differences */
   if (precision != FB_FP64) b += (size_t)p->nfluids * rings * (sizeof(double) + 3 * esz);
@@ -432,7 +432,7 @@ int fb_disk_set_tiles(fb_disk *D, int cx, int ns) {
   if (cx != 0) {
     /* whole rings per CTA of 256 threads, two buffers of (1 + nq) fields
      * plus the velocity ring, in the sweep's element size: at most 227 KiB */
-    size_t rpc = 256 / (D->d.nx / cx), nq = D->d.is3d ? 6 : 4;
+    size_t rpc = 256 / (D->d.nx / cx), nq = D->d.is3d ? 6 : (D->d.adiabatic ? 5 : 4);
     size_t nxp = (size_t)D->d.nx + 16 / D->esz; /* padded ring row */
     size_t bytes = rpc * nxp * (2 * (1 + nq) + 1) * D->esz;
     if (bytes > FB_SMEM_MAX)
@@ -504,6 +504,10 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
   if (p->nfluids < 1 || p->nfluids > FB_MAXFLUIDS) return fail(FB_ERR_ARG, "nfluids out of range");
   if (p->frame != FB_FRAME_FIXED && p->nplanets < 1) return fail(FB_ERR_ARG, "rotating frame needs a planet");
   if (precision != FB_FP64 && precision != FB_FP32) return fail(FB_ERR_ARG, "precision");
+  if (p->adiabatic && (precision != FB_FP64 || p->nz > 1 || p->nfluids != 1 || !(p->gamma > 1.0)))
+    return fail(FB_ERR_ARG, "adiabatic disks are FP64, 2D cylindrical, one fluid, with GAMMA > 1");
+  if (p->dust_diffusion && (precision != FB_FP64 || p->nz > 1 || p->nfluids < 2))
+    return fail(FB_ERR_ARG, "dust diffusion runs on FP64 2D cylindrical disks with dust fluids");
   e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev <= device || device < 0)
     return fail(FB_ERR_CUDA, "no CUDA device %d available (%s)", device, cudaGetErrorString(e));
@@ -532,6 +536,9 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
     D->d.alpha[f + 0 * p->nfluids] = p->invstokes[f - 1];
   }
   D->d.aspectratio = p->aspectratio; D->d.sigmaslope = p->sigmaslope; D->d.flaringindex = p->flaringindex;
+  D->d.adiabatic = p->adiabatic;
+  D->d.dust_diffusion = p->dust_diffusion;
+  D->d.gamma = p->gamma;
   D->ncell = nc = D->d.stride * D->d.sz;
   D->xmin = calloc(p->nx + 1, 8); D->ymin = calloc(D->d.sy + 1, 8); D->zmin = calloc(D->d.sz + 1, 8);
   D->xmed = calloc(p->nx, 8); D->ymed = calloc(D->d.sy, 8); D->zmed = calloc(D->d.sz, 8);
@@ -605,6 +612,10 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
         (rc = dalloc(D, (void **)&F->nshift, sizeof(int) * D->d.sy * D->d.sz)) ||
         (rc = dalloc(D, &F->rho0, e2)) || (rc = dalloc(D, &F->vx0, e2)) || (rc = dalloc(D, &F->vy0, e2)) ||
         (rc = dalloc(D, &F->vz0, e2))) {
+      fb_disk_destroy(D);
+      return rc;
+    }
+    if (p->adiabatic && ((rc = dalloc(D, &F->et, fb)) || (rc = dalloc(D, &F->e_a, fb)))) {
       fb_disk_destroy(D);
       return rc;
     }
@@ -794,6 +805,21 @@ int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, co
   if (D->d.is3d && (rc = put(D, F->vz, vz))) return rc;
   CU(cudaStreamSynchronize(D->stream));
   return FB_OK;
+}
+
+int fb_disk_get_energy(fb_disk *D, int f, double *e) {
+  if (!D || !e || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
+  CU(cudaSetDevice(D->device));
+  if (D->d.precision == FB_FP32) {
+    double *st = dstage_lock(D->device);
+    int rc = FB_OK;
+    if (!st) return fail(FB_ERR_CUDA, "device staging");
+    if (stage_move(D, st, e, D->d.fl[f].cs, (size_t)D->ncell, 0) || cudaStreamSynchronize(D->stream) != cudaSuccess)
+      rc = fail(FB_ERR_CUDA, "energy download");
+    stage_unlock();
+    return rc;
+  }
+  return get(D, e, D->d.fl[f].cs);
 }
 
 int fb_disk_get_state(fb_disk *D, int f, double *rho, double *vx, double *vy, double *vz) {
@@ -993,6 +1019,10 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   for (f = 0; f < D->p.nfluids; f++) {
     LCH(LAUNCH(sources, &D->d, f, D->stream));
     mark(D, "sources");
+    if (D->d.adiabatic) {   /* SubStep3 (algogas.c:82-84), before the ghost fill */
+      LCH(LAUNCH(substep3, &D->d, f, D->stream));
+      mark(D, "substep3");
+    }
     LCH(LAUNCH(bnd, &D->d, f, 1, D->stream));
     mark(D, "bnd_vtemp");
   }
@@ -1000,6 +1030,11 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   if (D->p.nfluids > 1) {
     LCH(LAUNCH(collisions, &D->d, D->stream));
     mark(D, "collisions");
+  }
+  /* DustDiffusion_Main (main.c:417-419), every dust fluid */
+  if (D->d.dust_diffusion) {
+    for (f = 1; f < D->p.nfluids; f++) LCH(LAUNCH(dust_diffusion, &D->d, f, D->stream));
+    mark(D, "dust_diffusion");
   }
   /* Transport (algogas.c:135-159) */
   for (f = 0; f < D->p.nfluids; f++) {

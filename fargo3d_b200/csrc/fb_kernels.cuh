@@ -65,6 +65,8 @@ struct Dims {
   int nx, ny, nz, sy, sz, pitch;
   long long stride;
   int is3d, sph, alpha;
+  int adiab;        // ADIABATIC: the cs field holds the internal energy e
+  double gam;       // GAMMA
   __device__ __forceinline__ long long l(int i, int j, int k) const {
     return (long long)i + (long long)j * pitch + (long long)k * stride;
   }
@@ -74,6 +76,7 @@ __host__ __device__ inline Dims dims_of(const fb_disk_dev &d) {
   Dims m;
   m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.sy = d.sy; m.sz = d.sz; m.pitch = d.pitch;
   m.stride = d.stride; m.is3d = d.is3d; m.sph = d.spherical; m.alpha = d.alpha_visc;
+  m.adiab = d.adiabatic; m.gam = d.gamma;
   return m;
 }
 
@@ -233,10 +236,15 @@ __device__ __forceinline__ T cfl_cell(const Dims &m, const Geo<T> &g, const S *_
   const long long lxp = (i < m.nx - 1) ? l + 1 : l - (m.nx - 1);
   const T vxx = vx[l] - (T)vm, vxxp = vx[lxp] - (T)vm;
   const T c = cs[l];
-  const T ss2 = c * c;
+  T ss2 = c * c;
   T visc;
   if (m.alpha) visc = alpha * c * c * ld(g.visc_j + j);
   else visc = nu;
+  if (m.adiab) {   // cs holds the internal energy (cfl.c:164-172)
+    const T gm = (T)m.gam;
+    ss2 = gm * (gm - (T)1) * c / (T)rho[l];
+    if (m.alpha) visc = alpha * gm * (gm - (T)1.0) * c / (T)rho[l] * ld(g.visc_j + j);
+  }
   const T ss = sqrt(ss2);
   const T zx = zsx(m, g, i, j, k), zy = zsy(g, j);
   T c1a = ss / zx, c1b = ss / zy, c1c = 0, c4 = 0, c5c = 0, c7c = 0;
@@ -419,7 +427,8 @@ template <typename T, int TX, int TY, typename S = T>
 __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
     const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx,
     const S *__restrict__ vy, S *__restrict__ vxt, S *__restrict__ vyt,
-    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg, uint3 bid) {
+    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg,
+    S *__restrict__ et, uint3 bid) {
   constexpr int W = TX + 2, H = TY + 2;
   __shared__ T s_rho[H][W], s_cs[H][W], s_vx[H][W], s_vy[H][W], s_p[H][W];
   __shared__ double s_pot[H][W];
@@ -454,7 +463,9 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
       if (FAST) s_vx[lj][li] = ((T)vx[l] + (T)bg_at(vbg, j)) - domega * ld(g.ymed + j);
       else s_vx[lj][li] = vx[l] - domega * ld(g.ymed + j);
       s_vy[lj][li] = vy[l];
-      s_p[lj][li] = r * c * c;
+      // ComputePressureFieldIso, or ComputePressureFieldAd (CompPresAd.c:54)
+      // where cs holds the internal energy
+      s_p[lj][li] = m.adiab ? ((T)m.gam - (T)1.0) * c : r * c * c;
       s_pot[lj][li] = FAST ? potential_fast(m, gd, sc, s_ind, i, j, 0) : potential_at(m, gd, sc, i, j, 0);
     }
   }
@@ -470,9 +481,19 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
       if (m.alpha && lj >= 1 && li >= 1) {
         const TV e0 = (TV)s_cs[lj][li], ex = (TV)s_cs[lj][li - 1], ey = (TV)s_cs[lj - 1][li],
                  exy = (TV)s_cs[lj - 1][li - 1];
-        viscm = alpha * (TV)0.0625 * (e0 + ex + ey + exy) * (e0 + ex + ey + exy) * (TV)ld(g.viscm_j + j);
+        if (m.adiab)   // visctensor_cyl.c:148 (cs = internal energy)
+          viscm = alpha * (TV)m.gam * ((TV)m.gam - (TV)1.0) * (e0 + ex + ey + exy) /
+                  ((TV)s_rho[lj][li] + (TV)s_rho[lj][li - 1] + (TV)s_rho[lj - 1][li] + (TV)s_rho[lj - 1][li - 1]) *
+                  (TV)ld(g.viscm_j + j);
+        else
+          viscm = alpha * (TV)0.0625 * (e0 + ex + ey + exy) * (e0 + ex + ey + exy) * (TV)ld(g.viscm_j + j);
       }
-      if (m.alpha) visc = alpha * (TV)s_cs[lj][li] * (TV)s_cs[lj][li] * (TV)ld(g.visc_j + j);
+      if (m.alpha) {
+        if (m.adiab)   // visctensor_cyl.c:147
+          visc = alpha * (TV)m.gam * ((TV)m.gam - (TV)1.0) * (TV)s_cs[lj][li] / (TV)s_rho[lj][li] * (TV)ld(g.visc_j + j);
+        else
+          visc = alpha * (TV)s_cs[lj][li] * (TV)s_cs[lj][li] * (TV)ld(g.visc_j + j);
+      }
       if (li <= TX && lj <= TY) {
         const TV r = (TV)s_rho[lj][li];
         // FP32 storage: uniform azimuthal spacing, the x factors of cell 0
@@ -500,7 +521,9 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   }
   const int li = threadIdx.x + 1, lj = threadIdx.y + 1;
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-  if (i >= m.nx || j > m.ny + FB_NGH - 1) return;
+  // adiabatic disks also need V_temp of row Ny+3, the outer edge face, which
+  // SubStep3 reads before the ghost fill (substep1_y.c: j < Ny+2*NGHY-1)
+  if (i >= m.nx || j > m.ny + FB_NGH - 1 + m.adiab) return;
   const int im = wrapx(i - 1, m.nx);
   // FP32 storage: uniform azimuthal spacing, the x factors of cell 0
   const int ix = FAST ? 0 : i, ixm = FAST ? 0 : im;
@@ -575,18 +598,127 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
   }
   vxt[l] = FAST ? ax - (T)bg_at(vbg, j) : ax;
   vyt[l] = ay;
+  if (m.adiab && !dust && et) {
+    // SubStep2_b (substep2_b.c:161-178): the artificial viscosity's heating,
+    // with the velocities the step started from (after CorrectVtheta)
+    T e = s_cs[lj][li];
+    e += -(T)dt * (qx * (s_vx[lj][li + 1] - s_vx[lj][li]) / zsx(m, g, i, j, 0));
+    e += -(T)dt * (qy * (s_vy[lj + 1][li] - s_vy[lj][li]) / (yip - yi));
+    et[l] = e;
+  }
 }
 template <typename T, int TX, int TY, typename S = T>
 __global__ void __launch_bounds__(TX *TY) k_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
     const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx,
     const S *__restrict__ vy, S *__restrict__ vxt, S *__restrict__ vyt,
-    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg) {
-  b_sources_cyl<T, TX, TY, S>(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, vbg, blockIdx);
+    const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg,
+    S *__restrict__ et) {
+  b_sources_cyl<T, TX, TY, S>(m, g, gd, rho, cs, vx, vy, vxt, vyt, scp, dust, viscous, vbg, et, blockIdx);
 }
 
 }  // namespace fb
 
 namespace fb {
+
+// ---------------------------------------------------------------------------
+// Dust diffusion (DustDiffusion_Main, dust_diffusion_main.c:3-28), 2D
+// cylindrical: each dust fluid's density diffuses down the gradient of its
+// concentration c = rho_d / (rho_d + rho_g) with the gas's diffusivity --
+// Nu (VISCOSITY) or Alpha cs^2 / Omega_K (ALPHAVISCOSITY, isothermal), at cell
+// centres and at the radial faces (dust_diffusion_coefficients.c:94-120) --
+// rho_d += dt div(D grad c) in the reference's operation order
+// (dust_diffusion_core.c:132-185), into a buffer, for the active rows.
+template <typename T, typename S>
+__global__ void __launch_bounds__(128) k_dust_diffusion(Dims m, Geo<T> g, const S *__restrict__ rd,
+                                                        const S *__restrict__ rg, const S *__restrict__ csg,
+                                                        S *__restrict__ out, const fb_scalars *__restrict__ scp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = FB_NGH + blockIdx.y;
+  if (i >= m.nx) return;
+  const T dt = (T)scp->dt, nu = (T)scp->nu, alpha = (T)scp->alpha;
+  const long long l = m.l(i, j, 0);
+  const int ixp = i < m.nx - 1 ? i + 1 : 0;
+  const long long lxp = (i < m.nx - 1) ? l + 1 : l - (m.nx - 1), lxm = i > 0 ? l - 1 : l + (m.nx - 1);
+  const long long lyp = l + m.pitch, lym = l - m.pitch;
+  // Sdiffyczc at a cell of row jj, Sdiffyfzc at the lower face of row jj
+  auto sdc = [&](long long ll, int jj) -> T {
+    if (!m.alpha) return nu;
+    const T ss2 = (T)csg[ll] * (T)csg[ll];
+    const T r3 = ld(g.ymed + jj) * ld(g.ymed + jj) * ld(g.ymed + jj);
+    return alpha * ss2 / sqrt((T)1.0 * (T)1.0 / r3);
+  };
+  auto sdf = [&](long long ll, int jj) -> T {
+    if (!m.alpha) return nu;
+    T ssf2;
+    if (jj == 0) ssf2 = (T)csg[ll] * (T)csg[ll];
+    else ssf2 = (T)0.5 * ((T)csg[ll] + (T)csg[ll - m.pitch]) * (T)0.5 * ((T)csg[ll] + (T)csg[ll - m.pitch]);
+    const T r3 = ld(g.ymin + jj) * ld(g.ymin + jj) * ld(g.ymin + jj);
+    return alpha * ssf2 / sqrt((T)1.0 * (T)1.0 / r3);
+  };
+  const T d0 = rd[l], g0 = rg[l];
+  T update = 0.0;
+  const T c = d0 / (d0 + g0);
+  const T dxmin = ld(g.xmin + i + 1) - ld(g.xmin + i);
+  const T dxmedp = (T)1.0 / ld(g.invdiffxmed + ixp), dxmedm = (T)1.0 / ld(g.invdiffxmed + i);
+  const T dxp = rd[lxp], gxp = rg[lxp], dxm = rd[lxm], gxm = rg[lxm];
+  const T d1 = (T)0.25 * (d0 + g0 + dxp + gxp) * (sdc(lxp, j) + sdc(l, j));
+  const T d2 = (T)0.25 * (d0 + g0 + dxm + gxm) * (sdc(lxm, j) + sdc(l, j));
+  const T cxp = dxp / (dxp + gxp), cxm = dxm / (dxm + gxm);
+  const T ym = ld(g.ymed + j), ymp = ld(g.ymed + j + 1), ymm = ld(g.ymed + j - 1);
+  const T yi = ld(g.ymin + j), yip = ld(g.ymin + j + 1);
+  update += (T)1.0 / ym / ym / (dxmin) * (d1 * (cxp - c) / (dxmedp) - (d2 * (c - cxm)) / (dxmedm));
+  const T dyp = rd[lyp], gyp = rg[lyp], dym = rd[lym], gym = rg[lym];
+  const T d3 = (T)0.5 * (d0 + g0 + dyp + gyp) * sdf(lyp, j + 1);
+  const T d4 = (T)0.5 * (d0 + g0 + dym + gym) * sdf(l, j);
+  const T cyp = dyp / (dyp + gyp), cym = dym / (dym + gym);
+  update += (T)1.0 / ym / (yip - yi) * (yip * d3 * (cyp - c) / (ymp - ym) - (yi * d4 * (c - cym)) / (ym - ymm));
+  out[l] = d0 + dt * update;
+}
+
+// copy_field(Density, Pressure) of DustDiffusion_Main for the active rows
+template <typename S>
+__global__ void __launch_bounds__(128) k_copy_rows(Dims m, const S *__restrict__ src, S *__restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nx) return;
+  const long long l = m.l(i, FB_NGH + blockIdx.y, 0);
+  dst[l] = src[l];
+}
+
+// FillGhosts(DENS): the density's radial ghosts only (KEPLERIAN2DDENS)
+template <typename T, typename S>
+__global__ void k_bnd_rho_y(Dims m, Geo<T> g, const double *__restrict__ tab, S *__restrict__ rho) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y % 3, s = blockIdx.y / 3;
+  if (i >= m.nx) return;
+  const int jgh = s == 0 ? jj : m.ny + FB_NGH + jj, jact = s == 0 ? 2 * FB_NGH - jj - 1 : m.ny + FB_NGH - 1 - jj;
+  rho[m.l(i, jgh, 0)] = rho[m.l(i, jact, 0)] * (T)tab[s * 3 + jj];
+  (void)g;
+}
+
+// ---------------------------------------------------------------------------
+// SubStep3 (substep3.c:79-118), adiabatic disks: the compression work of the
+// source step, e *= (1 - theta) / (1 + theta) with theta = dt (GAMMA - 1)
+// div(V_temp) / (2 Vol), on the energy after SubStep2_b (et) into the Energy
+// field, for the active rows (the ghosts are refilled after it).  The
+// divergence uses the macros' unparenthesised products (SurfX, SurfY,
+// InvVol: define.h:228-235) in the reference's order.
+template <typename T>
+__global__ void __launch_bounds__(128) k_substep3(Dims m, Geo<T> g, const T *__restrict__ et,
+                                                  const T *__restrict__ vxt, const T *__restrict__ vyt,
+                                                  T *__restrict__ e, const fb_scalars *__restrict__ scp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = FB_NGH + blockIdx.y, k = 0;
+  if (i >= m.nx) return;
+  const T dt = (T)scp->dt;
+  const long long l = m.l(i, j, k);
+  const long long lxp = (i < m.nx - 1) ? l + 1 : l - (m.nx - 1);
+  T div_v = 0.0;
+  div_v += (vxt[lxp] - vxt[l]) * ld(g.sxj + j) * ld(g.sxk + k);
+  div_v += (vyt[l + m.pitch] * ld(g.syj + j + 1) * ld(g.syk + k) * ld(g.sxi + i) -
+            vyt[l] * ld(g.syj + j) * ld(g.syk + k) * ld(g.sxi + i));
+  const T term = (T)0.5 * dt * ((T)m.gam - (T)1.) * div_v * ld(g.invvj + j) / (ld(g.syk + k) * ld(g.sxi + i));
+  e[l] = et[l] * (((T)1.0 - term) / ((T)1.0 + term));
+}
 
 // ---------------------------------------------------------------------------
 // Ghost cells from the setups' boundary templates (std/boundaries.txt with
@@ -611,7 +743,7 @@ struct BndTab {
 template <typename T, typename S = T>
 __device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
                         S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
-                        int do_rho, const double *__restrict__ vbg, uint3 bid) {
+                        int do_rho, const double *__restrict__ vbg, uint3 bid, S *__restrict__ energy = nullptr) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   const int jj = bid.y % 3, s = bid.y / 3, k = bid.z;
   if (i >= m.nx) return;
@@ -636,6 +768,8 @@ __device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restri
     if (BG) vx[lgh] = (vact + of * yact * sz) * (T)tb.sqf(s, jj) * (T)tb.cf(s, jj) - ygh * of * sz - bgh;
     else vx[lgh] = (vx[lact] + of * yact * sz) * (T)tb.sqf(s, jj) * (T)tb.cf(s, jj) - ygh * of * sz;
   }
+  // Energy of adiabatic disks: SYMMETRIC (the ghost mirrors the active cell)
+  if (energy) energy[lgh] = energy[lact];
   // Vy: ANTISYMMETRIC, staggered in y (|-a|0|a|)
   if (s == 0) vy[lgh] = -vy[m.l(i, jlacts, k)];
   else if (jj < nghy - 1) vy[m.l(i, ny + nghy + 1 + jj, k)] = -vy[m.l(i, jlacts, k)];
@@ -646,8 +780,8 @@ __device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restri
 template <typename T, typename S = T>
 __global__ void k_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restrict__ rho, S *__restrict__ vx,
                         S *__restrict__ vy, S *__restrict__ vz, const fb_scalars *__restrict__ scp,
-                        int do_rho, const double *__restrict__ vbg) {
-  b_bnd_y<T, S>(m, g, tb, rho, vx, vy, vz, scp, do_rho, vbg, blockIdx);
+                        int do_rho, const double *__restrict__ vbg, S *__restrict__ energy) {
+  b_bnd_y<T, S>(m, g, tb, rho, vx, vy, vz, scp, do_rho, vbg, blockIdx, energy);
 }
 
 // Colatitude sides (3D): one thread per (i, j, ghost layer kk, side s).
@@ -794,7 +928,8 @@ template <typename T, int DIR, int NS, typename S = T>
 __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, int nq, int clo, int chi,
                                                    int t2lo, S *__restrict__ rho_out, S *q_out0, S *q_out1,
                                                    S *q_out2, S *q_out3, S *q_out4, S *q_out5,
-                                                   const fb_scalars *__restrict__ scp, uint3 bid) {
+                                                   const fb_scalars *__restrict__ scp, uint3 bid,
+                                                   const S *__restrict__ e_in = nullptr, S *__restrict__ e_out = nullptr) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   if (i >= m.nx) return;
   const int t2 = t2lo + bid.y;
@@ -883,6 +1018,25 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, in
       }
     }
   }
+  if (e_in) {
+    // TransportY/Z of the Energy of an adiabatic disk (transport.c:97-98,
+    // 122-123): DivideByRho, VanLeer a/b, Update, as for the momenta
+    T qv[NS + 4];
+#pragma unroll
+    for (int w = 0; w < NS + 4; w++) {
+      qv[w] = e_in[cidx(min(c0 - 2 + w, cmax))];
+      a[w] = qv[w] / r[w];
+    }
+    col_sweep_q<T, DIR, NS>(cg, c0, a, vel, nullptr, dt, qs);
+#pragma unroll
+    for (int u = 0; u < NS; u++) {
+      const int c = c0 + u;
+      if (c <= chi) {
+        const T flux = cg.surf(vel[u] * qs[u] * rs[u], c) - cg.surf(vel[u + 1] * qs[u + 1] * rs[u + 1], c + 1);
+        e_out[cidx(c)] = qv[u + 2] + cg.finish(flux, dt, c);
+      }
+    }
+  }
 #pragma unroll
   for (int u = 0; u < NS; u++) {
     const int c = c0 + u;
@@ -894,8 +1048,10 @@ template <typename T, int DIR, int NS, typename S = T>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, int nq, int clo, int chi,
                                                    int t2lo, S *__restrict__ rho_out, S *q_out0, S *q_out1,
                                                    S *q_out2, S *q_out3, S *q_out4, S *q_out5,
-                                                   const fb_scalars *__restrict__ scp) {
-  b_sweep_col<T, DIR, NS, S>(m, g, src, nq, clo, chi, t2lo, rho_out, q_out0, q_out1, q_out2, q_out3, q_out4, q_out5, scp, blockIdx);
+                                                   const fb_scalars *__restrict__ scp, const S *__restrict__ e_in,
+                                                   S *__restrict__ e_out) {
+  b_sweep_col<T, DIR, NS, S>(m, g, src, nq, clo, chi, t2lo, rho_out, q_out0, q_out1, q_out2, q_out3, q_out4, q_out5, scp,
+                             blockIdx, e_in, e_out);
 }
 
 }  // namespace fb
@@ -919,12 +1075,16 @@ __device__ __forceinline__ void b_newvel(Dims m, Geo<T> g, const S *__restrict__
                                                 S *__restrict__ vy, S *__restrict__ vz, const S *__restrict__ rho0,
                                                 const S *__restrict__ vx0, const S *__restrict__ vy0,
                                                 const S *__restrict__ vz0, const double *__restrict__ ramps,
-                                                int stockholm, const fb_scalars *__restrict__ scp, uint3 bid) {
+                                                int stockholm, const fb_scalars *__restrict__ scp, uint3 bid,
+                                                const S *__restrict__ e_src = nullptr, S *__restrict__ e_dst = nullptr) {
   const int i = bid.x * blockDim.x + threadIdx.x;
   const int j = FB_NGH + bid.y;
   const int k = m.is3d ? FB_NGH + bid.z : 0;
   if (i >= m.nx) return;
   const long long l = m.l(i, j, k);
+  // the transported energy of an adiabatic disk becomes its Energy field
+  // (StockholmBoundary leaves the energy alone: stockholm.c:167-186)
+  if (e_src) e_dst[l] = e_src[l];
   const int im = i > 0 ? i - 1 : m.nx - 1;
   const long long lxm = i > 0 ? l - 1 : l + (m.nx - 1);
   const T of = (T)scp->omegaframe;
@@ -1003,8 +1163,10 @@ __global__ void __launch_bounds__(256) k_newvel(Dims m, Geo<T> g, const S *__res
                                                 S *__restrict__ vy, S *__restrict__ vz, const S *__restrict__ rho0,
                                                 const S *__restrict__ vx0, const S *__restrict__ vy0,
                                                 const S *__restrict__ vz0, const double *__restrict__ ramps,
-                                                int stockholm, const fb_scalars *__restrict__ scp) {
-  b_newvel<T, S>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, rho, vx, vy, vz, rho0, vx0, vy0, vz0, ramps, stockholm, scp, blockIdx);
+                                                int stockholm, const fb_scalars *__restrict__ scp,
+                                                const S *__restrict__ e_src, S *__restrict__ e_dst) {
+  b_newvel<T, S>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, rho, vx, vy, vz, rho0, vx0, vy0, vz0, ramps, stockholm, scp,
+                 blockIdx, e_src, e_dst);
 }
 
 }  // namespace fb
@@ -1504,8 +1666,15 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
           // the residual of FP32 rings in FP32: vm_rel is the small mean of
           // the background-relative velocity
           const float vr = (float)vm_rel;
+          if constexpr (C == 4) {   // aligned float4 reads (no bank conflicts)
+            const int tpn = lt < tpr - 1 ? lt + 1 : 0;
+            const float4 a4 = reinterpret_cast<const float4 *>(svx + sl0 * nxp)[lt];
+            const float v4 = svx[sl0 * nxp + 4 * tpn];
+            v[0] = a4.x - vr; v[1] = a4.y - vr; v[2] = a4.z - vr; v[3] = a4.w - vr; v[4] = v4 - vr;
+          } else {
 #pragma unroll
-          for (int f = 0; f <= C; f++) v[f] = svx[sl0 * nxp + P(wrap(c0 + f))] - vr;
+            for (int f = 0; f <= C; f++) v[f] = svx[sl0 * nxp + P(wrap(c0 + f))] - vr;
+          }
         } else {
 #pragma unroll
           for (int f = 0; f <= C; f++) v[f] = (T)((double)svx[sl0 * nxp + P(wrap(c0 + f))] - vm_rel);  // residual
@@ -1611,16 +1780,22 @@ __device__ __forceinline__ void b_sweep_x2(const Dims &m, const Geo<T> &g, const
       const int nsh = s_nsh[slot];
       int it0 = (c0 - nsh) % nx;
       if (it0 < 0) it0 += nx;
-      int its[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) its[u] = (it0 + u < nx) ? it0 + u : it0 + u - nx;
+      // the four source cells it0 .. it0+3 (mod nx) lie in the aligned float4
+      // blocks q0 = it0 / 4 and the next one (mod nx / 4); the offset
+      // it0 % 4 is the same for the whole ring (c0 is a multiple of 4)
+      const int q0 = it0 >> 2, q1 = (q0 + 1 < tpr) ? q0 + 1 : 0, sh = it0 & 3;
       const T *b = bufA + (size_t)slot * nf * nxp;
       const long long l = m.l(c0, j, k);
-      reinterpret_cast<float4 *>(rho + l)[0] = make_float4(b[its[0]], b[its[1]], b[its[2]], b[its[3]]);
-      for (int q = 0; q < nq; q++) {
-        const T *bq = b + (1 + q) * nxp;
-        reinterpret_cast<float4 *>(qg[q] + l)[0] = make_float4(bq[its[0]], bq[its[1]], bq[its[2]], bq[its[3]]);
-      }
+      auto realign = [&](const T *row) -> float4 {
+        const float4 x = reinterpret_cast<const float4 *>(row)[q0], y = reinterpret_cast<const float4 *>(row)[q1];
+        const float w[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+        return sh == 0 ? make_float4(w[0], w[1], w[2], w[3])
+             : sh == 1 ? make_float4(w[1], w[2], w[3], w[4])
+             : sh == 2 ? make_float4(w[2], w[3], w[4], w[5])
+                       : make_float4(w[3], w[4], w[5], w[6]);
+      };
+      reinterpret_cast<float4 *>(rho + l)[0] = realign(b);
+      for (int q = 0; q < nq; q++) reinterpret_cast<float4 *>(qg[q] + l)[0] = realign(b + (1 + q) * nxp);
     }
     return;
   }

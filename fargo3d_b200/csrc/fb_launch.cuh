@@ -66,9 +66,10 @@ static int launch_sources(const fb_disk_dev *d, int f, cudaStream_t st) {
         F.dust, viscous, F.vbg, (const float *)F.shear_bg);
   } else if (!m.is3d) {
     constexpr int TX = 32, TY = 8;
-    dim3 grid((m.nx + TX - 1) / TX, (m.ny + TY - 1) / TY);
+    // adiabatic: one more row (the outer edge face, read by SubStep3)
+    dim3 grid((m.nx + TX - 1) / TX, (m.ny + m.adiab + TY - 1) / TY);
     k_sources_cyl<T, TX, TY, S><<<grid, dim3(TX, TY), 0, st>>>(m, g, gd, (const S *)F.rho, (const S *)F.cs,
-        (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, d->scal_dev, F.dust, viscous, F.vbg);
+        (const S *)F.vx, (const S *)F.vy, (S *)F.vxt, (S *)F.vyt, d->scal_dev, F.dust, viscous, F.vbg, (S *)F.et);
   } else {
     constexpr int TX = 32, TY = 4;
     dim3 grid((m.nx + TX - 1) / TX, (m.ny + TY - 1) / TY, m.nz);
@@ -93,7 +94,9 @@ static int launch_bnd(const fb_disk_dev *d, int f, int vtemp, cudaStream_t st) {
     k_bnd_z<T, S><<<gz, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp, F.vbg);
   }
   dim3 gy((m.nx + bx - 1) / bx, 6, m.sz);
-  k_bnd_y<T, S><<<gy, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp, F.vbg);
+  // adiabatic disks: the energy's ghosts too, after the sources and at the end
+  k_bnd_y<T, S><<<gy, bx, 0, st>>>(m, g, tb, rho, vx, vy, vz, d->scal_dev, !vtemp, F.vbg,
+                                  m.adiab ? (S *)F.cs : (S *)nullptr);
   return (int)cudaGetLastError();
 }
 
@@ -123,8 +126,10 @@ static int launch_sweep_cols_n(const fb_disk_dev *d, int f, cudaStream_t st) {
     rho_out = (S *)F.rho_a;
     q[0] = (S *)F.mpx; q[1] = (S *)F.mmx; q[2] = (S *)F.mpy; q[3] = (S *)F.mmy; q[4] = q[5] = nullptr;
     dim3 grid((m.nx + bx - 1) / bx, 1, (yhi - ylo + NS) / NS);
+    // adiabatic disks transport their energy into e_a as a fifth quantity
     k_sweep_col<T, 0, NS, S><<<grid, bx, 0, st>>>(m, g, src, nq, ylo, yhi, 0, rho_out, q[0], q[1], q[2], q[3], q[4],
-                                               q[5], d->scal_dev);
+                                               q[5], d->scal_dev, m.adiab ? (const S *)F.cs : (const S *)nullptr,
+                                               m.adiab ? (S *)F.e_a : (S *)nullptr);
   } else {
     nq = 6;
     const int zlo = FB_NGH - 1, zhi = m.nz + FB_NGH - 1;
@@ -133,7 +138,8 @@ static int launch_sweep_cols_n(const fb_disk_dev *d, int f, cudaStream_t st) {
     src.dl = (const T *)F.dlb_z;
     dim3 gz((m.nx + bx - 1) / bx, m.sy - 1, (zhi - zlo + NS) / NS);
     k_sweep_col<T, 1, NS, S><<<gz, bx, 0, st>>>(m, g, src, nq, zlo, zhi, 0, (S *)F.rho_a, (S *)F.mpx, (S *)F.mmx,
-                                             (S *)F.mpy, (S *)F.mmy, (S *)F.mpz, (S *)F.mmz, d->scal_dev);
+                                             (S *)F.mpy, (S *)F.mmy, (S *)F.mpz, (S *)F.mmz, d->scal_dev,
+                                             (const S *)nullptr, (S *)nullptr);
     // Y sweep from set A into set B, layers 2 .. Nz+2
     QSrc<T, S> sa;
     sa.rho = (const S *)F.rho_a; sa.vxt = (const S *)F.vxt; sa.vyt = (const S *)F.vyt; sa.vzt = (const S *)F.vzt;
@@ -145,7 +151,7 @@ static int launch_sweep_cols_n(const fb_disk_dev *d, int f, cudaStream_t st) {
     q[0] = (S *)F.mpx_b; q[1] = (S *)F.mmx_b; q[2] = (S *)F.mpy_b; q[3] = (S *)F.mmy_b; q[4] = (S *)F.mpz_b;
     q[5] = (S *)F.mmz_b;
     k_sweep_col<T, 0, NS, S><<<gy, bx, 0, st>>>(m, g, sa, nq, ylo, yhi, zlo, rho_out, q[0], q[1], q[2], q[3], q[4],
-                                             q[5], d->scal_dev);
+                                             q[5], d->scal_dev, (const S *)nullptr, (S *)nullptr);
   }
   return (int)cudaGetLastError();
 }
@@ -168,10 +174,11 @@ static int launch_sweep_x(const fb_disk_dev *d, int f, cudaStream_t st) {
   Geo<double> gd = geo_of<double>(d->geomd);
   const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;
   const bool b = m.is3d;
-  const int nq = b ? 6 : 4;
+  // 2D adiabatic disks: the energy is the fifth transported quantity
+  const int nq = b ? 6 : (m.adiab ? 5 : 4);
   S *rho_out = (S *)(b ? F.rho_b : F.rho_a);
   S *q[6] = {(S *)(b ? F.mpx_b : F.mpx), (S *)(b ? F.mmx_b : F.mmx), (S *)(b ? F.mpy_b : F.mpy),
-             (S *)(b ? F.mmy_b : F.mmy), (S *)(b ? F.mpz_b : F.mpz), (S *)(b ? F.mmz_b : F.mmz)};
+             (S *)(b ? F.mmy_b : F.mmy), (S *)(b ? F.mpz_b : (m.adiab ? F.e_a : F.mpz)), (S *)(b ? F.mmz_b : F.mmz)};
   // azimuthal sweep: C cells per thread, whole rings per CTA of 256 threads
   const int C = disk_cx(*d);
   if (!valid_cx(m.nx, C)) return (int)cudaErrorInvalidValue;
@@ -223,7 +230,8 @@ static int launch_newvel(const fb_disk_dev *d, int f, cudaStream_t st) {
   dim3 grid((m.nx + bx - 1) / bx, m.ny, m.is3d ? m.nz : 1);
   k_newvel<T, S><<<grid, bx, 0, st>>>(m, g, rt, mpx, mmx, mpy, mmy, mpz, mmz, (S *)F.rho, (S *)F.vx, (S *)F.vy,
                                    (S *)F.vz, (const S *)F.rho0, (const S *)F.vx0, (const S *)F.vy0,
-                                   (const S *)F.vz0, d->ramps, d->stockholm, d->scal_dev);
+                                   (const S *)F.vz0, d->ramps, d->stockholm, d->scal_dev,
+                                   m.adiab ? (const S *)F.e_a : (const S *)nullptr, m.adiab ? (S *)F.cs : (S *)nullptr);
   return (int)cudaGetLastError();
 }
 
@@ -243,6 +251,35 @@ static int launch_collisions(const fb_disk_dev *d, cudaStream_t st) {
     case 8: k_collisions<T, 8, S><<<g, 128, 0, st>>>(*d, m, gd, d->scal_dev); break;
     default: return (int)cudaErrorInvalidValue;
   }
+  return (int)cudaGetLastError();
+}
+
+// DustDiffusion_Main for dust fluid f (FP64, 2D): the diffused density into
+// rho_a (free until transport), copied back over the active rows, then the
+// density's ghosts (FillGhosts(DENS))
+template <typename T, typename S>
+static int launch_dust_diffusion(const fb_disk_dev *d, int f, cudaStream_t st) {
+  if (!d->dust_diffusion || f < 1 || sizeof(S) != 8 || d->is3d) return (int)cudaErrorInvalidValue;
+  const fb_fluid_dev &F = d->fl[f], &G = d->fl[0];
+  Dims m = dims_of(*d);
+  const Geo<double> g = geo_of<double>(d->geomd);
+  const dim3 grid((m.nx + 127) / 128, m.ny);
+  k_dust_diffusion<double, double><<<grid, 128, 0, st>>>(m, g, (const double *)F.rho, (const double *)G.rho,
+                                                          (const double *)G.cs, (double *)F.rho_a, d->scal_dev);
+  k_copy_rows<double><<<grid, 128, 0, st>>>(m, (const double *)F.rho_a, (double *)F.rho);
+  k_bnd_rho_y<double, double><<<dim3((m.nx + 127) / 128, 6), 128, 0, st>>>(m, g, d->bnd_tab, (double *)F.rho);
+  return (int)cudaGetLastError();
+}
+
+// SubStep3 of an adiabatic disk (FP64 storage and arithmetic)
+template <typename T, typename S>
+static int launch_substep3(const fb_disk_dev *d, int f, cudaStream_t st) {
+  if (!d->adiabatic || sizeof(S) != 8) return (int)cudaErrorInvalidValue;
+  const fb_fluid_dev &F = d->fl[f];
+  Dims m = dims_of(*d);
+  k_substep3<double><<<dim3((m.nx + 127) / 128, m.ny), 128, 0, st>>>(
+      m, geo_of<double>(d->geomd), (const double *)F.et, (const double *)F.vxt, (const double *)F.vyt,
+      (double *)F.cs, d->scal_dev);
   return (int)cudaGetLastError();
 }
 
@@ -296,6 +333,12 @@ int FB_CAT(fb_launch_newvel, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
 }
 int FB_CAT(fb_launch_collisions, FB_SUF)(const fb_disk_dev *d, void *s) {
   return fb::launch_collisions<FB_REAL, FB_STORE>(d, (cudaStream_t)s);
+}
+int FB_CAT(fb_launch_dust_diffusion, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
+  return fb::launch_dust_diffusion<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
+}
+int FB_CAT(fb_launch_substep3, FB_SUF)(const fb_disk_dev *d, int fluid, void *s) {
+  return fb::launch_substep3<FB_REAL, FB_STORE>(d, fluid, (cudaStream_t)s);
 }
 int FB_CAT(fb_launch_mass, FB_SUF)(const fb_disk_dev *d, int fluid, double *part, double *out, void *s) {
   return fb::launch_mass<FB_STORE>(d, fluid, part, out, (cudaStream_t)s);

@@ -159,6 +159,7 @@ extern "C" int fb_cfl_dt_static(const fb_cfl_static_args *a, double *dt_out, voi
   m.nx = a->nx; m.ny = a->ny; m.nz = is3d ? a->nz : 1; m.sy = a->ny + 6; m.sz = is3d ? a->nz + 6 : 1;
   m.pitch = (int)pitch; m.stride = stride; m.is3d = is3d; m.sph = a->spherical;
   m.alpha = a->alpha_visc;
+  m.adiab = 0; m.gam = 0.0;   // isothermal fields
   fb::Geo<double> gd{};
   gd.xmin = a->xmin;
   k_reset_min<<<1, 1, 0, st>>>(dtmin);

@@ -111,13 +111,31 @@ static FB_HD FB_FI void fb_nbody_deriv(const fb_psys *S, const double *q, const 
   double dist[FB_MAXPLANETS], coef, dd;
   int i, j;
   for (i = 0; i < n; i++) dist[i] = sqrt(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+#ifdef __CUDA_ARCH__
+  /* on the device (batched steps): one reciprocal of d^3 per planet instead
+     of the three chained divisions of runge_kutta.c -- the same quantity,
+     rounded differently, in a step whose latency is this dependency chain */
+  double id3[FB_MAXPLANETS];
+  for (i = 0; i < n; i++) id3[i] = 1.0 / (dist[i] * dist[i] * dist[i]);
+#define FB_INV_D3(k) (id3[k])
+#else
+#define FB_INV_D3(k) (1.0 / dist[k] / dist[k] / dist[k])
+#endif
   for (i = 0; i < n; i++) {
     der[i] = vx[i]; der[i + n] = vy[i]; der[i + 2 * n] = vz[i];
+#ifdef __CUDA_ARCH__
+    coef = -FB_G * FB_MSTAR * FB_INV_D3(i);
+#else
     coef = -FB_G * FB_MSTAR / dist[i] / dist[i] / dist[i];
+#endif
     der[i + 3 * n] = coef * x[i]; der[i + 4 * n] = coef * y[i]; der[i + 5 * n] = coef * z[i];
     for (j = 0; j < n; j++) {
       if (S->indirect_term) {
+#ifdef __CUDA_ARCH__
+        coef = FB_G * ms[j] * FB_INV_D3(j);
+#else
         coef = FB_G * ms[j] / dist[j] / dist[j] / dist[j];
+#endif
         der[i + 3 * n] -= coef * x[j]; der[i + 4 * n] -= coef * y[j]; der[i + 5 * n] -= coef * z[j];
       }
       if (j != i && S->feelothers[i]) {
@@ -130,6 +148,7 @@ static FB_HD FB_FI void fb_nbody_deriv(const fb_psys *S, const double *q, const 
     }
   }
   for (i = 0; i < 6 * n; i++) der[i] *= dt;
+#undef FB_INV_D3
 }
 
 static FB_HD FB_FI void fb_nbody_rk5_n(fb_psys *S, double dt, const int n) {

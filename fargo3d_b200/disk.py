@@ -94,6 +94,13 @@ class Disk:
         _abi.check(_abi.lib().fb_disk_device_fields(self._h, fluid, ptrs, C.byref(esz)))
         return [p for p in ptrs], esz.value
 
+    def energy(self, fluid: int = 0):
+        """The fluid's Energy field: the internal energy of an adiabatic disk,
+        the sound speed of an isothermal one."""
+        e = np.empty(self.shape)
+        _abi.check(_abi.lib().fb_disk_get_energy(self._h, fluid, _ptr(e)))
+        return e
+
     def mass(self, fluid: int = 0) -> float:
         """Total mass of a fluid (compensated FP64 sum of rho * Vol over the
         active cells, on the device)."""

@@ -64,6 +64,9 @@ class DiskConfig:
     nfluids: int = 1
     invstokes: Tuple[float, ...] = ()
     stockholm: bool = True
+    dust_diffusion: bool = False      # DUSTDIFFUSION of the dust fluids (multifluid)
+    adiabatic: bool = False           # ADIABATIC equation of state (else ISOTHERMAL)
+    gamma: float = 1.66666667         # GAMMA
     noise: float = 1e-4
     seed: int = 0
     dt_output: float = 0.314159265359  # DT
@@ -94,14 +97,25 @@ def config_fargo2d(nx: int = 384, ny: int = 128, seed: int = 0) -> DiskConfig:
 
 
 def config_multifluid(nx: int = 768, ny: int = 256, nfluids: int = 5,
-                      invstokes=(1000.0, 100.0, 10.0, 1.0), seed: int = 0) -> DiskConfig:
+                      invstokes=(1000.0, 100.0, 10.0, 1.0), seed: int = 0, dust_diffusion: bool = False) -> DiskConfig:
     """2D cylindrical gas disk with nfluids - 1 dust species coupled by
     implicit drag (setups/fargo_multifluid with DRAGFORCE + STOKESNUMBER):
     1/St per dust species `invstokes`, dust-to-gas ratio 0.01 / (nfluids - 1)
     per species, fixed frame, no indirect term, constant nu = 1e-5, planet
-    q = 1e-3 at r = 1."""
+    q = 1e-3 at r = 1; with dust_diffusion, the dust densities also diffuse
+    down their concentration gradients (DUSTDIFFUSION, the setup's stock
+    flag)."""
     return DiskConfig(nx=nx, ny=ny, sigma0=1e-4, frame="F", omegaframe=0.0, indirect_term=False,
-                      nfluids=nfluids, invstokes=tuple(invstokes[:nfluids - 1]), seed=seed)
+                      nfluids=nfluids, invstokes=tuple(invstokes[:nfluids - 1]), seed=seed,
+                      dust_diffusion=dust_diffusion)
+
+
+def config_adiabatic2d(nx: int = 384, ny: int = 128, seed: int = 0, gamma: float = 1.4) -> DiskConfig:
+    """The 2D cylindrical disk of config_fargo2d with an ADIABATIC equation of
+    state (internal energy e, P = (GAMMA - 1) e) and alpha viscosity
+    (alpha = 1e-3): the initial energy gives the isothermal disk's pressure,
+    and the energy's radial boundaries mirror the active cells."""
+    return DiskConfig(nx=nx, ny=ny, adiabatic=True, gamma=gamma, alpha_visc=True, alpha=1e-3, nu=0.0, seed=seed)
 
 
 def config_p3disof(nx: int = 512, ny: int = 256, nz: int = 48, seed: int = 0) -> DiskConfig:
@@ -175,6 +189,10 @@ def initial_state(cfg: DiskConfig, fluid: int = 0):
         cs = hh * np.sqrt(1.0 / r)
         vy = np.zeros(cfg.shape)
         vz = np.zeros(cfg.shape)
+    if cfg.adiabatic:
+        # the internal energy whose pressure (GAMMA - 1) e is the isothermal
+        # disk's rho cs^2 (FARGO3D's Energy field holds e)
+        cs = rho * cs * cs / (cfg.gamma - 1.0)
     if fluid > 0:
         # dust (setups/fargo_multifluid/condinit.c:38-44): eps times the gas
         # density, Keplerian azimuthal velocity without pressure support, no

@@ -56,6 +56,15 @@ typedef struct {
   int nfluids;                 /* 1: gas; >1: gas + dust with implicit drag      */
   double invstokes[FB_MAXFLUIDS];   /* drag (STOKESNUMBER): [f-1] = 1/St of dust fluid f */
   int stockholm;               /* STOCKHOLM damping                             */
+  int adiabatic;               /* ADIABATIC equation of state: the Energy field is
+                                  the internal energy e, P = (GAMMA - 1) e; else
+                                  ISOTHERMAL (Energy = sound speed).  FP64, 2D
+                                  cylindrical, one fluid, one-disk path only     */
+  double gamma;                /* GAMMA                                         */
+  int dust_diffusion;          /* DUSTDIFFUSION: the dust densities diffuse down
+                                  their concentration gradients with the gas's
+                                  diffusivity (dust_diffusion_main.c).  FP64, 2D,
+                                  nfluids > 1, one-disk path only               */
 } fb_params;
 
 typedef struct fb_disk fb_disk;
@@ -70,6 +79,9 @@ int fb_disk_destroy(fb_disk *d);
 int fb_disk_set_state(fb_disk *d, int fluid, const double *rho, const double *vx, const double *vy,
                       const double *vz, const double *cs);
 int fb_disk_get_state(fb_disk *d, int fluid, double *rho, double *vx, double *vy, double *vz);
+/* The fluid's Energy field (the cs array fb_disk_set_state takes): the
+ * internal energy of an adiabatic disk, the sound speed of an isothermal one. */
+int fb_disk_get_energy(fb_disk *d, int fluid, double *energy);
 
 int fb_disk_initialize(fb_disk *d);
 

@@ -46,6 +46,9 @@ typedef struct {
   int nfluids;                 /* 1: gas only; >1: gas + dust, implicit drag       */
   double invstokes[FO_MAXFLUIDS]; /* STOKESNUMBER drag: [f-1] = 1/St of dust fluid f */
   int stockholm;               /* STOCKHOLM damping on/off                        */
+  int adiabatic;               /* ADIABATIC equation of state (reference builds only) */
+  double gamma;                /* GAMMA                                            */
+  int dust_diffusion;          /* DUSTDIFFUSION (reference builds only)            */
 } fo_params;
 
 typedef struct fo_disk fo_disk;

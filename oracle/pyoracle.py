@@ -37,6 +37,7 @@ class FoParams(C.Structure):
         ("eccentricity", C.c_double), ("inclination", C.c_double),
         ("nfluids", C.c_int), ("invstokes", C.c_double * MAXF),
         ("stockholm", C.c_int),
+        ("adiabatic", C.c_int), ("gamma", C.c_double), ("dust_diffusion", C.c_int),
     ]
 
 
@@ -60,6 +61,9 @@ def make_params(cfg) -> FoParams:
     for i, v in enumerate(cfg.invstokes):
         p.invstokes[i] = v
     p.stockholm = int(cfg.stockholm)
+    p.adiabatic = int(getattr(cfg, "adiabatic", False))
+    p.gamma = float(getattr(cfg, "gamma", 1.66666667))
+    p.dust_diffusion = int(getattr(cfg, "dust_diffusion", False))
     return p
 
 
@@ -82,10 +86,14 @@ def build_dropin(ref: str | None = None):
 
 
 def ref_variant(cfg) -> str:
+    if getattr(cfg, "adiabatic", False):
+        if cfg.is3d or not cfg.alpha_visc or cfg.nfluids > 1:
+            raise ValueError("the compiled reference has one adiabatic variant: 2D, one fluid, alpha viscosity")
+        return "cyl2d_ad"
     if cfg.nfluids > 1:
         if cfg.nfluids != 5 or cfg.is3d or cfg.alpha_visc:
             raise ValueError("the compiled reference has one multifluid variant: 2D, 5 fluids, constant nu")
-        return "mf5"
+        return "mf5_dd" if getattr(cfg, "dust_diffusion", False) else "mf5"
     if cfg.is3d:
         return "sph3d"
     return "cyl2d_alpha" if cfg.alpha_visc else "cyl2d"
@@ -110,6 +118,9 @@ class Disk:
         as the parity tests build them), 'ref_o3' (the same sources with the
         reference's stock -O3, for timing) or 'dropin'."""
         self.cfg, self.kind = cfg, kind
+        if kind == "oracle" and (getattr(cfg, "adiabatic", False) or getattr(cfg, "dust_diffusion", False)):
+            raise ValueError("the oracle restatement has neither the adiabatic EOS nor dust diffusion: "
+                             "those disks run on the reference build")
         if kind == "oracle":
             path = os.path.join(HERE, "_build", "libfargo_oracle.so")
         elif kind == "dropin":
@@ -194,6 +205,16 @@ class Disk:
         xa, ya, za = np.zeros(nx + 1), np.zeros(ny + 1), np.zeros(nz + 1)
         self._call("get_geometry", _ptr(xa), _ptr(ya), _ptr(za))
         return xa, ya, za
+
+    def energy(self, fluid: int = 0):
+        """The fluid's Energy field (the internal energy of an adiabatic
+        build, the sound speed of an isothermal one); 'ref' kinds."""
+        if self.kind not in ("ref", "ref_o3", "dropin"):
+            raise NotImplementedError
+        out = np.zeros(self.shape)
+        self.lib.ref_get_energy.restype = None
+        self.lib.ref_get_energy(C.c_int(fluid), _ptr(out))
+        return out
 
     def write_outputs(self, outdir: str, n: int, fluid: int = 0):
         """The reference's own output writers ('ref' kinds): fluid's merged

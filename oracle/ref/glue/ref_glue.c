@@ -43,7 +43,11 @@ void CheckMuteY_cpu(void) {}
 void CheckMuteZ_cpu(void) {}
 static void comm_none(int v) { (void)v; }
 /* PrimitiveVariables (LowTasks.c:13-36); only its value is passed to comm. */
+#ifdef ADIABATIC
+int PrimitiveVariables(void) { return DENS | ENERGY | VX | VY; }
+#else
 int PrimitiveVariables(void) { return DENS | VX | VY; }
+#endif
 
 /* SelectFluid (LowTasks.c:565-593) */
 void SelectFluid(int n) {
@@ -78,6 +82,16 @@ void SelectFluid(int n) {
         for (i = 0; i < Nx + 2 * NGHX; i++) { side_body }               \
   }
 
+/* The adiabatic variant of the fargo setup (written for this oracle: no
+ * setup of the reference runs a 2D adiabatic disk) adds
+ *   Energy: Ymin: SYMMETRIC  Ymax: SYMMETRIC
+ * to setups/fargo/fargo.bound: the ghost energy mirrors the active cell. */
+#ifdef ADIABATIC
+#define BND_ENERGY_SYMMETRIC Energy->field_cpu[lgh] = Energy->field_cpu[lact];
+#else
+#define BND_ENERGY_SYMMETRIC
+#endif
+
 #ifdef CYLINDRICAL
 /* setups/fargo/fargo.bound: KEPLERIAN2DDENS, KEPLERIAN2DVAZIM, ANTISYMMETRIC */
 static void bnd_ymin(void) {
@@ -91,6 +105,7 @@ static void bnd_ymin(void) {
     jgh = j; jact = (2 * nghy - j - 1);
     density[lgh] = density[lact] * pow(Ymed(jact) / Ymed(jgh), sigmaslope);
     vx[lgh] = (vx[lact] + Ymed(jact) * omegaframe) * sqrt(Ymed(jact) / Ymed(jgh)) - Ymed(jgh) * omegaframe;
+    BND_ENERGY_SYMMETRIC
     vy[lghs] = -vy[lacts];
     vy[lacts_null] = 0;)
 }
@@ -106,6 +121,7 @@ static void bnd_ymax(void) {
     jgh = (ny + nghy + j); jact = (ny + nghy - 1 - j);
     density[lgh] = density[lact] * pow(Ymed(jact) / Ymed(jgh), sigmaslope);
     vx[lgh] = (vx[lact] + Ymed(jact) * omegaframe) * sqrt(Ymed(jact) / Ymed(jgh)) - Ymed(jgh) * omegaframe;
+    BND_ENERGY_SYMMETRIC
     if (j < size_y - 1) vy[lghs] = -vy[lacts];
     vy[lacts_null] = 0;)
 }
@@ -304,6 +320,15 @@ static void glue_change_arch(void) {
 #ifdef DRAGFORCE
   _collisions = _collisions_cpu;
 #endif
+#ifdef ADIABATIC
+  ComputePressureFieldAd = ComputePressureFieldAd_cpu;
+  SubStep3 = SubStep3_cpu;
+#endif
+#ifdef DUSTDIFFUSION
+  DustDiffusion_Core = DustDiffusion_Core_cpu;
+  DustDiffusion_Coefficients = DustDiffusion_Coefficients_cpu;
+  copy_field = copy_field_cpu;
+#endif
   comm = comm_none;
 }
 
@@ -348,7 +373,17 @@ int ref_create(const fo_params *p) {
   XMIN = p->xmin; XMAX = p->xmax; YMIN = p->ymin; YMAX = p->ymax; ZMIN = p->zmin; ZMAX = p->zmax;
   strcpy(SPACING, p->log_spacing ? "Log" : "Lin");
   ASPECTRATIO = p->aspectratio; SIGMASLOPE = p->sigmaslope; FLARINGINDEX = p->flaringindex;
-  NU = p->nu; ALPHA = p->alpha; CFL = p->cfl; GAMMA = 1.66666667;
+  NU = p->nu; ALPHA = p->alpha; CFL = p->cfl; GAMMA = p->adiabatic ? p->gamma : 1.66666667;
+#ifdef ADIABATIC
+  if (!p->adiabatic) return -3;
+#else
+  if (p->adiabatic) return -3;
+#endif
+#ifdef DUSTDIFFUSION
+  if (!p->dust_diffusion) return -4;
+#else
+  if (p->dust_diffusion) return -4;
+#endif
   OMEGAFRAME = p->omegaframe;
   INDIRECTTERM = p->indirect_term ? YES : NO;
   THICKNESSSMOOTHING = p->thickness_smoothing; ROCHESMOOTHING = p->roche_smoothing; MASSTAPER = p->mass_taper;
@@ -399,6 +434,11 @@ int ref_create(const fo_params *p) {
   Total_Density = CreateField("Total_Density", 0, 0, 0, 0);
   QL = CreateField("QLeft", 0, 0, 0, 0);
   QR = CreateField("QRight", 0, 0, 0, 0);
+#ifdef DUSTDIFFUSION
+  /* CreateFields (LowTasks.c:649-655): the diffusion coefficients */
+  Sdiffyczc = CREATEFIELDALIAS("Sdiffyczc", Mpx, 0);
+  Sdiffyfzc = CREATEFIELDALIAS("Sdiffyfzc", Mmx, 0);
+#endif
   glue_planets(p);
   /* main.c:240-242 */
   if (Corotating && ThereArePlanets) OMEGAFRAME = GetPsysInfo(FREQUENCY);
@@ -440,6 +480,12 @@ void ref_set_state(int f, const double *rho, const double *vx, const double *vy,
   (void)vz;
 #endif
   if (cs) memcpy(Fluids[f]->Energy->field_cpu, cs, n);
+}
+
+/* the fluid's Energy field: the internal energy (ADIABATIC) or the sound
+ * speed (ISOTHERMAL) */
+void ref_get_energy(int f, double *e) {
+  memcpy(e, Fluids[f]->Energy->field_cpu, sizeof(real) * ncell());
 }
 
 void ref_get_state(int f, double *rho, double *vx, double *vy, double *vz) {
@@ -495,6 +541,9 @@ double ref_step(double DTint) {
   MULTIFLUID(Sources(dt));
 #ifdef DRAGFORCE
   Collisions(dt, 1);
+#endif
+#ifdef DUSTDIFFUSION
+  DustDiffusion_Main(dt);   /* main.c:417-419 */
 #endif
   MULTIFLUID(Transport(dt));
   PhysicalTime += dt;
