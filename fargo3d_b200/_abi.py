@@ -36,6 +36,7 @@ class FbParams(C.Structure):
         ("nfluids", C.c_int), ("invstokes", C.c_double * FB_MAXFLUIDS),
         ("stockholm", C.c_int),
         ("adiabatic", C.c_int), ("gamma", C.c_double), ("dust_diffusion", C.c_int),
+        ("slab_y0", C.c_int), ("slab_ny_global", C.c_int),
     ]
 
 
@@ -64,6 +65,8 @@ def params_of(cfg) -> FbParams:
     p.adiabatic = int(cfg.adiabatic)
     p.gamma = float(cfg.gamma)
     p.dust_diffusion = int(cfg.dust_diffusion)
+    p.slab_y0 = int(getattr(cfg, "slab_y0", 0))
+    p.slab_ny_global = int(getattr(cfg, "slab_ny_global", 0))
     return p
 
 
@@ -95,6 +98,11 @@ def lib():
     L.fb_disk_set_wait_limit.argtypes = [C.c_void_p, C.c_longlong]
     L.fb_disk_mass.argtypes = [C.c_void_p, C.c_int, _D]
     L.fb_disk_get_energy.argtypes = [C.c_void_p, C.c_int, _D]
+    L.fb_disk_step_begin.argtypes = [C.c_void_p, _D]
+    L.fb_disk_step_advance.argtypes = [C.c_void_p, C.c_double, C.c_double, _D]
+    L.fb_disk_step_transport.argtypes = [C.c_void_p]
+    L.fb_disk_halo_bytes.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t)]
+    L.fb_disk_halo.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int]
     L.fb_disk_stream.restype = C.c_void_p
     L.fb_disk_stream.argtypes = [C.c_void_p]
     L.fb_params_bytes.argtypes = [C.POINTER(FbParams), C.c_int, C.POINTER(C.c_size_t)]

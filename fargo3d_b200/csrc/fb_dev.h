@@ -83,6 +83,7 @@ typedef struct {
   double aspectratio, sigmaslope, flaringindex;
   int adiabatic;          /* ADIABATIC: fl[].cs holds the internal energy */
   int dust_diffusion;     /* DUSTDIFFUSION of the dust fluids */
+  int bc_lo, bc_hi;       /* the inner / outer radial edge is the mesh's own (1) or a slab's (0) */
   double gamma;           /* GAMMA */
   fb_geom_dev geom;       /* precision of the disk */
   fb_geom_dev geomd;      /* always double */

@@ -203,13 +203,16 @@ static int upload(fb_disk *D, const void **dst, const double *src, int n, int as
 static void mesh(fb_disk *D) {
   const fb_params *p = &D->p;
   int i, j, k, sx = p->nx, sy = D->d.sy, sz = D->d.sz, is3d = D->d.is3d;
-  double dx = (p->xmax - p->xmin) / p->nx, dy = (p->ymax - p->ymin) / p->ny;
+  /* a slab's rows are rows y0 .. y0 + ny - 1 of the whole mesh: its edges
+     are the whole mesh's, from the global index (split.c / InitSpace) */
+  const int nyg = p->slab_ny_global > 0 ? p->slab_ny_global : p->ny, y0 = p->slab_ny_global > 0 ? p->slab_y0 : 0;
+  double dx = (p->xmax - p->xmin) / p->nx, dy = (p->ymax - p->ymin) / nyg;
   double dz = is3d ? (p->zmax - p->zmin) / p->nz : 0.0;
   if (p->log_spacing) {
-    dy = (log(p->ymax) - log(p->ymin)) / p->ny;
-    for (j = 0; j < sy + 1; j++) D->ymin[j] = exp(log(p->ymin) + dy * (j - NG));
+    dy = (log(p->ymax) - log(p->ymin)) / nyg;
+    for (j = 0; j < sy + 1; j++) D->ymin[j] = exp(log(p->ymin) + dy * (j + y0 - NG));
   } else {
-    for (j = 0; j < sy + 1; j++) D->ymin[j] = p->ymin + dy * (j - NG);
+    for (j = 0; j < sy + 1; j++) D->ymin[j] = p->ymin + dy * (j + y0 - NG);
   }
   for (k = 0; k < sz + 1; k++) D->zmin[k] = is3d ? p->zmin + dz * (k - NG) : 0.0;
   for (i = 0; i < sx + 1; i++) D->xmin[i] = p->xmin + dx * i;
@@ -508,6 +511,13 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
     return fail(FB_ERR_ARG, "adiabatic disks are FP64, 2D cylindrical, one fluid, with GAMMA > 1");
   if (p->dust_diffusion && (precision != FB_FP64 || p->nz > 1 || p->nfluids < 2))
     return fail(FB_ERR_ARG, "dust diffusion runs on FP64 2D cylindrical disks with dust fluids");
+  if (p->slab_ny_global > 0) {
+    int n;
+    if (p->slab_y0 < 0 || p->slab_y0 + p->ny > p->slab_ny_global || precision != FB_FP64 || p->nfluids != 1)
+      return fail(FB_ERR_ARG, "a slab is FP64, one fluid, rows inside [0, slab_ny_global)");
+    for (n = 0; n < p->nplanets; n++)
+      if (p->pl_feeldisk[n]) return fail(FB_ERR_ARG, "planets that feel the disk need the whole disk");
+  }
   e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev <= device || device < 0)
     return fail(FB_ERR_CUDA, "no CUDA device %d available (%s)", device, cudaGetErrorString(e));
@@ -538,6 +548,8 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
   D->d.aspectratio = p->aspectratio; D->d.sigmaslope = p->sigmaslope; D->d.flaringindex = p->flaringindex;
   D->d.adiabatic = p->adiabatic;
   D->d.dust_diffusion = p->dust_diffusion;
+  D->d.bc_lo = p->slab_ny_global <= 0 || p->slab_y0 == 0;
+  D->d.bc_hi = p->slab_ny_global <= 0 || p->slab_y0 + p->ny == p->slab_ny_global;
   D->d.gamma = p->gamma;
   D->ncell = nc = D->d.stride * D->d.sz;
   D->xmin = calloc(p->nx + 1, 8); D->ymin = calloc(D->d.sy + 1, 8); D->zmin = calloc(D->d.sz + 1, 8);
@@ -973,13 +985,15 @@ int fb_disk_initialize(fb_disk *D) {
   return FB_OK;
 }
 
-int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
+/* Part 1 of a step: ComputeVmed(Vx) + cfl (main.c:366-388), and the disk's
+ * pull on the planets that feel it (AdvanceSystemFromDisk's accelerations,
+ * planets.c:86-114), from the state at the step's start; the CFL minimum
+ * and the failure flags come back to the host. */
+int fb_disk_step_begin(fb_disk *D, double *cfl_min) {
   int f, rc;
-  double dt;
   const uint64_t start_bits = 0x4415AF1D78B58C40ULL; /* 1e20, the MIN reduction start (define.h:165) */
   if (!D) return fail(FB_ERR_ARG, "null disk");
   CU(cudaSetDevice(D->device));
-  /* ComputeVmed(Vx) + cfl (main.c:366-388) */
   CU(cudaMemcpyAsync(D->d.dtmin, &start_bits, 8, cudaMemcpyHostToDevice, D->stream));
   if ((rc = push_scalars(D))) return rc;
   D->nev = 0;
@@ -988,8 +1002,6 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
   mark(D, "rowsum");
   for (f = 0; f < D->p.nfluids; f++) LCH(LAUNCH(cfl, &D->d, f, D->stream));
   mark(D, "cfl");
-  /* AdvanceSystemFromDisk's accelerations (planets.c:86-114): the disk's
-   * pull at each planet that feels it, from the state at the step start */
   if (D->feeldisk) {
     int n;
     for (n = 0; n < D->ps.np; n++) {
@@ -1009,12 +1021,23 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
     return fail(FB_ERR_NONFINITE, "a staged ring load of the azimuthal sweep did not complete in time");
   if (((const uint64_t *)D->h_dtmin)[1] != 0)
     return fail(FB_ERR_NONFINITE, "non-finite time step or non-positive density in the state");
-  /* CflFluidsMin (cfl_fluids_min.c:3-22), the DT clip (main.c:388-395) and
-   * compute_potential's planetary update (potential.c:10-49) */
-  dt = fb_psys_step(&D->ps, D->h_dtmin[0], DT, &D->sc, D->feeldisk ? D->h_dtmin + 8 : NULL);
-  if (dt < 0.0) return fail(FB_ERR_NULL_DT, "null time step (CFL minimum %g)", D->h_dtmin[0]);
+  if (cfl_min) *cfl_min = D->h_dtmin[0];
+  return FB_OK;
+}
+
+/* Part 2: CflFluidsMin with the (global) CFL minimum, the DT clip
+ * (main.c:388-395) and compute_potential's planetary update
+ * (potential.c:10-49), then Sources (algogas.c:30-120) with SubStep3 and the
+ * ghost fill of V_temp on the mesh's own edges, the implicit drag
+ * (main.c:412-414) and the dust diffusion (main.c:417-419). */
+int fb_disk_step_advance(fb_disk *D, double DT, double cfl_min, double *dt_out) {
+  int f, rc;
+  double dt;
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  CU(cudaSetDevice(D->device));
+  dt = fb_psys_step(&D->ps, cfl_min, DT, &D->sc, D->feeldisk ? D->h_dtmin + 8 : NULL);
+  if (dt < 0.0) return fail(FB_ERR_NULL_DT, "null time step (CFL minimum %g)", cfl_min);
   if ((rc = push_scalars(D))) return rc;
-  /* Sources (algogas.c:30-120) with its closing FillGhosts on V_temp */
   mark(D, "host_scalars");
   for (f = 0; f < D->p.nfluids; f++) {
     LCH(LAUNCH(sources, &D->d, f, D->stream));
@@ -1026,17 +1049,25 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
     LCH(LAUNCH(bnd, &D->d, f, 1, D->stream));
     mark(D, "bnd_vtemp");
   }
-  /* implicit drag between the fluids on V_temp (main.c:412-414) */
   if (D->p.nfluids > 1) {
     LCH(LAUNCH(collisions, &D->d, D->stream));
     mark(D, "collisions");
   }
-  /* DustDiffusion_Main (main.c:417-419), every dust fluid */
   if (D->d.dust_diffusion) {
     for (f = 1; f < D->p.nfluids; f++) LCH(LAUNCH(dust_diffusion, &D->d, f, D->stream));
     mark(D, "dust_diffusion");
   }
-  /* Transport (algogas.c:135-159) */
+  if (dt_out) *dt_out = dt;
+  if (D->p.slab_ny_global > 0) CU(cudaStreamSynchronize(D->stream));   /* V_temp is read for the halos */
+  return FB_OK;
+}
+
+/* Part 3: Transport (algogas.c:135-159), NewVelocity + StockholmBoundary and
+ * the ghost fill on the mesh's own edges (main.c:427-431). */
+int fb_disk_step_transport(fb_disk *D) {
+  int f;
+  if (!D) return fail(FB_ERR_ARG, "null disk");
+  CU(cudaSetDevice(D->device));
   for (f = 0; f < D->p.nfluids; f++) {
     LCH(LAUNCH(rowsum, &D->d, f, 1, D->stream));
     mark(D, "rowsum_vtemp");
@@ -1045,7 +1076,6 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
     LCH(LAUNCH(sweep_x, &D->d, f, D->stream));
     mark(D, "sweep_x");
   }
-  /* NewVelocity + StockholmBoundary + FillGhosts (main.c:427-431) */
   for (f = 0; f < D->p.nfluids; f++) {
     LCH(LAUNCH(newvel, &D->d, f, D->stream));
     mark(D, "newvel");
@@ -1058,7 +1088,63 @@ int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
     D->prof_n = D->nev - 1;
     for (i = 1; i < D->nev; i++) cudaEventElapsedTime(&D->prof_ms[i - 1], D->ev[i - 1], D->ev[i]);
   }
-  if (dt_out) *dt_out = dt;
+  if (D->p.slab_ny_global > 0) CU(cudaStreamSynchronize(D->stream));   /* the state is read for the halos */
+  return FB_OK;
+}
+
+int fb_disk_step(fb_disk *D, double DT, double *dt_out) {
+  double cflmin = 0.0;
+  int rc = fb_disk_step_begin(D, &cflmin);
+  if (!rc) rc = fb_disk_step_advance(D, DT, cflmin, dt_out);
+  if (!rc) rc = fb_disk_step_transport(D);
+  return rc;
+}
+
+/* The fields a halo carries: state (rho, vx, vy[, vz][, energy]) or V_temp
+ * (rho, vx_temp, vy_temp[, vz_temp][, energy]) of the disk's one fluid. */
+static int halo_fields(fb_disk *D, int which, void **out) {
+  const fb_fluid_dev *F = &D->d.fl[0];
+  int n = 0;
+  out[n++] = F->rho;
+  out[n++] = which == FB_HALO_VTEMP ? F->vxt : F->vx;
+  out[n++] = which == FB_HALO_VTEMP ? F->vyt : F->vy;
+  if (D->d.is3d) out[n++] = which == FB_HALO_VTEMP ? F->vzt : F->vz;
+  if (D->d.adiabatic) out[n++] = F->cs;
+  return n;
+}
+
+int fb_disk_halo_bytes(fb_disk *D, int which, size_t *bytes) {
+  void *fl[8];
+  if (!D || !bytes || (which != FB_HALO_STATE && which != FB_HALO_VTEMP)) return fail(FB_ERR_ARG, "bad arguments");
+  *bytes = (size_t)halo_fields(D, which, fl) * D->d.sz * NG * D->d.nx * D->esz;
+  return FB_OK;
+}
+
+/* NGHY rows of every halo field, per layer, between the disk and a
+ * contiguous buffer [field][layer][3][Nx] (comm.c:197-363 sends the same
+ * rows of the primitive fields to the neighbouring domains). */
+int fb_disk_halo(fb_disk *D, int which, int side, int unpack, void *buf, int host) {
+  void *fl[8];
+  int n, q;
+  size_t rowb, lay;
+  int j0;
+  if (!D || !buf || (which != FB_HALO_STATE && which != FB_HALO_VTEMP) || side < 0 || side > 1)
+    return fail(FB_ERR_ARG, "bad arguments");
+  CU(cudaSetDevice(D->device));
+  n = halo_fields(D, which, fl);
+  rowb = (size_t)NG * D->d.nx * D->esz;              /* three rows of one layer */
+  lay = (size_t)D->d.stride * D->esz;                 /* one layer */
+  if (!unpack) j0 = side == 0 ? NG : D->d.ny;         /* the first / last three active rows */
+  else j0 = side == 0 ? 0 : D->d.ny + NG;             /* the ghost rows */
+  for (q = 0; q < n; q++) {
+    char *field = (char *)fl[q] + (size_t)j0 * D->d.pitch * D->esz;
+    char *b = (char *)buf + (size_t)q * D->d.sz * rowb;
+    enum cudaMemcpyKind kind = unpack ? (host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice)
+                                      : (host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice);
+    if (unpack) CU(cudaMemcpy2DAsync(field, lay, b, rowb, rowb, D->d.sz, kind, D->stream));
+    else CU(cudaMemcpy2DAsync(b, rowb, field, lay, rowb, D->d.sz, kind, D->stream));
+  }
+  CU(cudaStreamSynchronize(D->stream));
   return FB_OK;
 }
 

@@ -67,6 +67,7 @@ struct Dims {
   int is3d, sph, alpha;
   int adiab;        // ADIABATIC: the cs field holds the internal energy e
   double gam;       // GAMMA
+  int bclo, bchi;   // the radial edges are the mesh's own (boundary templates) or a slab's
   __device__ __forceinline__ long long l(int i, int j, int k) const {
     return (long long)i + (long long)j * pitch + (long long)k * stride;
   }
@@ -77,6 +78,7 @@ __host__ __device__ inline Dims dims_of(const fb_disk_dev &d) {
   m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.sy = d.sy; m.sz = d.sz; m.pitch = d.pitch;
   m.stride = d.stride; m.is3d = d.is3d; m.sph = d.spherical; m.alpha = d.alpha_visc;
   m.adiab = d.adiabatic; m.gam = d.gamma;
+  m.bclo = d.bc_lo; m.bchi = d.bc_hi;
   return m;
 }
 
@@ -747,6 +749,8 @@ __device__ __forceinline__ void b_bnd_y(Dims m, Geo<T> g, BndTab tb, S *__restri
   const int i = bid.x * blockDim.x + threadIdx.x;
   const int jj = bid.y % 3, s = bid.y / 3, k = bid.z;
   if (i >= m.nx) return;
+  // a slab's inner edge takes its ghosts from the neighbouring slab
+  if ((s == 0 && !m.bclo) || (s == 1 && !m.bchi)) return;
   const T of = (T)scp->omegaframe;
   const int nghy = FB_NGH, ny = m.ny;
   int jgh, jact, jlacts, jnull;

@@ -160,6 +160,7 @@ extern "C" int fb_cfl_dt_static(const fb_cfl_static_args *a, double *dt_out, voi
   m.pitch = (int)pitch; m.stride = stride; m.is3d = is3d; m.sph = a->spherical;
   m.alpha = a->alpha_visc;
   m.adiab = 0; m.gam = 0.0;   // isothermal fields
+  m.bclo = m.bchi = 1;
   fb::Geo<double> gd{};
   gd.xmin = a->xmin;
   k_reset_min<<<1, 1, 0, st>>>(dtmin);

@@ -83,6 +83,33 @@ class Disk:
     def run(self, nsteps: int, dt_interval: float = 1e30):
         return [self.step(dt_interval) for _ in range(nsteps)]
 
+    # the step in three parts (a radial slab of a disk split over GPUs)
+    def step_begin(self) -> float:
+        """ComputeVmed + cfl: this disk's CFL minimum."""
+        m = C.c_double()
+        _abi.check(_abi.lib().fb_disk_step_begin(self._h, C.byref(m)))
+        return m.value
+
+    def step_advance(self, dt_interval: float, cfl_min: float) -> float:
+        """DT clip and planets with the (global) CFL minimum, Sources."""
+        dt = C.c_double()
+        _abi.check(_abi.lib().fb_disk_step_advance(self._h, dt_interval, cfl_min, C.byref(dt)))
+        return dt.value
+
+    def step_transport(self):
+        """Transport, NewVelocity, Stockholm, the mesh-edge ghosts."""
+        _abi.check(_abi.lib().fb_disk_step_transport(self._h))
+
+    def halo_bytes(self, which: int) -> int:
+        n = C.c_size_t()
+        _abi.check(_abi.lib().fb_disk_halo_bytes(self._h, which, C.byref(n)))
+        return n.value
+
+    def halo(self, which: int, side: int, unpack: bool, ptr: int, on_host: bool):
+        """Copy the halo rows of one edge between the disk and a buffer at
+        `ptr` (device or host memory)."""
+        _abi.check(_abi.lib().fb_disk_halo(self._h, which, side, int(unpack), C.c_void_p(ptr), int(on_host)))
+
     def scalars(self):
         o = np.zeros(8)
         _abi.check(_abi.lib().fb_disk_get_scalars(self._h, _ptr(o)))

@@ -69,6 +69,8 @@ class DiskConfig:
     gamma: float = 1.66666667         # GAMMA
     noise: float = 1e-4
     seed: int = 0
+    slab_y0: int = 0                  # radial slab of a larger disk: rows [slab_y0, slab_y0 + ny)
+    slab_ny_global: int = 0           # of a mesh of slab_ny_global rows (0: the disk is whole)
     dt_output: float = 0.314159265359  # DT
 
     @property

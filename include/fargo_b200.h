@@ -65,6 +65,12 @@ typedef struct {
                                   their concentration gradients with the gas's
                                   diffusivity (dust_diffusion_main.c).  FP64, 2D,
                                   nfluids > 1, one-disk path only               */
+  int slab_y0;                 /* radial slab of a larger disk (split.c:76-213):  */
+  int slab_ny_global;          /* rows [slab_y0, slab_y0 + ny) of a mesh of
+                                  slab_ny_global rows spanning [ymin, ymax]; the
+                                  boundary templates apply on the mesh's own
+                                  edges only.  0: the disk is whole.  One fluid,
+                                  FP64, planets that do not feel the disk        */
 } fb_params;
 
 typedef struct fb_disk fb_disk;
@@ -88,6 +94,34 @@ int fb_disk_initialize(fb_disk *d);
 /* One hydro step: dt = min(CFL dt, what is left of a DT interval of length
  * dt_interval), exactly as main.c:388-395.  *dt_out receives dt. */
 int fb_disk_step(fb_disk *d, double dt_interval, double *dt_out);
+
+/* One hydro step in three parts, for a disk split into radial slabs over
+ * several GPUs (one slab per process; the reference's MPI run: split.c,
+ * comm.c:197-363).  fb_disk_step is the three in a row.
+ *   fb_disk_step_begin     ComputeVmed + cfl (main.c:366-388): the slab's CFL
+ *                          minimum, to be reduced with MIN over the slabs
+ *                          (CflFluidsMin's MPI_Allreduce, cfl_fluids_min.c:14-17)
+ *   fb_disk_step_advance   DT clip and planets with the global minimum, then
+ *                          Sources (+ SubStep3): V_temp complete on the active
+ *                          rows, physical ghosts filled; the caller then
+ *                          exchanges the FB_HALO_VTEMP halos (FillGhosts after
+ *                          Sources, algogas.c:116-118)
+ *   fb_disk_step_transport Transport, NewVelocity, Stockholm and the physical
+ *                          ghosts; the caller then exchanges the FB_HALO_STATE
+ *                          halos (FillGhosts, main.c:431)
+ * Halos: fb_disk_halo copies NGHY = 3 rows of every exchanged field (state:
+ * rho, vx, vy[, vz][, energy]; vtemp: rho, vx_temp, vy_temp[, vz_temp][,
+ * energy]) between the slab and a contiguous buffer [field][layer][3][Nx] of
+ * fb_disk_halo_bytes bytes, device or host memory: side 0 = the inner (lower
+ * radius) edge, side 1 = the outer; unpack = 0 packs the slab's first / last
+ * three active rows, unpack = 1 writes its three ghost rows.  Synchronous. */
+#define FB_HALO_STATE 0
+#define FB_HALO_VTEMP 1
+int fb_disk_step_begin(fb_disk *d, double *cfl_min);
+int fb_disk_step_advance(fb_disk *d, double dt_interval, double cfl_min_global, double *dt_out);
+int fb_disk_step_transport(fb_disk *d);
+int fb_disk_halo_bytes(fb_disk *d, int which, size_t *bytes);
+int fb_disk_halo(fb_disk *d, int which, int side, int unpack, void *buf, int buf_on_host);
 
 /* [0] PhysicalTime [1] OMEGAFRAME [2] last dt [3..6] planet 0 x, y, vx, vy [7] Domega */
 int fb_disk_get_scalars(fb_disk *d, double out8[8]);

@@ -49,6 +49,7 @@ typedef struct {
   int adiabatic;               /* ADIABATIC equation of state (reference builds only) */
   double gamma;                /* GAMMA                                            */
   int dust_diffusion;          /* DUSTDIFFUSION (reference builds only)            */
+  int slab_y0, slab_ny_global; /* the library's radial slabs (unused here: whole disks) */
 } fo_params;
 
 typedef struct fo_disk fo_disk;

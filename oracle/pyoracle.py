@@ -38,6 +38,7 @@ class FoParams(C.Structure):
         ("nfluids", C.c_int), ("invstokes", C.c_double * MAXF),
         ("stockholm", C.c_int),
         ("adiabatic", C.c_int), ("gamma", C.c_double), ("dust_diffusion", C.c_int),
+        ("slab_y0", C.c_int), ("slab_ny_global", C.c_int),
     ]
 
 
