@@ -79,11 +79,13 @@ def build(ref: str | None = None):
 
 
 def build_dropin(ref: str | None = None):
-    """The drop-in variants of the reference build (needs libfargo_b200.so
-    and the reference tree, as for build())."""
+    """The drop-in variants of the reference build -- the step loop's body
+    handed to the library ('dropin') and the stock step loop with the
+    setup-directory files of fargo3d_b200/integration/setup ('shadow') --
+    (needs libfargo_b200.so and the reference tree, as for build())."""
     ref = ref or os.environ.get("FARGO_REFERENCE")
     if ref and os.path.isdir(os.path.join(ref, "src")):
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref, "dropin"], check=True)
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref, "dropin", "shadow"], check=True)
 
 
 def ref_variant(cfg) -> str:
@@ -117,22 +119,23 @@ class Disk:
     def __init__(self, cfg, kind: str = "oracle"):
         """kind: 'oracle' (the C restatement), 'ref' (the reference's sources
         as the parity tests build them), 'ref_o3' (the same sources with the
-        reference's stock -O3, for timing) or 'dropin'."""
+        reference's stock -O3, for timing), 'dropin' or 'shadow' (the
+        reference's build with its hydro step on the B200 library)."""
         self.cfg, self.kind = cfg, kind
         if kind == "oracle" and (getattr(cfg, "adiabatic", False) or getattr(cfg, "dust_diffusion", False)):
             raise ValueError("the oracle restatement has neither the adiabatic EOS nor dust diffusion: "
                              "those disks run on the reference build")
         if kind == "oracle":
             path = os.path.join(HERE, "_build", "libfargo_oracle.so")
-        elif kind == "dropin":
-            path = os.path.join(HERE, "_ref", "libfargo_ref_dropin_%s.so" % ref_variant(cfg))
+        elif kind in ("dropin", "shadow"):
+            path = os.path.join(HERE, "_ref", "libfargo_ref_%s_%s.so" % (kind, ref_variant(cfg)))
         elif kind == "ref_o3":
             path = os.path.join(HERE, "_ref", "libfargo_ref_%s_o3.so" % ref_variant(cfg))
         else:
             path = os.path.join(HERE, "_ref", "libfargo_ref_%s.so" % ref_variant(cfg))
         if not os.path.exists(path):
             raise FileNotFoundError(path)
-        if kind in ("ref", "ref_o3", "dropin"):
+        if kind in ("ref", "ref_o3", "dropin", "shadow"):
             # Each reference library holds one disk in its globals (and in
             # function-level statics such as potential.c's alreadycalculated):
             # load a fresh private copy per Disk.  dlopen identifies a library
@@ -210,7 +213,7 @@ class Disk:
     def energy(self, fluid: int = 0):
         """The fluid's Energy field (the internal energy of an adiabatic
         build, the sound speed of an isothermal one); 'ref' kinds."""
-        if self.kind not in ("ref", "ref_o3", "dropin"):
+        if self.kind not in ("ref", "ref_o3", "dropin", "shadow"):
             raise NotImplementedError
         out = np.zeros(self.shape)
         self.lib.ref_get_energy.restype = None
@@ -221,7 +224,7 @@ class Disk:
         """The reference's own output writers ('ref' kinds): fluid's merged
         <outdir>/<name><field><n>.dat files (WriteMerging) and, for fluid 0,
         the planet files' next line (WritePlanetSystemFile)."""
-        if self.kind not in ("ref", "ref_o3"):
+        if self.kind not in ("ref", "ref_o3", "shadow"):
             raise NotImplementedError("only the reference-source libraries write FARGO3D outputs")
         self.lib.ref_write_outputs.restype = C.c_int
         self.lib.ref_write_outputs.argtypes = [C.c_int, C.c_char_p, C.c_int]

@@ -9,7 +9,11 @@
  * boundaries() and all *_cpu kernels.
  * With -DFB_DROPIN the step instead runs through the drop-in binding
  * (fargo3d_b200/integration/b200_hydro.c) on the B200 library, from the same
- * Fields, .par globals and planetary system.
+ * Fields, .par globals and planetary system.  With -DFB_SHADOW the step
+ * body stays the stock one and the setup-directory files of
+ * fargo3d_b200/integration/setup (algogas.c, cfl.c, compute_vmed.c,
+ * dust_diffusion_main.c, fresh.c) replace the reference's, as a FARGO3D setup
+ * directory would (VPATH, src/makefile:306).
  * What is written here: what FARGO3D's build generates or its start-up does
  * (main.c, ChangeArch, var.c/param.h, the generated boundary functions from
  * std/boundaries.txt + the setup's .bound file, InitSpace/InitSurfaces,
@@ -23,6 +27,9 @@
 #include "fargo_oracle.h"
 
 /* ---- stand-ins for functions outside the compiled set ------------------- */
+#ifndef FB_SHADOW
+/* fresh.c (a CPU build keeps no device copies); with -DFB_SHADOW the
+ * setup-directory fresh.c of fargo3d_b200/integration/setup is linked */
 void Input_CPU(Field *f, int line, const char *file) { (void)f; (void)line; (void)file; }
 void Output_CPU(Field *f, int line, const char *file) { (void)f; (void)line; (void)file; }
 void Input2D_CPU(Field2D *f, int line, const char *file) { (void)f; (void)line; (void)file; }
@@ -30,6 +37,7 @@ void Output2D_CPU(Field2D *f, int line, const char *file) { (void)f; (void)line;
 void Input2DInt_CPU(FieldInt2D *f, int line, const char *file) { (void)f; (void)line; (void)file; }
 void Output2DInt_CPU(FieldInt2D *f, int line, const char *file) { (void)f; (void)line; (void)file; }
 void Draft(Field *f, int line, const char *file) { (void)f; (void)line; (void)file; }
+#endif
 void masterprint(const char *t, ...) { (void)t; }
 void mastererr(const char *t, ...) { (void)t; }
 void prs_exit(int c) { fprintf(stderr, "reference prs_exit(%d)\n", c); exit(c); }
@@ -471,6 +479,15 @@ static size_t ncell(void) { return (size_t)(Nx + 2 * NGHX) * (Ny + 2 * NGHY) * (
 void ref_set_state(int f, const double *rho, const double *vx, const double *vy, const double *vz,
                    const double *cs) {
   size_t n = sizeof(real) * ncell();
+  /* host code announces the Fields it writes (OUTPUT) and reads (INPUT):
+   * FARGO3D's freshness protocol, fresh.c */
+  OUTPUT(Fluids[f]->Density);
+  OUTPUT(Fluids[f]->Vx);
+  OUTPUT(Fluids[f]->Vy);
+#ifdef Z
+  OUTPUT(Fluids[f]->Vz);
+#endif
+  OUTPUT(Fluids[f]->Energy);
   if (rho) memcpy(Fluids[f]->Density->field_cpu, rho, n);
   if (vx) memcpy(Fluids[f]->Vx->field_cpu, vx, n);
   if (vy) memcpy(Fluids[f]->Vy->field_cpu, vy, n);
@@ -485,11 +502,18 @@ void ref_set_state(int f, const double *rho, const double *vx, const double *vy,
 /* the fluid's Energy field: the internal energy (ADIABATIC) or the sound
  * speed (ISOTHERMAL) */
 void ref_get_energy(int f, double *e) {
+  INPUT(Fluids[f]->Energy);
   memcpy(e, Fluids[f]->Energy->field_cpu, sizeof(real) * ncell());
 }
 
 void ref_get_state(int f, double *rho, double *vx, double *vy, double *vz) {
   size_t n = sizeof(real) * ncell();
+  INPUT(Fluids[f]->Density);
+  INPUT(Fluids[f]->Vx);
+  INPUT(Fluids[f]->Vy);
+#ifdef Z
+  INPUT(Fluids[f]->Vz);
+#endif
   if (rho) memcpy(rho, Fluids[f]->Density->field_cpu, n);
   if (vx) memcpy(vx, Fluids[f]->Vx->field_cpu, n);
   if (vy) memcpy(vy, Fluids[f]->Vy->field_cpu, n);
@@ -528,6 +552,7 @@ double ref_step(double DTint) {
   return dt;
 #endif
   if (g_dtemp >= DTint) g_dtemp = 0.0;
+  DT = DTint;
 #ifdef X
   MULTIFLUID(ComputeVmed(Vx));
 #endif
