@@ -366,6 +366,8 @@ def run_ours(args, rank, world, local_rank):
     inits = [[initial_state(c, f) for f in range(nf)] for c in cfgs]   # [disk][fluid]
     if batched:
         runner = Batch(cfgs, precision, device=local_rank)
+        if args.chains:
+            runner.set_chains(args.chains)
         for i, sts in enumerate(inits):
             for f, st in enumerate(sts):
                 runner.set_state(i, *st, fluid=f)
@@ -417,6 +419,8 @@ def run_ours(args, rank, world, local_rank):
     prof.pop("host_scalars", None)
     count.pop("host_scalars", None)
     launches_per_step = sum(KERNELS_PER_GROUP[dim].get(k, 1) * count[k] for k in prof)
+    if batched:   # every chain that holds disks launches its own groups
+        launches_per_step *= min(runner.chains(), len(cfgs))
     dom = max((k for k in prof if LAUNCH_WORDS[dim].get(k, 0) > 0), key=lambda k: prof[k])
     hbm, peak_kind = peaks()
     # a group's time covers all its fluids: its words per cell, once per fluid
@@ -461,7 +465,8 @@ def run_ours(args, rank, world, local_rank):
                    "active_cells_per_gpu": cells,
                    "disk_seeds": [c.seed for c in cfgs] if batched else [cfgs[0].seed],
                    "parallelism": "independent disks per GPU (no collective)" if world > 1 else "one GPU",
-                   "mode": "batched launches + CUDA graph" if batched else "plain, one disk",
+                   "mode": ("batched launches + CUDA graph, %s concurrent chains" % (args.chains or "default")
+                            if batched else "plain, one disk"),
                    "l2": "state (%d MB) larger than L2 (126 MB); no flush needed" % (nstored * esz * 5 // 2 ** 20)},
         "e2e": {"value": total_cells * args.steps / t_e2e, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": (5 if dim == "3d" else 4) * nstored * 8 / args.steps,
@@ -606,6 +611,8 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-vs-FP64 error leg of the default run")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg (profiling runs)")
+    ap.add_argument("--chains", type=int, default=0,
+                    help="batched: concurrent step chains (0 = the library's default; 1 for per-launch profiles)")
     ap.add_argument("--plan", action="store_true",
                     help="print every rank's share of the workload and exit (no GPU work; gloo when N > 1)")
     args = ap.parse_args()

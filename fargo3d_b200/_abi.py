@@ -145,6 +145,8 @@ def bind_batch(L):
     L.fb_batch_capacity.argtypes = [C.c_void_p]
     L.fb_batch_poll.argtypes = [C.c_void_p, C.POINTER(C.c_int), _D, C.POINTER(C.c_longlong)]
     L.fb_batch_set_tiles.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+    L.fb_batch_set_chains.argtypes = [C.c_void_p, C.c_int]
+    L.fb_batch_get_chains.argtypes = [C.c_void_p]
     L.fb_disk_set_tiles.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.fb_disk_get_tiles.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L._batch_bound = True

@@ -95,6 +95,13 @@ class Batch:
         _abi.check(_abi.lib().fb_disk_mass(self._members[i]._h, fluid, C.byref(m)))
         return m.value
 
+    def set_chains(self, chains: int):
+        """Step the disks as this many concurrent groups (streams); 1..8."""
+        _abi.check(_abi.lib().fb_batch_set_chains(self._h, chains))
+
+    def chains(self) -> int:
+        return _abi.lib().fb_batch_get_chains(self._h)
+
     def set_tiles(self, i, sweep_x_cells: int = 0, col_segment: int = 0):
         _abi.check(_abi.lib().fb_batch_set_tiles(self._h, i, sweep_x_cells, col_segment))
 

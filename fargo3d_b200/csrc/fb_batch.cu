@@ -20,18 +20,68 @@
 
 #include <stdio.h>
 
+#include <algorithm>
+
 Prof *g_prof = nullptr;
 
-extern "C" int fb_batch_launch_step_f64(fb_batch *B, double DT);
-extern "C" int fb_batch_launch_step_f32(fb_batch *B, double DT);
+extern "C" int fb_batch_launch_step_f64(fb_batch *B, double DT, int chain);
+extern "C" int fb_batch_launch_step_f32(fb_batch *B, double DT, int chain);
 extern "C" size_t fb_batch_sweep_x_esz_f32(void);
 // fb_host.c: lend a region of one batch-wide allocation and the batch's
 // stream to the next fb_disk_create on this thread
 extern "C" void fb_disk_internal_provide(void *arena, size_t size, void *stream);
 extern "C" size_t fb_disk_internal_arena_bytes(const fb_params *p, int precision);
 
-static int launch_step_any(fb_batch *B, double DT) {
-  return B->precision == FB_FP64 ? fb_batch_launch_step_f64(B, DT) : fb_batch_launch_step_f32(B, DT);
+static int launch_step_chain(fb_batch *B, double DT, int chain) {
+  return B->precision == FB_FP64 ? fb_batch_launch_step_f64(B, DT, chain) : fb_batch_launch_step_f32(B, DT, chain);
+}
+
+// nsteps steps of every active disk.  With several chains the batch's stream
+// forks into the chains' streams, each runs its disks' nsteps steps, and the
+// batch's stream joins them: the chains share no data, so they need no
+// ordering between one another inside the run (also when captured).
+static int launch_steps(fb_batch *B, double DT, int nsteps) {
+  int e = 0;
+  if (B->nchains <= 1) {
+    for (int s = 0; s < nsteps && !e; s++) e = launch_step_chain(B, DT, -1);
+    return e;
+  }
+  if ((e = (int)cudaEventRecord(B->ev_fork, B->stream))) return e;
+  for (int c = 0; c < B->nchains && !e; c++) {
+    if (c > 0 && (e = (int)cudaStreamWaitEvent(B->cstream[c], B->ev_fork, 0))) break;
+    for (int s = 0; s < nsteps && !e; s++) e = launch_step_chain(B, DT, c);
+    if (!e && c > 0) {
+      if ((e = (int)cudaEventRecord(B->ev_join[c], B->cstream[c]))) break;
+      e = (int)cudaStreamWaitEvent(B->stream, B->ev_join[c], 0);
+    }
+  }
+  return e;
+}
+
+static void free_lists(fb_batch *B) {
+  for (int s = 0; s < ST_N; s++) {
+    if (B->items[s]) cudaFree(B->items[s]);
+    B->items[s] = nullptr;
+    B->nitems[s] = 0;
+  }
+  for (int c = 0; c < FB_MAX_CHAINS; c++) {
+    for (int s = 0; s < ST_N; s++) {
+      if (B->citems[c][s]) cudaFree(B->citems[c][s]);
+      B->citems[c][s] = nullptr;
+      B->ncitems[c][s] = 0;
+    }
+    if (B->cdisks[c]) cudaFree(B->cdisks[c]);
+    B->cdisks[c] = nullptr;
+    B->ncdisks[c] = 0;
+  }
+}
+
+static int upload_list(int4 **dst, int *n, int count, const std::vector<int4> &v) {
+  *n = count;
+  if (count <= 0) return FB_OK;
+  if (cudaMalloc(dst, sizeof(int4) * v.size()) != cudaSuccess) return FB_ERR_NOMEM;
+  cudaError_t e = cudaMemcpy(*dst, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? FB_OK : fb_internal_fail(FB_ERR_CUDA, "work list upload", (int)e);
 }
 
 // Work lists, chunk width and shared-memory size for the active set; drops
@@ -39,11 +89,7 @@ static int launch_step_any(fb_batch *B, double DT) {
 static int rebuild(fb_batch *B) {
   if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
   B->graph_steps = 0;
-  for (int s = 0; s < ST_N; s++) {
-    if (B->items[s]) cudaFree(B->items[s]);
-    B->items[s] = nullptr;
-    B->nitems[s] = 0;
-  }
+  free_lists(B);
   std::vector<const fb_disk_dev *> act;
   for (int i = 0; i < B->n; i++)
     if (B->state[i] == 2) act.push_back(fb_disk_internal_dev(B->disks[i]));
@@ -61,13 +107,47 @@ static int rebuild(fb_batch *B) {
                              B->precision == FB_FP64 ? 8 : fb_batch_sweep_x_esz_f32());
     if (s > B->smem_x[k]) B->smem_x[k] = s;
   }
+  int rc;
   for (int s = 0; s < ST_N; s++) {
     std::vector<int4> v;
-    B->nitems[s] = tiles(B, s, v);
-    if (B->nitems[s] > 0) {
-      if (cudaMalloc(&B->items[s], sizeof(int4) * v.size()) != cudaSuccess) return FB_ERR_NOMEM;
-      cudaError_t e = cudaMemcpy(B->items[s], v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice);
-      if (e != cudaSuccess) return fb_internal_fail(FB_ERR_CUDA, "work list upload", (int)e);
+    const int cnt = tiles(B, s, v);
+    if ((rc = upload_list(&B->items[s], &B->nitems[s], cnt, v))) return rc;
+  }
+  // chains: the largest disks first, each to the chain with the fewest cells
+  B->chain_of.assign(B->n, -1);
+  if (B->nchains > 1) {
+    std::vector<int> order;
+    for (int i = 0; i < B->n; i++)
+      if (B->state[i] == 2) order.push_back(i);
+    auto cells = [&](int i) {
+      const fb_disk_dev &D = *fb_disk_internal_dev(B->disks[i]);
+      return (long long)D.nx * D.ny * (D.is3d ? D.nz : 1);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cells(a) > cells(b); });
+    long long load[FB_MAX_CHAINS] = {0};
+    std::vector<int> members[FB_MAX_CHAINS];
+    for (int i : order) {
+      int c = 0;
+      for (int k = 1; k < B->nchains; k++)
+        if (load[k] < load[c]) c = k;
+      B->chain_of[i] = c;
+      load[c] += cells(i);
+      members[c].push_back(i);
+    }
+    for (int c = 0; c < B->nchains; c++) {
+      std::sort(members[c].begin(), members[c].end());
+      B->ncdisks[c] = (int)members[c].size();
+      if (!members[c].empty()) {
+        if (cudaMalloc(&B->cdisks[c], sizeof(int) * members[c].size()) != cudaSuccess) return FB_ERR_NOMEM;
+        if (cudaMemcpy(B->cdisks[c], members[c].data(), sizeof(int) * members[c].size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+          return FB_ERR_CUDA;
+      }
+      for (int s = 0; s < ST_N; s++) {
+        std::vector<int4> v;
+        const int cnt = tiles(B, s, v, c);
+        if ((rc = upload_list(&B->citems[c][s], &B->ncitems[c][s], cnt, v))) return rc;
+      }
     }
   }
   return FB_OK;
@@ -79,9 +159,15 @@ int fb_batch_destroy(fb_batch *B) {
   if (!B) return FB_OK;
   cudaSetDevice(B->device);
   if (B->stream) cudaStreamSynchronize(B->stream);
+  for (int c = 1; c < FB_MAX_CHAINS; c++)
+    if (B->cstream[c]) cudaStreamSynchronize(B->cstream[c]);
   if (B->exec) cudaGraphExecDestroy(B->exec);
-  for (int s = 0; s < ST_N; s++)
-    if (B->items[s]) cudaFree(B->items[s]);
+  free_lists(B);
+  for (int c = 1; c < FB_MAX_CHAINS; c++) {
+    if (B->cstream[c]) cudaStreamDestroy(B->cstream[c]);
+    if (B->ev_join[c]) cudaEventDestroy(B->ev_join[c]);
+  }
+  if (B->ev_fork) cudaEventDestroy(B->ev_fork);
   if (B->d_disks) cudaFree(B->d_disks);
   if (B->d_psys) cudaFree(B->d_psys);
   for (fb_disk *d : B->disks)
@@ -105,10 +191,19 @@ int fb_batch_create_slots(int capacity, int precision, int device, int is3d, int
   B->t_end.assign(capacity, 0.0);
   B->disks.assign(capacity, nullptr);
   if (cudaSetDevice(device) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&B->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
     fb_batch_destroy(B);
     return FB_ERR_CUDA;
   }
+  B->cstream[0] = B->stream;
+  for (int c = 1; c < FB_MAX_CHAINS; c++)
+    if (cudaStreamCreateWithFlags(&B->cstream[c], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&B->ev_join[c], cudaEventDisableTiming) != cudaSuccess) {
+      fb_batch_destroy(B);
+      return FB_ERR_CUDA;
+    }
+  B->nchains = precision == FB_FP32 ? FB_DEFAULT_CHAINS_F32 : FB_DEFAULT_CHAINS_F64;
   if (cudaMalloc(&B->d_disks, sizeof(fb_disk_dev) * capacity) != cudaSuccess ||
       cudaMalloc(&B->d_psys, sizeof(fb_psys) * capacity) != cudaSuccess) {
     fb_batch_destroy(B);
@@ -253,8 +348,9 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
     if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
     cudaGraph_t g;
     if (cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FB_ERR_CUDA;
-    for (int s = 0; s < chunk; s++) launch_step_any(B, DT);
+    const int le = launch_steps(B, DT, chunk);
     cudaError_t e = cudaStreamEndCapture(B->stream, &g);
+    if (le && e == cudaSuccess) { cudaGraphDestroy(g); return fb_internal_fail(FB_ERR_CUDA, "step graph capture", le); }
     if (e != cudaSuccess) return fb_internal_fail(FB_ERR_CUDA, "step graph capture", (int)e);
     if (cudaGraphInstantiate(&B->exec, g, 0) != cudaSuccess) { cudaGraphDestroy(g); return FB_ERR_CUDA; }
     cudaGraphDestroy(g);
@@ -267,12 +363,24 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
     if (e != cudaSuccess) return fb_internal_fail(FB_ERR_CUDA, "cudaGraphLaunch", (int)e);
     done += chunk;
   }
-  for (; done < nsteps; done++) {
-    int e = launch_step_any(B, DT);
+  if (done < nsteps) {
+    int e = launch_steps(B, DT, nsteps - done);
     if (e) return fb_internal_fail(FB_ERR_CUDA, "batched step launch", e);
   }
   return FB_OK;
 }
+
+int fb_batch_set_chains(fb_batch *B, int chains) {
+  if (!B || chains < 1 || chains > FB_MAX_CHAINS) return FB_ERR_ARG;
+  if (cudaSetDevice(B->device) != cudaSuccess || cudaStreamSynchronize(B->stream) != cudaSuccess) return FB_ERR_CUDA;
+  if (chains != B->nchains) {
+    B->nchains = chains;
+    B->dirty = 1;
+  }
+  return FB_OK;
+}
+
+int fb_batch_get_chains(fb_batch *B) { return B ? B->nchains : FB_ERR_ARG; }
 
 int fb_batch_sync(fb_batch *B) {
   if (!B) return FB_ERR_ARG;
@@ -329,7 +437,7 @@ int fb_batch_profile_step(fb_batch *B, double DT, float *ms, const char **names,
   Prof P;
   P.n = 0;
   g_prof = &P;
-  int rc = launch_step_any(B, DT);
+  int rc = launch_step_chain(B, DT, -1);   // one chain: the launch groups in order
   g_prof = nullptr;
   if (rc) return FB_ERR_CUDA;
   cudaEventSynchronize(P.ev[P.n - 1]);

@@ -41,6 +41,20 @@ constexpr int SRC2_TX = 32, SRC2_TY = 8, SRC3_TX = 32, SRC3_TY = 4, COL_BX = 128
 #ifndef FB_SX_MINB32
 #define FB_SX_MINB32 4
 #endif
+// FP32 2D CFL, NewVelocity and column sweep (kb_cfl_cyl32, kb_newvel_cyl32,
+// kb_sweep_col32): 6, 8 and 8 CTAs of 128 threads per SM (80, 64 and 64
+// registers).  Measured on the batched 64-disk step against the unconstrained
+// builds (147, 128 and 128 registers): CFL 0.090 -> 0.061 ms, NewVelocity
+// 0.088 -> 0.078 ms, column sweep 0.164 -> 0.135 ms (segments of 4 rows).
+#ifndef FB_CFL32_MINB
+#define FB_CFL32_MINB 6
+#endif
+#ifndef FB_NV32_MINB
+#define FB_NV32_MINB 8
+#endif
+#ifndef FB_COL32_MINB
+#define FB_COL32_MINB 8
+#endif
 #ifndef FB_COL_MINB32
 #define FB_COL_MINB32 4
 #endif
@@ -113,7 +127,7 @@ __global__ void __launch_bounds__(256) kb_cfl(const fb_disk_dev *ds, const int4 
 }
 
 // FP32 2D: 128 columns x CFL32_R rows a tile (fb_sources32.cuh)
-static __global__ void __launch_bounds__(128) kb_cfl_cyl32(const fb_disk_dev *ds, const int4 *items, int f) {
+static __global__ void __launch_bounds__(128, FB_CFL32_MINB) kb_cfl_cyl32(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   b_cfl_cyl32(dims_of(D), geo_of<float>(D.geom), (const float *)F.rho, (const float *)F.cs, (const float *)F.vx,
               (const float *)F.vy, F.vxmed, F.vbg, (float)scp->nu, (float)scp->alpha, D.cfl, D.mindx,
@@ -162,6 +176,15 @@ __global__ void __launch_bounds__(128) kb_collisions(const fb_disk_dev *ds, cons
   b_collisions<T, N, S>(D, dims_of(D), geo_of<double>(D.geomd), D.scal_dev, make_uint3(w.y, w.z, w.w));
 }
 
+// FP32 2D disks: the radial sweep of fb_sources32.cuh
+template <int COL_NS>
+static __global__ void __launch_bounds__(COL_BX, FB_COL32_MINB) kb_sweep_col32(const fb_disk_dev *ds, const int4 *items, int f) {
+  FB_TILE
+  b_sweep_col32<COL_NS>(dims_of(D), geo_of<float>(D.geom), (const float *)F.rho, (const float *)F.vxt,
+                        (const float *)F.vyt, (const float *)F.dlb_y, FB_NGH - 1, D.ny + FB_NGH - 1, (float *)F.rho_a,
+                        (float *)F.mpx, (float *)F.mmx, (float *)F.mpy, (float *)F.mmy, scp, bid);
+}
+
 template <typename T, int DIR, int COL_NS, typename S>
 __global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? FB_COL_MINB32 : 1) kb_sweep_col(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
@@ -180,11 +203,7 @@ __global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? FB_COL_MINB32 : 1) kb
     src.q[3] = (const S *)F.mmy; src.q[4] = (const S *)F.mpz; src.q[5] = (const S *)F.mmz;
     src.from_v = 0;
   }
-  if (!m.is3d && sizeof(S) == 4 && sizeof(T) == 4) {   // FP32 2D (fb_sources32.cuh)
-    b_sweep_col32<COL_NS>(m, geo_of<float>(D.geom), (const float *)F.rho, (const float *)F.vxt, (const float *)F.vyt,
-                          (const float *)F.dlb_y, ylo, yhi, (float *)F.rho_a, (float *)F.mpx, (float *)F.mmx,
-                          (float *)F.mpy, (float *)F.mmy, scp, bid);
-  } else if (!m.is3d) {
+  if (!m.is3d) {
     b_sweep_col<T, 0, COL_NS, S>(m, geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), src, 4, ylo, yhi, 0, (S *)F.rho_a, (S *)F.mpx, (S *)F.mmx,
                               (S *)F.mpy, (S *)F.mmy, nullptr, nullptr, scp, bid);
   } else if (DIR == 1) {
@@ -227,7 +246,7 @@ __global__ void __launch_bounds__(NV_BX) kb_newvel(const fb_disk_dev *ds, const 
 }
 
 // FP32 2D: column-marching rows (fb_sources32.cuh); 128 columns x NV32_R rows a tile
-static __global__ void __launch_bounds__(128) kb_newvel_cyl32(const fb_disk_dev *ds, const int4 *items, int f) {
+static __global__ void __launch_bounds__(128, FB_NV32_MINB) kb_newvel_cyl32(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   b_newvel_cyl32(dims_of(D), geo_of<float>(D.geom), (const float *)F.rho_a, (const float *)F.mpx,
                  (const float *)F.mmx, (const float *)F.mpy, (const float *)F.mmy, (float *)F.rho, (float *)F.vx,
@@ -235,15 +254,17 @@ static __global__ void __launch_bounds__(128) kb_newvel_cyl32(const fb_disk_dev 
                  D.stockholm, scp, bid);
 }
 
-// The scalar work of the step for every disk, one thread per disk; then the
+// The scalar work of the step for every disk of the list dl (all n disks when
+// dl is null), one thread per disk; then the
 // CFL minimum is reset for the next step.  dtmin[1] carries the kernels'
 // non-finite flag.  A disk with an end time uses it as its DT interval, so
 // its last step is clipped to land on it; that step still runs in full, and
 // the disk is frozen (FB_DONE) when the next step's scalar work finds it
 // there.  Empty slots (zeroed descriptors) are passed over.
-static __global__ void kb_scalars(const fb_disk_dev *ds, fb_psys *ps, int n, double DT) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+static __global__ void kb_scalars(const fb_disk_dev *ds, fb_psys *ps, const int *dl, int n, double DT) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = dl ? dl[t] : t;
   const fb_disk_dev &D = ds[i];
   if (D.nx == 0) return;
   unsigned long long *dm = (unsigned long long *)D.dtmin;
@@ -271,6 +292,13 @@ static __global__ void kb_scalars(const fb_disk_dev *ds, fb_psys *ps, int n, dou
 
 using namespace fb;
 
+#define FB_MAX_CHAINS 8
+/* FP32 batches step as 4 concurrent chains (measured: 0.741 ms -> 0.684 ms for
+   the 64-disk workload); FP64 batches, whose stage kernels fill the GPU on
+   their own, as one */
+#define FB_DEFAULT_CHAINS_F32 4
+#define FB_DEFAULT_CHAINS_F64 1
+
 // Slots: state[i] 0 empty, 1 reserved (created, not activated), 2 active.
 // n is the capacity; the work lists cover the active slots only.
 struct fb_batch {
@@ -285,15 +313,29 @@ struct fb_batch {
   fb_psys *d_psys;
   int4 *items[ST_N];
   int nitems[ST_N];
+  /* concurrent step chains: the active disks split into nchains groups of
+     about equal cells, each group stepped on its own stream with its own work
+     lists (chain c: citems[c], its disks cdisks[c]), so that one group's
+     latency-bound launches (the scalar step, reductions, boundaries, launch
+     tails) overlap another's throughput-bound ones */
+  int nchains;
+  cudaStream_t cstream[FB_MAX_CHAINS];
+  cudaEvent_t ev_fork, ev_join[FB_MAX_CHAINS];
+  int4 *citems[FB_MAX_CHAINS][ST_N];
+  int ncitems[FB_MAX_CHAINS][ST_N];
+  int *cdisks[FB_MAX_CHAINS];
+  int ncdisks[FB_MAX_CHAINS];
+  std::vector<int> chain_of;
   size_t smem_x[NXC];  /* shared memory of each chunk-width class of the azimuthal sweep */
   cudaGraphExec_t exec;
   int graph_steps;
   double graph_dt;
 };
 
-static int tiles(fb_batch *B, int st, std::vector<int4> &v) {
+static int tiles(fb_batch *B, int st, std::vector<int4> &v, int chain = -1) {
   for (int di = 0; di < B->n; di++) {
     if (B->state[di] != 2) continue;
+    if (chain >= 0 && B->chain_of[di] != chain) continue;
     const fb_disk_dev &D = *fb_disk_internal_dev(B->disks[di]);
     const int nx = D.nx, ny = D.ny, nz = D.nz, sy = D.sy, sz = D.sz;
     dim3 g(1, 1, 1);
@@ -375,38 +417,45 @@ static void pmark(cudaStream_t st, const char *name) {
 // T: compute type of the source stage; TC, TX, TN, TF: of the column sweeps,
 // the azimuthal sweep, NewVelocity and the CFL's per-cell limits (its
 // minimum is always FP64); S: storage type.
+// chain < 0: every active disk on the batch's stream (one chain); else the
+// disks of that chain on its stream.
 template <typename T, typename S, typename TC = T, typename TX = T, typename TN = T, typename TF = T>
-static int launch_step(fb_batch *B, double DT) {
-  if (B->nitems[ST_CFL] == 0) return 0;  // no active disk
+static int launch_step(fb_batch *B, double DT, int chain) {
+  int4 *const *items = chain < 0 ? B->items : B->citems[chain];
+  const int *nitems = chain < 0 ? B->nitems : B->ncitems[chain];
+  if (nitems[ST_CFL] == 0) return 0;  // no active disk
   configure_sweep_x<TX, S>(B);
-  cudaStream_t st = B->stream;
+  cudaStream_t st = chain < 0 ? B->stream : B->cstream[chain];
   pmark(st, "start");
   const fb_disk_dev *ds = B->d_disks;
   const int nf = B->nfluids;
-  auto grid = [&](int s) { return dim3((unsigned)B->nitems[s]); };
+  auto grid = [&](int s) { return dim3((unsigned)nitems[s]); };
   for (int f = 0; f < nf; f++) {
-    if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
-    else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 0);
+    if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, items[ST_ROWSUM], f, 0);
+    else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, items[ST_ROWSUM], f, 0);
   }
   pmark(st, "rowsum");
   for (int f = 0; f < nf; f++) {
-    if (!B->is3d && sizeof(S) == 4) kb_cfl_cyl32<<<grid(ST_CFL), 128, 0, st>>>(ds, B->items[ST_CFL], f);
-    else kb_cfl<TF, S><<<grid(ST_CFL), 256, 0, st>>>(ds, B->items[ST_CFL], f);
+    if (!B->is3d && sizeof(S) == 4) kb_cfl_cyl32<<<grid(ST_CFL), 128, 0, st>>>(ds, items[ST_CFL], f);
+    else kb_cfl<TF, S><<<grid(ST_CFL), 256, 0, st>>>(ds, items[ST_CFL], f);
   }
   pmark(st, "cfl");
-  kb_scalars<<<(B->n + 63) / 64, 64, 0, st>>>(ds, B->d_psys, B->n, DT);
+  {
+    const int nd = chain < 0 ? B->n : B->ncdisks[chain];
+    kb_scalars<<<(nd + 63) / 64, 64, 0, st>>>(ds, B->d_psys, chain < 0 ? nullptr : B->cdisks[chain], nd, DT);
+  }
   pmark(st, "scalars");
   for (int f = 0; f < nf; f++) {
-    if (B->is3d) kb_sources_sph<T, S><<<grid(ST_SOURCES), dim3(SRC3_TX, SRC3_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
-    else if (sizeof(S) == 4) kb_sources_cyl32<<<grid(ST_SOURCES), S32_WARPS * 32, 0, st>>>(ds, B->items[ST_SOURCES], f);
-    else kb_sources_cyl<T, S><<<grid(ST_SOURCES), dim3(SRC2_TX, SRC2_TY), 0, st>>>(ds, B->items[ST_SOURCES], f);
+    if (B->is3d) kb_sources_sph<T, S><<<grid(ST_SOURCES), dim3(SRC3_TX, SRC3_TY), 0, st>>>(ds, items[ST_SOURCES], f);
+    else if (sizeof(S) == 4) kb_sources_cyl32<<<grid(ST_SOURCES), S32_WARPS * 32, 0, st>>>(ds, items[ST_SOURCES], f);
+    else kb_sources_cyl<T, S><<<grid(ST_SOURCES), dim3(SRC2_TX, SRC2_TY), 0, st>>>(ds, items[ST_SOURCES], f);
     pmark(st, "sources");
-    if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 1, 1);
-    kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 1, 0);
+    if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, items[ST_BND_Z], f, 1, 1);
+    kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, items[ST_BND_Y], f, 1, 0);
     pmark(st, "bnd_vtemp");
   }
-  if (nf > 1 && B->nitems[ST_COLL]) {  // implicit drag between the fluids
-    const int4 *it = B->items[ST_COLL];
+  if (nf > 1 && nitems[ST_COLL]) {  // implicit drag between the fluids
+    const int4 *it = items[ST_COLL];
     switch (nf) {
       case 2: kb_collisions<T, 2, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
       case 3: kb_collisions<T, 3, S><<<grid(ST_COLL), 128, 0, st>>>(ds, it); break;
@@ -419,22 +468,28 @@ static int launch_step(fb_batch *B, double DT) {
     pmark(st, "collisions");
   }
   for (int f = 0; f < nf; f++) {
-    if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
-    else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, B->items[ST_ROWSUM], f, 1);
+    if (B->precision == FB_FP64) kb_rowsum<T, true, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, items[ST_ROWSUM], f, 1);
+    else kb_rowsum<T, false, S><<<grid(ST_ROWSUM), 256, 0, st>>>(ds, items[ST_ROWSUM], f, 1);
     pmark(st, "rowsum_vtemp");
     if (B->is3d) {
-      if (B->nitems[ST_Z4]) kb_sweep_col<TC, 1, 4, S><<<grid(ST_Z4), COL_BX, 0, st>>>(ds, B->items[ST_Z4], f);
-      if (B->nitems[ST_Z8]) kb_sweep_col<TC, 1, 8, S><<<grid(ST_Z8), COL_BX, 0, st>>>(ds, B->items[ST_Z8], f);
-      if (B->nitems[ST_Z16]) kb_sweep_col<TC, 1, 16, S><<<grid(ST_Z16), COL_BX, 0, st>>>(ds, B->items[ST_Z16], f);
+      if (nitems[ST_Z4]) kb_sweep_col<TC, 1, 4, S><<<grid(ST_Z4), COL_BX, 0, st>>>(ds, items[ST_Z4], f);
+      if (nitems[ST_Z8]) kb_sweep_col<TC, 1, 8, S><<<grid(ST_Z8), COL_BX, 0, st>>>(ds, items[ST_Z8], f);
+      if (nitems[ST_Z16]) kb_sweep_col<TC, 1, 16, S><<<grid(ST_Z16), COL_BX, 0, st>>>(ds, items[ST_Z16], f);
     }
-    if (B->nitems[ST_Y4]) kb_sweep_col<TC, 0, 4, S><<<grid(ST_Y4), COL_BX, 0, st>>>(ds, B->items[ST_Y4], f);
-    if (B->nitems[ST_Y8]) kb_sweep_col<TC, 0, 8, S><<<grid(ST_Y8), COL_BX, 0, st>>>(ds, B->items[ST_Y8], f);
-    if (B->nitems[ST_Y16]) kb_sweep_col<TC, 0, 16, S><<<grid(ST_Y16), COL_BX, 0, st>>>(ds, B->items[ST_Y16], f);
+    if (!B->is3d && sizeof(S) == 4 && sizeof(TC) == 4) {   // FP32 2D
+      if (nitems[ST_Y4]) kb_sweep_col32<4><<<grid(ST_Y4), COL_BX, 0, st>>>(ds, items[ST_Y4], f);
+      if (nitems[ST_Y8]) kb_sweep_col32<8><<<grid(ST_Y8), COL_BX, 0, st>>>(ds, items[ST_Y8], f);
+      if (nitems[ST_Y16]) kb_sweep_col32<16><<<grid(ST_Y16), COL_BX, 0, st>>>(ds, items[ST_Y16], f);
+    } else {
+      if (nitems[ST_Y4]) kb_sweep_col<TC, 0, 4, S><<<grid(ST_Y4), COL_BX, 0, st>>>(ds, items[ST_Y4], f);
+      if (nitems[ST_Y8]) kb_sweep_col<TC, 0, 8, S><<<grid(ST_Y8), COL_BX, 0, st>>>(ds, items[ST_Y8], f);
+      if (nitems[ST_Y16]) kb_sweep_col<TC, 0, 16, S><<<grid(ST_Y16), COL_BX, 0, st>>>(ds, items[ST_Y16], f);
+    }
     pmark(st, "sweep_cols");
     for (int k = 0; k < NXC; k++) {
-      const int n = B->nitems[ST_X1 + k];
+      const int n = nitems[ST_X1 + k];
       if (!n) continue;
-      const int4 *it = B->items[ST_X1 + k];
+      const int4 *it = items[ST_X1 + k];
       const size_t sm = B->smem_x[k];
       switch (k) {
         case 4: kb_sweep_x<TX, 16, S><<<n, 256, sm, st>>>(ds, it, f); break;
@@ -447,11 +502,11 @@ static int launch_step(fb_batch *B, double DT) {
     pmark(st, "sweep_x");
   }
   for (int f = 0; f < nf; f++) {
-    if (!B->is3d && sizeof(S) == 4) kb_newvel_cyl32<<<grid(ST_NEWVEL), 128, 0, st>>>(ds, B->items[ST_NEWVEL], f);
-    else kb_newvel<TN, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, B->items[ST_NEWVEL], f);
+    if (!B->is3d && sizeof(S) == 4) kb_newvel_cyl32<<<grid(ST_NEWVEL), 128, 0, st>>>(ds, items[ST_NEWVEL], f);
+    else kb_newvel<TN, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, items[ST_NEWVEL], f);
     pmark(st, "newvel");
-    if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, B->items[ST_BND_Z], f, 0, 1);
-    kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, B->items[ST_BND_Y], f, 0, 0);
+    if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, items[ST_BND_Z], f, 0, 1);
+    kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, items[ST_BND_Y], f, 0, 0);
     pmark(st, "bnd");
   }
   return (int)cudaGetLastError();

@@ -15,8 +15,8 @@
 #ifndef FB_TF
 #define FB_TF float
 #endif
-extern "C" int fb_batch_launch_step_f32(fb_batch *B, double DT) {
-  return launch_step<double, float, FB_TC, FB_TX, FB_TN, FB_TF>(B, DT);
+extern "C" int fb_batch_launch_step_f32(fb_batch *B, double DT, int chain) {
+  return launch_step<double, float, FB_TC, FB_TX, FB_TN, FB_TF>(B, DT, chain);
 }
 // element size of the azimuthal sweep's shared-memory rings
 extern "C" size_t fb_batch_sweep_x_esz_f32(void) { return sizeof(FB_TX); }

@@ -242,6 +242,14 @@ int fb_disk_set_tiles(fb_disk *d, int sweep_x_cells, int col_segment);
 int fb_disk_set_wait_limit(fb_disk *d, long long polls);
 int fb_disk_get_tiles(fb_disk *d, int *sweep_x_cells, int *col_segment);
 int fb_batch_set_tiles(fb_batch *b, int slot, int sweep_x_cells, int col_segment);
+/* Concurrent step chains (1..8; default 4 for FP32 batches, 1 for FP64): the
+ * active disks are split into
+ * this many groups of about equal cells, each stepped on its own stream, so
+ * that the latency-bound launches of one group (the per-disk scalar step,
+ * reductions, ghost fills, launch tails) overlap the others' stencil work.
+ * Results do not depend on it (each disk's arithmetic is the same). */
+int fb_batch_set_chains(fb_batch *b, int chains);
+int fb_batch_get_chains(fb_batch *b);
 
 /* Device bytes: an upper bound of what fb_disk_create requests for these
  * parameters, and what a disk actually requested. */

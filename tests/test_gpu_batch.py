@@ -88,6 +88,31 @@ def test_batch_member_alone_equals_in_mix(precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_concurrent_chains_give_the_same_bits(precision):
+    """The disks stepped as 1, 3 or 8 concurrent chains (streams), through
+    the captured graph (10 steps) and the eager remainder (3 steps): every
+    member's state and scalars are the same bits."""
+    from fargo3d_b200 import Batch
+    cfgs = small_mix()
+    out = {}
+    for k in (1, 3, 8):
+        b = Batch(cfgs, precision)
+        b.load_initial_states()
+        b.set_chains(k)
+        b.run(13)
+        b.sync()
+        out[k] = [(b.state(i), list(b.scalars(i)[0])) for i in range(len(cfgs))]
+        b.close()
+    for k in (3, 8):
+        for i in range(len(cfgs)):
+            (a, sa), (r, sr) = out[k][i], out[1][i]
+            assert sa == sr, (k, i)
+            for key in ("rho", "vx", "vy"):
+                assert np.array_equal(a[key], r[key]), (k, i, key)
+
+
+@pytest.mark.gpu
 def test_batch_failing_member_is_frozen_others_continue():
     """Fault injection on the host: one member starts with a NaN density.
     It is frozen with FB_ERR_NONFINITE; the others match their solo runs."""
