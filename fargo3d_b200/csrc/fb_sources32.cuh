@@ -314,14 +314,13 @@ static __global__ void __launch_bounds__(128) k_newvel_cyl32(Dims m, Geo<float> 
 // ---------------------------------------------------------------------------
 // The radial sweep of FP32 2D disks (TransportY, transport.c:24-46, for the
 // density and the four momenta; vanleer_y_a/_b, divrho, update_y,
-// update_density_y): b_sweep_col's work with every per-row factor formed once
-// per thread -- the zone sizes and their reciprocals, the face areas and the
-// cell updates for the uniform azimuthal spacing -- and the specific momenta
-// taken directly as v R or v (DivideByRho of rho v R is v R), so the only
-// division per cell and quantity is the limiter's harmonic mean.  Table
-// indices are clamped like the field rows (cells past chi + 2 never reach an
-// output).  The azimuthal momenta are frame- and background-relative as in
-// b_sweep_col.
+// update_density_y): b_sweep_col's work with the per-row factors formed from
+// the row tables -- the zone sizes and their reciprocals, the face areas and
+// the cell updates for the uniform azimuthal spacing -- and the specific
+// momenta taken directly as v R or v (DivideByRho of rho v R is v R), so the
+// only division per cell and quantity is the limiter's harmonic mean.  A
+// thread marches down a segment of NS rows of one column.  The azimuthal
+// momenta are frame- and background-relative as in b_sweep_col.
 template <int NS>
 __device__ __forceinline__ void b_sweep_col32(const Dims m, const Geo<float> g, const float *__restrict__ rho,
     const float *__restrict__ vxt, const float *__restrict__ vyt, const float *__restrict__ dlb, int clo, int chi,
@@ -335,90 +334,102 @@ __device__ __forceinline__ void b_sweep_col32(const Dims m, const Geo<float> g, 
   const int cmax = chi + 2;
   const int ixp = i < m.nx - 1 ? i + 1 : 0;
   const float sxi0 = ld(g.sxi + 0), isxi0 = 1.0f / sxi0;
-  float r[NS + 4], izn[NS + 4], vel[NS + 1];
-  // zone_size_y = Ymin(j+1) - Ymin(j) of window cell w (a broadcast table load)
-  auto zn = [&](int w) -> float { return ld(g.sxj + min(c0 - 2 + w, cmax)); };
-#pragma unroll
-  for (int w = 0; w < NS + 4; w++) {
-    r[w] = rho[m.l(i, min(c0 - 2 + w, cmax), 0)];
-    izn[w] = 1.0f / zn(w);
-  }
-#pragma unroll
-  for (int f = 0; f < NS + 1; f++) vel[f] = vyt[m.l(i, min(c0 + f, cmax - 1), 0)];
-  // van Leer interface values of a window a[] (cells c0-2 .. c0+NS+1) at the
-  // faces c0 .. c0+NS; off[] (when given) are the neighbour differences of
-  // the offset the window leaves out
-  auto iface = [&](const float *a, const float *off, float *qs) {
-    float slope[NS + 2];
-#pragma unroll
-    for (int s2 = 0; s2 < NS + 2; s2++) {
-      float dqm = a[s2 + 1] - a[s2], dqp = a[s2 + 2] - a[s2 + 1];
-      if (off) { dqm += off[s2]; dqp += off[s2 + 1]; }
-      dqm *= izn[s2 + 1];
-      dqp *= izn[s2 + 2];
-      slope[s2] = (dqp * dqm <= 0.0f) ? 0.0f : 2.0f * dqp * dqm / (dqm + dqp);
-    }
-#pragma unroll
-    for (int f = 0; f < NS + 1; f++) {
-      if (vel[f] > 0.0f) qs[f] = a[f + 1] + 0.5f * (zn(f + 1) - vel[f] * dt) * slope[f];
-      else qs[f] = a[f + 2] - 0.5f * (zn(f + 2) + vel[f] * dt) * slope[f + 1];
-    }
+  // The thread marches down its column from face c0 to face c0 + NS, holding
+  // of every quantity only the cells around the current face: each cell is
+  // loaded once, its van Leer slope formed once and each face's interface
+  // value once (a window per segment would form them for the halo cells
+  // again).  Quantities: 0 rho, 1 vxt(i+1) R, 2 vxt(i) R, 3 vyt(c+1), 4 vyt(c)
+  // (momenta_x.c:76-85 relative, momenta_y.c:65-66, over rho); rows past
+  // cmax are clamped like the field rows and only feed faces and cells that
+  // are not stored.
+  auto load = [&](int c, float *A) {
+    const int rc = min(c, cmax);
+    const long long l = m.l(i, rc, 0);
+    const float ym = ld(g.ymed + rc);
+    A[0] = rho[l];
+    A[1] = vxt[m.l(ixp, rc, 0)] * ym;
+    A[2] = vxt[l] * ym;
+    A[3] = vyt[l + m.pitch];
+    A[4] = vyt[l];
   };
-  // face area factor (Surf_y over v rho*) at face c0 + f, and the cell
-  // update dt / Vol at cell c0 + u (broadcast table loads)
-  auto sf = [&](int f) -> float { return ld(g.syj + min(c0 + f, cmax)) * sxi0; };
-  auto fin = [&](int u) -> float { return dt * ld(g.invvj + min(c0 + u, cmax)) * isxi0; };
-  float rs[NS + 1];
-  iface(r, nullptr, rs);
-  // OMEGAFRAME (R^2(c) - R^2(c-1)) + (vbg R)(c) - (vbg R)(c-1)
-  auto dr2 = [&](int c) -> float { return of * ld(g.dr2_j + c) + (dlb ? ld(dlb + c) : 0.0f); };
-  float off[NS + 3];
+  // OMEGAFRAME (R^2(c) - R^2(c-1)) + (vbg R)(c) - (vbg R)(c-1): the
+  // neighbour difference of the offset the azimuthal momenta leave out
+  auto offr = [&](int c) -> float { return c <= cmax ? of * ld(g.dr2_j + c) + (dlb ? ld(dlb + c) : 0.0f) : 0.0f; };
+  auto zn = [&](int c) -> float { return ld(g.sxj + min(c, cmax)); };
+  // vanleer_y_a: the slope of cell c from cells c-1, c, c+1, the zone
+  // reciprocals of c and c+1 and (momenta 1, 2) the offsets of c and c+1
+  auto slope = [&](int q, float am, float a0, float ap, float offc, float offp, float izc, float izp) -> float {
+    float dqm = a0 - am, dqp = ap - a0;
+    if (q == 1 || q == 2) { dqm += offc; dqp += offp; }
+    dqm *= izc;
+    dqp *= izp;
+    return (dqp * dqm <= 0.0f) ? 0.0f : 2.0f * dqp * dqm / (dqm + dqp);
+  };
+  float Am[5], A0[5], Ap[5], slm[5], sl0[5], qsm[5], qs0[5];
+  load(c0 - 2, Am);
+  load(c0 - 1, A0);
+  load(c0, Ap);
+  float offm = offr(c0 - 1), off0 = offr(c0), offp;
+  float znm = zn(c0 - 1), zn0 = zn(c0), znp;
+  float iz0 = 1.0f / zn0, izp;
+  {
+    const float izm = 1.0f / znm;
 #pragma unroll
-  for (int w = 0; w < NS + 3; w++) {
-    const int c = c0 - 1 + w;
-    off[w] = c <= cmax ? dr2(c) : 0.0f;
+    for (int q = 0; q < 5; q++) slm[q] = slope(q, Am[q], A0[q], Ap[q], offm, off0, izm, iz0);
   }
-  float *qo[4] = {o_mpx, o_mmx, o_mpy, o_mmy};
+  // shift: cells c0-1, c0 become "previous" and "current"
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    float a[NS + 4], qs[NS + 1];
+  for (int q = 0; q < 5; q++) { Am[q] = A0[q]; A0[q] = Ap[q]; }
+  // now Am = A(c0-1), A0 = A(c0), slm = slope(c0-1), znm = zn(c0-1), zn0 = zn(c0),
+  // offm = off(c0-1), off0 = off(c0)
+  float velm = 0.0f, sfm = 0.0f;
 #pragma unroll
-    for (int w = 0; w < NS + 4; w++) {
-      const int c = min(c0 - 2 + w, cmax);
-      const long long l = m.l(i, c, 0);
-      // momenta_x.c:76-85 (relative), momenta_y.c:65-66, over rho
-      if (q == 0) a[w] = vxt[m.l(ixp, c, 0)] * ld(g.ymed + c);
-      else if (q == 1) a[w] = vxt[l] * ld(g.ymed + c);
-      else if (q == 2) a[w] = vyt[l + m.pitch];
-      else a[w] = vyt[l];
+  for (int s2 = 0; s2 <= NS; s2++) {
+    const int f = c0 + s2;   // the face between cells f-1 and f
+    load(f + 1, Ap);
+    offp = offr(f + 1);
+    znp = zn(f + 1);
+    izp = 1.0f / znp;
+#pragma unroll
+    for (int q = 0; q < 5; q++) sl0[q] = slope(q, Am[q], A0[q], Ap[q], off0, offp, iz0, izp);
+    // vanleer_y_b: interface values at face f, upwind by the face velocity
+    const float vel = A0[4];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      if (vel > 0.0f) qs0[q] = Am[q] + 0.5f * (znm - vel * dt) * slm[q];
+      else qs0[q] = A0[q] - 0.5f * (zn0 + vel * dt) * sl0[q];
     }
-    iface(a, q < 2 ? off : nullptr, qs);
-#pragma unroll
-    for (int u = 0; u < NS; u++) {
-      const int c = c0 + u;
+    const float sf0 = ld(g.syj + min(f, cmax)) * sxi0;
+    if (s2 > 0) {   // update_y / update_density_y of cell c = f - 1
+      const int c = f - 1;
       if (c <= chi) {
-        float qin = qs[u], qout = qs[u + 1];
-        if (q < 2) {
-          if (vel[u] > 0.0f) qin -= off[u + 1];            // upwind cell c-1
-          if (!(vel[u + 1] > 0.0f)) qout += off[u + 2];    // upwind cell c+1
+        const float fin = dt * ld(g.invvj + min(c, cmax)) * isxi0;
+        const long long l = m.l(i, c, 0);
+        float *qo[4] = {o_mpx, o_mmx, o_mpy, o_mmy};
+#pragma unroll
+        for (int q = 1; q < 5; q++) {
+          float qin = qsm[q], qout = qs0[q];
+          if (q <= 2) {
+            if (velm > 0.0f) qin -= offm;          // upwind cell c-1
+            if (!(vel > 0.0f)) qout += off0;       // upwind cell c+1
+          }
+          const float flux = velm * qin * qsm[0] * sfm - vel * qout * qs0[0] * sf0;
+          qo[q - 1][l] = Am[q] * Am[0] + flux * fin;
         }
-        const float flux = vel[u] * qin * rs[u] * sf(u) - vel[u + 1] * qout * rs[u + 1] * sf(u + 1);
-        qo[q][m.l(i, c, 0)] = a[u + 2] * r[u + 2] + flux * fin(u);
+        const float flux = velm * qsm[0] * sfm - vel * qs0[0] * sf0;
+        rho_out[l] = Am[0] + flux * fin;
       }
     }
-  }
 #pragma unroll
-  for (int u = 0; u < NS; u++) {
-    const int c = c0 + u;
-    if (c <= chi) {
-      const float flux = vel[u] * rs[u] * sf(u) - vel[u + 1] * rs[u + 1] * sf(u + 1);
-      rho_out[m.l(i, c, 0)] = r[u + 2] + flux * fin(u);
-    }
+    for (int q = 0; q < 5; q++) { Am[q] = A0[q]; A0[q] = Ap[q]; slm[q] = sl0[q]; qsm[q] = qs0[q]; }
+    velm = vel; sfm = sf0;
+    offm = off0; off0 = offp;
+    znm = zn0; zn0 = znp; iz0 = izp;
   }
 }
 
 template <int NS>
-static __global__ void __launch_bounds__(128, 4) k_sweep_col32(Dims m, Geo<float> g, const float *__restrict__ rho,
+static __global__ void __launch_bounds__(128, 8) k_sweep_col32(Dims m, Geo<float> g, const float *__restrict__ rho,
     const float *__restrict__ vxt, const float *__restrict__ vyt, const float *__restrict__ dlb, int clo, int chi,
     float *__restrict__ rho_out, float *__restrict__ o_mpx, float *__restrict__ o_mmx, float *__restrict__ o_mpy,
     float *__restrict__ o_mmy, const fb_scalars *__restrict__ scp) {
