@@ -1,8 +1,11 @@
 /*
  * fargo_oracle.c -- TEST INFRASTRUCTURE ONLY (see fargo_oracle.h).
  *
- * A CPU restatement of FARGO3D's hydro step, written from the equations and
- * loop bounds of the reference sources.  Each function names the reference
+ * A CPU restatement of FARGO3D's hydro step (isothermal 2D cylindrical and
+ * 3D spherical disks, several fluids with implicit drag, planets feeling the
+ * disk; the ADIABATIC equation of state and DUSTDIFFUSION on 2D cylindrical
+ * disks), written from the equations and loop bounds of the reference
+ * sources.  Each function names the reference
  * file:line it follows (paths relative to the reference's src/ directory).
  * Floating-point expressions keep the reference's evaluation order, including
  * the order implied by its un-parenthesised geometry macros (define.h:226-260),
@@ -45,6 +48,7 @@ struct fo_disk {
   double *pres, *pot, *mpx, *mmx, *mpy, *mmy, *mpz, *mmz;
   double *slope, *divrho, *densstar, *qs, *ql, *qr, *totdens;
   double *red2d; int *nshift;
+  double *sdiff_c, *sdiff_f;              /* Sdiffyczc, Sdiffyfzc (DUSTDIFFUSION) */
   /* scalars */
   double omegaframe, omegaframe0, phys_time, domega, dtemp, last_dt;
   double minstep[FO_MAXFLUIDS];
@@ -383,10 +387,14 @@ static void cfl(fo_disk *d) {
         double vxxp = F->vx[LXP] - F->vxmed[L2D(j, k)];
         double ss2 = F->cs[l] * F->cs[l], ss, visc, c1a, c1b, c1c = 0.0, c1, c2, c3, c4 = 0.0;
         double c5a, c5b, c5c = 0.0, c5, c7a, c7b, c7c = 0.0, c7;
-        if (d->p.alpha_visc)
+        const double gm = d->p.gamma;
+        if (d->p.alpha_visc && d->p.adiabatic)   /* cfl.c:162-164: cs holds the internal energy */
+          visc = d->p.alpha * gm * (gm - 1.0) * F->cs[l] / F->rho[l] * sqrt(Ymed(j) * Ymed(j) * Ymed(j) / (G * MSTAR));
+        else if (d->p.alpha_visc)
           visc = d->p.alpha * F->cs[l] * F->cs[l] * sqrt(Ymed(j) * Ymed(j) * Ymed(j) / (G * MSTAR));
         else
           visc = d->p.nu;
+        if (d->p.adiabatic) ss2 = gm * (gm - 1) * F->cs[l] / F->rho[l];   /* cfl.c:170-172 */
         ss = sqrt(ss2);
         c1a = ss / zone_size_x(d, i, j, k);
         c1b = ss / zone_size_y(d, j);
@@ -416,11 +424,15 @@ static void cfl(fo_disk *d) {
     }
 }
 
-/* ComputePressureFieldIso (CompPresIso.c:10-64). */
-static void pressure_iso(fo_disk *d) {
+/* ComputePressureFieldIso (CompPresIso.c:10-64) or, ADIABATIC,
+ * ComputePressureFieldAd (CompPresAd.c:52-53): P = (gamma - 1) e. */
+static void pressure(fo_disk *d) {
   fo_fluid *F = &d->fl[d->cur];
   long l;
-  for (l = 0; l < d->ncell; l++) d->pres[l] = F->rho[l] * F->cs[l] * F->cs[l];
+  if (d->p.adiabatic)
+    for (l = 0; l < d->ncell; l++) d->pres[l] = (d->p.gamma - 1.0) * F->cs[l];
+  else
+    for (l = 0; l < d->ncell; l++) d->pres[l] = F->rho[l] * F->cs[l] * F->cs[l];
 }
 
 /* _ComputeForce_cpu (compute_force.c:16-219) for x=y=z=0 (the star): only the
@@ -651,7 +663,21 @@ static void substep1_z(fo_disk *d, double dt) {
 /* Viscosity coefficients (visctensor_cyl.c:140-151; visctensor_sph.c). */
 static void visc_coeffs(const fo_disk *d, const fo_fluid *F, int i, int j, int k, long l,
                         double *v, double *vm, double *vzm, double *vzmym) {
-  if (d->p.alpha_visc) {
+  if (d->p.alpha_visc && d->p.adiabatic) {
+    /* visctensor_cyl.c:146-150: gamma (gamma - 1) e / rho in place of cs^2 */
+    const double *e = F->cs, *r = F->rho;
+    long lxm = LXM, lym = LYM, lzm = l, lxm_s = lxm, lym_s = lym;
+    double a = d->p.alpha, gm = d->p.gamma;
+    (void)i;
+    (void)k;
+    *v = a * gm * (gm - 1.0) * e[l] / r[l] * sqrt(Ymed(j) * Ymed(j) * Ymed(j) / (G * MSTAR));
+    *vm = a * gm * (gm - 1.0) * (e[l] + e[lxm] + e[lym] + e[lxm - d->pitch]) /
+          (r[l] + r[lxm] + r[lym] + r[lxm - d->pitch]) * sqrt(Ymin(j) * Ymin(j) * Ymin(j) / (G * MSTAR));
+    *vzmym = a * gm * (gm - 1.0) * (e[l] + e[lym] + e[lzm] + e[lym_s]) / (r[l] + r[lym] + r[lzm] + r[lym_s]) *
+             sqrt(Ymin(j) * Ymin(j) * Ymin(j) / (G * MSTAR));
+    *vzm = a * gm * (gm - 1.0) * (e[l] + e[lzm] + e[lxm] + e[lxm_s]) / (r[l] + r[lzm] + r[lxm] + r[lxm_s]) *
+           sqrt(Ymed(j) * Ymed(j) * Ymed(j) / (G * MSTAR));
+  } else if (d->p.alpha_visc) {
     const double *e = F->cs;
     long lxm = LXM, lym = LYM, lzm = d->is3d ? LZM : l;
     long lxm_s = d->is3d ? lxm - d->stride : lxm, lym_s = d->is3d ? lym - d->stride : lym;
@@ -805,7 +831,11 @@ static void substep2_b(fo_disk *d, double dt) {
         double dyrho1 = Ymin(j + 1) - Ymin(j), dyrho2 = Ymin(j) - Ymin(j - 1);
         F->vxt[l] += -2.0 * dt * dxmed * (d->mpx[l] - d->mpx[lxm]) / (F->rho[l] * dxrho1 + F->rho[lxm] * dxrho2) *
                      inv_zone_size_xmed(d, i, j, k);
+        if (d->p.adiabatic)   /* substep2_b.c:161-163: the artificial viscosity's heating */
+          F->cs[l] += -dt * (d->mpx[l] * (F->vx[LXP] - F->vx[l]) / zone_size_x(d, i, j, k));
         F->vyt[l] += -2.0 * (d->mpy[l] - d->mpy[lym]) / (F->rho[l] * dyrho1 + F->rho[lym] * dyrho2) * dt;
+        if (d->p.adiabatic)   /* substep2_b.c:176-178 */
+          F->cs[l] += -dt * (d->mpy[l] * (F->vy[LYP] - F->vy[l]) / zone_size_y(d, j));
         if (d->is3d) {
           long lzm = LZM;
           double dzmed = Zmed(k) - Zmed(k - 1), dzrho1 = Zmin(k + 1) - Zmin(k), dzrho2 = Zmin(k) - Zmin(k - 1);
@@ -813,6 +843,24 @@ static void substep2_b(fo_disk *d, double dt) {
                        (Ymed(j) * (Zmed(k) - Zmed(k - 1)));
         }
       }
+}
+
+/* SubStep3_cpu (substep3.c:79-118), ADIABATIC: the compressional heating
+ * -P div v, implicit in e, with the velocities after the source terms. */
+static void substep3(fo_disk *d, double dt) {
+  fo_fluid *F = &d->fl[d->cur];
+  const double *vx = F->vxt, *vy = F->vyt;
+  const double gm = d->p.gamma;
+  int i, j, k = 0;
+  for (j = 0; j < d->sy - 1; j++)
+    for (i = 0; i < d->nx; i++) {
+      long l = L(i, j, k);
+      double div_v = 0.0, term;
+      div_v += (vx[LXP] - vx[l]) * Sxj(j) * Sxk(k);
+      div_v += (vy[LYP] * Syj(j + 1) * Syk(k) * Sxi(i) - vy[l] * Syj(j) * Syk(k) * Sxi(i));
+      term = 0.5 * dt * (gm - 1.) * div_v * InvVj(j) / (Syk(k) * Sxi(i));
+      F->cs[l] *= (1.0 - term) / (1.0 + term);
+    }
 }
 
 /* ------------------------------------------------------------------------- */
@@ -880,6 +928,9 @@ static void boundary_y(fo_disk *d, int right) {
           /* KEPLERIAN2DDENS, KEPLERIAN2DVAZIM, ANTISYMMETRIC */
           F->rho[lgh] = F->rho[lact] * pow(Ymed(jact) / Ymed(jgh), ss);
           F->vx[lgh] = (F->vx[lact] + Ymed(jact) * of) * sqrt(Ymed(jact) / Ymed(jgh)) - Ymed(jgh) * of;
+          /* ADIABATIC: the energy's ghosts mirror the active cells (SYMMETRIC,
+             std/boundaries.txt), the oracle's adiabatic variant of fargo.bound */
+          if (d->p.adiabatic) F->cs[lgh] = F->cs[lact];
         } else {
           /* KEPLERIAN3DSPHDENSRAD, KEPLERIAN3DSPHVAZIMRAD */
           F->rho[lgh] = F->rho[lact] * pow(Ymed(jact) / Ymed(jgh), ss + fi + 1.) *
@@ -1185,6 +1236,7 @@ static void x_advection(fo_disk *d, int ppa, const double *vx, double dt) { /* t
   transport_x(d, ppa, d->mpy, vx, dt);
   transport_x(d, ppa, d->mmy, vx, dt);
   if (d->is3d) { transport_x(d, ppa, d->mpz, vx, dt); transport_x(d, ppa, d->mmz, vx, dt); }
+  if (d->p.adiabatic) transport_x(d, ppa, F->cs, vx, dt);   /* transport.c:63-65 */
   transport_x(d, ppa, F->rho, vx, dt);
 }
 
@@ -1279,6 +1331,7 @@ static void transport(fo_disk *d, double dt) {
     transport_y(d, d->mpx, dt); transport_y(d, d->mmx, dt);
     transport_y(d, d->mpy, dt); transport_y(d, d->mmy, dt);
     if (d->is3d) { transport_y(d, d->mpz, dt); transport_y(d, d->mmz, dt); }
+    if (d->p.adiabatic) transport_y(d, F->cs, dt);   /* transport.c:122-124 */
     transport_y(d, F->rho, dt);
   }
   if (d->nx > 1) {
@@ -1288,6 +1341,7 @@ static void transport(fo_disk *d, double dt) {
     advect_shift(d, d->mpx); advect_shift(d, d->mmx);
     advect_shift(d, d->mpy); advect_shift(d, d->mmy);
     if (d->is3d) { advect_shift(d, d->mpz); advect_shift(d, d->mmz); }
+    if (d->p.adiabatic) advect_shift(d, F->cs);   /* transport.c:155-157 */
     advect_shift(d, F->rho);
   }
   new_velocity(d);
@@ -1353,6 +1407,13 @@ fo_disk *fo_create(const fo_params *p) {
   int f, n;
   d->p = *p;
   if (d->p.nfluids < 1) d->p.nfluids = 1;
+  /* the adiabatic EOS and dust diffusion are restated for 2D cylindrical
+     disks (each on its own: the dust coefficients of an adiabatic gas are not) */
+  if ((p->adiabatic || p->dust_diffusion) && (p->nz > 1 || p->spherical || (p->adiabatic && p->dust_diffusion) ||
+                                              (p->dust_diffusion && d->p.nfluids < 2))) {
+    free(d);
+    return NULL;
+  }
   d->is3d = p->nz > 1;
   d->nx = p->nx; d->ny = p->ny; d->nz = d->is3d ? p->nz : 1;
   d->sx = d->nx; d->sy = d->ny + 2 * NG; d->sz = d->is3d ? d->nz + 2 * NG : 1;
@@ -1381,6 +1442,7 @@ fo_disk *fo_create(const fo_params *p) {
   d->densstar = xcalloc(d->ncell, 8); d->qs = xcalloc(d->ncell, 8);
   d->ql = xcalloc(d->ncell, 8); d->qr = xcalloc(d->ncell, 8); d->totdens = xcalloc(d->ncell, 8);
   d->red2d = xcalloc((size_t)d->sy * d->sz, 8); d->nshift = xcalloc((size_t)d->sy * d->sz, sizeof(int));
+  d->sdiff_c = xcalloc(d->ncell, 8); d->sdiff_f = xcalloc(d->ncell, 8);
   /* planets (psys.c:141-225) */
   d->np = p->nplanets;
   for (n = 0; n < d->np; n++) {
@@ -1415,6 +1477,7 @@ void fo_destroy(fo_disk *d) {
   free(d->pres); free(d->pot); free(d->mpx); free(d->mmx); free(d->mpy); free(d->mmy);
   free(d->mpz); free(d->mmz); free(d->slope); free(d->divrho); free(d->densstar); free(d->qs);
   free(d->ql); free(d->qr); free(d->totdens); free(d->red2d); free(d->nshift);
+  free(d->sdiff_c); free(d->sdiff_f);
   free(d->xmin); free(d->ymin); free(d->zmin); free(d->xmed); free(d->ymed); free(d->zmed);
   free(d->invdiffxmed); free(d->sxi); free(d->sxj); free(d->syj); free(d->szj); free(d->invvj);
   free(d->sxk); free(d->syk); free(d->szk);
@@ -1436,6 +1499,10 @@ void fo_set_state(fo_disk *d, int f, const double *rho, const double *vx, const 
   if (vy) memcpy(F->vy, vy, n);
   if (vz && d->is3d) memcpy(F->vz, vz, n);
   if (cs) memcpy(F->cs, cs, n);
+}
+
+void fo_get_energy(const fo_disk *d, int f, double *e) {
+  memcpy(e, d->fl[f].cs, sizeof(double) * d->ncell);
 }
 
 void fo_get_state(const fo_disk *d, int f, double *rho, double *vx, double *vy, double *vz) {
@@ -1464,9 +1531,72 @@ void fo_initialize(fo_disk *d) {
   d->cur = 0;
 }
 
+/* DustDiffusion_Main (dust_diffusion_main.c:3-28): the diffusion
+ * coefficients from the gas (DustDiffusion_Coefficients_cpu,
+ * dust_diffusion_coefficients.c:56-118; 2D cylindrical), then for every dust
+ * fluid the update of its density from the gradient of its concentration
+ * rho_d / (rho_d + rho_g) (DustDiffusion_Core_cpu, dust_diffusion_core.c:
+ * 97-170) into the Pressure scratch, copied to the density, and FillGhosts.
+ * copy_field copies the whole field; its rows 0 and Ny+5, which the core
+ * does not write, are ghost rows that FillGhosts rewrites, so only the rows
+ * the core writes are copied here. */
+static void dust_diffusion(fo_disk *d, double dt) {
+  const fo_fluid *Gs = &d->fl[0];
+  const double *cs = Gs->cs, *rhog = Gs->rho;
+  double *sdc = d->sdiff_c, *sdf = d->sdiff_f, *temp = d->pres;
+  int i, j, k = 0, f;
+  for (j = 0; j < d->sy; j++)
+    for (i = 0; i < d->nx; i++) {
+      long l = L(i, j, k);
+      if (d->p.alpha_visc) {
+        double ss2 = cs[l] * cs[l], ssf2, r3c, r3f;
+        if (j == 0) ssf2 = ss2;
+        else ssf2 = 0.5 * (cs[l] + cs[LYM]) * 0.5 * (cs[l] + cs[LYM]);
+        r3c = Ymed(j) * Ymed(j) * Ymed(j);
+        r3f = Ymin(j) * Ymin(j) * Ymin(j);
+        sdc[l] = d->p.alpha * ss2 / sqrt(G * MSTAR / r3c);
+        sdf[l] = d->p.alpha * ssf2 / sqrt(G * MSTAR / r3f);
+      } else {
+        sdc[l] = d->p.nu;
+        sdf[l] = d->p.nu;
+      }
+    }
+  for (f = 1; f < d->p.nfluids; f++) {
+    fo_fluid *F = &d->fl[f];
+    const double *rhod = F->rho;
+    d->cur = f;
+    for (j = 1; j < d->sy - 1; j++)
+      for (i = 0; i < d->nx; i++) {
+        long l = L(i, j, k), lxp = LXP, lxm = LXM, lyp = LYP, lym = LYM;
+        double c, update, d1, d2, d3, d4, cxp, cxm, cyp, cym, dxmin, dxmedp, dxmedm;
+        update = 0.0;
+        c = rhod[l] / (rhod[l] + rhog[l]);
+        dxmin = Xmin(i + 1) - Xmin(i);
+        dxmedp = 1.0 / d->invdiffxmed[ixp_(d, i)];
+        dxmedm = 1.0 / d->invdiffxmed[i];
+        d1 = 0.25 * (rhod[l] + rhog[l] + rhod[lxp] + rhog[lxp]) * (sdc[lxp] + sdc[l]);
+        d2 = 0.25 * (rhod[l] + rhog[l] + rhod[lxm] + rhog[lxm]) * (sdc[lxm] + sdc[l]);
+        cxp = rhod[lxp] / (rhod[lxp] + rhog[lxp]);
+        cxm = rhod[lxm] / (rhod[lxm] + rhog[lxm]);
+        update += 1.0 / Ymed(j) / Ymed(j) / (dxmin) * (d1 * (cxp - c) / (dxmedp) - (d2 * (c - cxm)) / (dxmedm));
+        d3 = 0.5 * (rhod[l] + rhog[l] + rhod[lyp] + rhog[lyp]) * sdf[lyp];
+        d4 = 0.5 * (rhod[l] + rhog[l] + rhod[lym] + rhog[lym]) * sdf[l];
+        cyp = rhod[lyp] / (rhod[lyp] + rhog[lyp]);
+        cym = rhod[lym] / (rhod[lym] + rhog[lym]);
+        update += 1.0 / Ymed(j) / (Ymin(j + 1) - Ymin(j)) *
+                  (Ymin(j + 1) * d3 * (cyp - c) / (Ymed(j + 1) - Ymed(j)) -
+                   (Ymin(j) * d4 * (c - cym)) / (Ymed(j) - Ymed(j - 1)));
+        temp[l] = rhod[l] + dt * update;
+      }
+    memcpy(F->rho + L(0, 1, 0), temp + L(0, 1, 0), sizeof(double) * (size_t)(d->sy - 2) * d->pitch);
+    fill_ghosts(d);
+  }
+  d->cur = 0;
+}
+
 static void sources(fo_disk *d, double dt) { /* algogas.c:30-133 */
   fo_fluid *F = &d->fl[d->cur];
-  pressure_iso(d);
+  pressure(d);
   compute_potential(d, dt);
   if (d->p.frame != FO_FRAME_FIXED) correct_vtheta(d, d->domega);
   substep1_x(d, dt);
@@ -1475,6 +1605,7 @@ static void sources(fo_disk *d, double dt) { /* algogas.c:30-133 */
   if (!F->dust && (d->p.nu != 0.0 || d->p.alpha_visc)) { visctensor(d); addviscosity(d, dt); }
   substep2_a(d);
   substep2_b(d, dt);
+  if (d->p.adiabatic && !F->dust) substep3(d, dt);   /* algogas.c:82-84 */
   /* copy_velocities(VTEMP2V); FillGhosts; copy_velocities(V2VTEMP) */
   memcpy(F->vx, F->vxt, sizeof(double) * d->ncell);
   memcpy(F->vy, F->vyt, sizeof(double) * d->ncell);
@@ -1503,6 +1634,7 @@ double fo_step(fo_disk *d, double DT) {
     for (l = 0; l < d->ncell; l++) d->totdens[l] += d->fl[f].rho[l];
   for (f = 0; f < d->p.nfluids; f++) { d->cur = f; sources(d, dt); }
   if (d->p.nfluids > 1) collisions(d, dt);
+  if (d->p.dust_diffusion) dust_diffusion(d, dt);   /* main.c:417-419 */
   for (f = 0; f < d->p.nfluids; f++) {
     d->cur = f;
     compute_vmed(d, d->fl[f].vxt); /* algogas.c:141 */

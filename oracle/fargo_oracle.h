@@ -46,9 +46,9 @@ typedef struct {
   int nfluids;                 /* 1: gas only; >1: gas + dust, implicit drag       */
   double invstokes[FO_MAXFLUIDS]; /* STOKESNUMBER drag: [f-1] = 1/St of dust fluid f */
   int stockholm;               /* STOCKHOLM damping on/off                        */
-  int adiabatic;               /* ADIABATIC equation of state (reference builds only) */
+  int adiabatic;               /* ADIABATIC equation of state (2D cylindrical, gas) */
   double gamma;                /* GAMMA                                            */
-  int dust_diffusion;          /* DUSTDIFFUSION (reference builds only)            */
+  int dust_diffusion;          /* DUSTDIFFUSION (2D cylindrical, dust fluids)       */
   int slab_y0, slab_ny_global; /* the library's radial slabs (unused here: whole disks) */
 } fo_params;
 
@@ -77,6 +77,9 @@ double fo_step(fo_disk *d, double dt_interval);
 void fo_get_scalars(const fo_disk *d, double *out8);
 /* Total mass of fluid f over the active mesh (compensated sum). */
 double fo_mass(const fo_disk *d, int f);
+/* the fluid's Energy field: the internal energy of an adiabatic disk, the
+ * sound speed of an isothermal one */
+void fo_get_energy(const fo_disk *d, int f, double *e);
 
 #ifdef __cplusplus
 }

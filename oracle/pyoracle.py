@@ -122,9 +122,6 @@ class Disk:
         reference's stock -O3, for timing), 'dropin' or 'shadow' (the
         reference's build with its hydro step on the B200 library)."""
         self.cfg, self.kind = cfg, kind
-        if kind == "oracle" and (getattr(cfg, "adiabatic", False) or getattr(cfg, "dust_diffusion", False)):
-            raise ValueError("the oracle restatement has neither the adiabatic EOS nor dust diffusion: "
-                             "those disks run on the reference build")
         if kind == "oracle":
             path = os.path.join(HERE, "_build", "libfargo_oracle.so")
         elif kind in ("dropin", "shadow"):
@@ -164,7 +161,11 @@ class Disk:
             for n in ("fo_set_state", "fo_get_state", "fo_initialize", "fo_get_scalars",
                       "fo_destroy", "fo_get_geometry"):
                 getattr(lib, n).restype = None
+            lib.fo_get_energy.restype = None
             self.h = lib.fo_create(C.byref(self.params))
+            if not self.h:
+                raise ValueError("the oracle restatement has the adiabatic EOS and dust diffusion for 2D "
+                                 "cylindrical disks only (not together)")
         else:
             lib.ref_create.restype = C.c_int
             lib.ref_create.argtypes = [C.POINTER(FoParams)]
@@ -212,10 +213,11 @@ class Disk:
 
     def energy(self, fluid: int = 0):
         """The fluid's Energy field (the internal energy of an adiabatic
-        build, the sound speed of an isothermal one); 'ref' kinds."""
-        if self.kind not in ("ref", "ref_o3", "dropin", "shadow"):
-            raise NotImplementedError
+        disk, the sound speed of an isothermal one)."""
         out = np.zeros(self.shape)
+        if self.kind == "oracle":
+            self.lib.fo_get_energy(C.c_void_p(self.h), C.c_int(fluid), _ptr(out))
+            return out
         self.lib.ref_get_energy.restype = None
         self.lib.ref_get_energy(C.c_int(fluid), _ptr(out))
         return out
@@ -244,7 +246,8 @@ class Disk:
 
 
 def run(cfg, nsteps: int, kind: str = "oracle", dt_interval: float = 1e30, state=None):
-    """Initial state -> nsteps hydro steps; returns (state dict, dts, scalars)."""
+    """Initial state -> nsteps hydro steps; returns (per fluid the state dict
+    with its energy "e", dts, scalars)."""
     from fargo3d_b200.setups import initial_state
     d = Disk(cfg, kind)
     for f in range(cfg.nfluids):
@@ -252,7 +255,7 @@ def run(cfg, nsteps: int, kind: str = "oracle", dt_interval: float = 1e30, state
         d.set_state(*st, fluid=f)
     d.initialize()
     dts = [d.step(dt_interval) for _ in range(nsteps)]
-    out = [d.state(f) for f in range(cfg.nfluids)]
+    out = [dict(d.state(f), e=d.energy(f)) for f in range(cfg.nfluids)]
     sc = d.scalars()
     d.close()
     return out, np.array(dts), sc

@@ -1,7 +1,8 @@
 """Small parity cases shared by the golden-vector generator and the tests."""
 import math
 
-from fargo3d_b200.setups import DiskConfig, Planet, config_fargo2d, config_multifluid, config_p3disof
+from fargo3d_b200.setups import (DiskConfig, Planet, config_adiabatic2d, config_fargo2d, config_multifluid,
+                                  config_p3disof)
 
 
 def cases():
@@ -26,6 +27,10 @@ def cases():
         "cyl2d_feeldisk": (config_fargo2d(32, 16, seed=8).replace(
             frame="F", omegaframe=1.0, indirect_term=False,
             planets=[Planet(1.0, 1e-3, True, True), Planet(1.4, 3e-4, True, True)]), 15, 1e30),
+        # ADIABATIC equation of state (the fargo flags with ADIABATIC and alpha viscosity)
+        "cyl2d_ad": (config_adiabatic2d(48, 20, seed=9), 20, 0.2),
+        # the multifluid flags with DUSTDIFFUSION
+        "mf5_dd": (config_multifluid(32, 16, seed=10, dust_diffusion=True), 12, 1e30),
     }
 
 
@@ -39,8 +44,9 @@ def golden_init(g, cfg):
 
 
 def golden_out(g, f=0):
-    """Fluid f's state after the golden run."""
-    return {k: g[_key(f, k)] for k in ("rho", "vx", "vy", "vz")}
+    """Fluid f's state after the golden run (with its energy "e" where the
+    file holds it)."""
+    return {k: g[_key(f, k)] for k in ("rho", "vx", "vy", "vz", "e") if _key(f, k) in g}
 
 
 def golden_arrays(init, out):
@@ -49,6 +55,7 @@ def golden_arrays(init, out):
     for f, (st, o) in enumerate(zip(init, out)):
         for k, v in zip(("rho0", "vx0", "vy0", "vz0", "cs"), st):
             d[_key(f, k)] = v
-        for k in ("rho", "vx", "vy", "vz"):
-            d[_key(f, k)] = o[k]
+        for k in ("rho", "vx", "vy", "vz", "e"):
+            if k in o:
+                d[_key(f, k)] = o[k]
     return d
