@@ -113,6 +113,14 @@ static int rebuild(fb_batch *B) {
     const int cnt = tiles(B, s, v);
     if ((rc = upload_list(&B->items[s], &B->nitems[s], cnt, v))) return rc;
   }
+  // the planet indices some member's disk force is needed for
+  B->force_np = 0;
+  for (int i = 0; i < B->n; i++) {
+    if (B->state[i] != 2) continue;
+    const fb_psys *S = fb_disk_internal_psys(B->disks[i]);
+    for (int n = 0; n < S->np; n++)
+      if (S->feeldisk[n] && n + 1 > B->force_np) B->force_np = n + 1;
+  }
   // chains: the largest disks first, each to the chain with the fewest cells
   B->chain_of.assign(B->n, -1);
   if (B->nchains > 1) {
@@ -221,9 +229,6 @@ int fb_batch_add(fb_batch *B, const fb_params *p, double t_end, int *slot) {
   if ((p->nz > 1) != (B->is3d != 0) || p->nfluids != B->nfluids) return FB_ERR_ARG;
   if (p->adiabatic || p->dust_diffusion)   // the batched stages have neither
     return fb_internal_fail(FB_ERR_ARG, "adiabatic disks and dust diffusion run on the one-disk path (fb_disk_step)", 0);
-  for (int n = 0; n < p->nplanets; n++)
-    if (p->pl_feeldisk[n])  // the batch's device-side planetary step has no disk force
-      return fb_internal_fail(FB_ERR_ARG, "planets that feel the disk run on the one-disk path (fb_disk_step)", 0);
   int s = -1;
   for (int i = 0; i < B->n && s < 0; i++)
     if (B->state[i] == 0) s = i;

@@ -22,7 +22,7 @@ namespace fb {
 // ST_Y4 + k for NS = 4 << k).  Both are per-disk tile choices (disk_cx,
 // disk_ns; the autotuner sets them).
 enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_COLL, ST_Z4, ST_Z8, ST_Z16, ST_Y4, ST_Y8, ST_Y16,
-       ST_X1, ST_X2, ST_X4, ST_X8, ST_X16, ST_NEWVEL, ST_N };
+       ST_X1, ST_X2, ST_X4, ST_X8, ST_X16, ST_NEWVEL, ST_FORCE, ST_N };
 constexpr int NXC = 5, NNS = 3;
 
 // tile shapes shared with the one-disk launchers (fb_launch.cuh)
@@ -254,6 +254,42 @@ static __global__ void __launch_bounds__(128, FB_NV32_MINB) kb_newvel_cyl32(cons
                  D.stockholm, scp, bid);
 }
 
+// The disk's acceleration at planet n of every disk whose planet n feels the
+// disk (ComputeAccel for AdvanceSystemFromDisk, planets.c:86-114), from the
+// density and planets at the start of the step: the ring sums (one lane per
+// ring, the reference's order), then one thread per disk folds them.  The
+// smoothing is the planet's (compute_potential's RocheSmoothing or the
+// flared thickness), formed on the device.
+__device__ __forceinline__ bool force_planet(const fb_disk_dev &D, const fb_psys &S, int n, double &x, double &y,
+                                             double &z, double &rs) {
+  if (!D.feeldisk || n >= S.np || !S.feeldisk[n]) return false;
+  x = S.px[n]; y = S.py[n]; z = S.pz[n];
+  const double r = sqrt(x * x + y * y + z * z), mp = S.pmass[n];
+  if (S.roche_smoothing != 0) rs = r * pow(mp / 3. / FB_MSTAR, 1. / 3.) * S.roche_smoothing;
+  else rs = S.aspectratio * pow(r / FB_R0, S.flaringindex) * r * S.thickness_smoothing;
+  return true;
+}
+template <typename S>
+static __global__ void __launch_bounds__(128) kb_disk_force_rings(const fb_disk_dev *ds, const fb_psys *ps,
+                                                                  const int4 *items, int n) {
+  const int4 w = items[blockIdx.x];
+  const fb_disk_dev &D = ds[w.x];
+  if (D.scal_dev->skip) return;
+  double x, y, z, rs;
+  if (!force_planet(D, ps[w.x], n, x, y, z, rs)) return;
+  b_disk_force_rings<S>(D, x, y, z, rs, D.ring3, w.y * 128 + threadIdx.x);
+}
+static __global__ void kb_disk_force_fold(const fb_disk_dev *ds, const fb_psys *ps, const int *dl, int nd, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nd) return;
+  const int i = dl ? dl[t] : t;
+  const fb_disk_dev &D = ds[i];
+  if (D.nx == 0 || D.scal_dev->skip) return;
+  double x, y, z, rs;
+  if (!force_planet(D, ps[i], n, x, y, z, rs)) return;
+  b_disk_force_fold(D, x, y, z, D.ring3, D.facc + 3 * n);
+}
+
 // The scalar work of the step for every disk of the list dl (all n disks when
 // dl is null), one thread per disk; then the
 // CFL minimum is reset for the next step.  dtmin[1] carries the kernels'
@@ -277,7 +313,7 @@ static __global__ void kb_scalars(const fb_disk_dev *ds, fb_psys *ps, const int 
     } else if (dm[1] != 0ull) {
       S.status = FB_ERR_NONFINITE;
       sc.skip = 1;
-    } else if (fb_psys_step(&S, cflmin, S.t_end > 0.0 ? S.t_end : DT, &sc, nullptr) < 0.0) {
+    } else if (fb_psys_step(&S, cflmin, S.t_end > 0.0 ? S.t_end : DT, &sc, D.feeldisk ? D.facc : nullptr) < 0.0) {
       sc.skip = 1;
     } else if (S.t_end > 0.0 && S.dtemp >= S.t_end) {
       S.status = FB_DONE;
@@ -318,6 +354,7 @@ struct fb_batch {
      lists (chain c: citems[c], its disks cdisks[c]), so that one group's
      latency-bound launches (the scalar step, reductions, boundaries, launch
      tails) overlap another's throughput-bound ones */
+  int force_np;   /* planet indices that feel the disk in some member (0: none) */
   int nchains;
   cudaStream_t cstream[FB_MAX_CHAINS];
   cudaEvent_t ev_fork, ev_join[FB_MAX_CHAINS];
@@ -369,6 +406,11 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v, int chain = -1) {
         if (disk_cx(D) != c) { g = dim3(0); break; }
         const int rpc = 256 / (nx / c), nr = (ny + 1) * (D.is3d ? nz + 1 : 1);
         g = dim3((nr + rpc - 1) / rpc);
+        break;
+      }
+      case ST_FORCE: {
+        const int nr = ny * (D.is3d ? nz : 1);
+        g = D.feeldisk ? dim3((nr + 127) / 128) : dim3(0);
         break;
       }
       case ST_NEWVEL:
@@ -442,7 +484,15 @@ static int launch_step(fb_batch *B, double DT, int chain) {
   pmark(st, "cfl");
   {
     const int nd = chain < 0 ? B->n : B->ncdisks[chain];
-    kb_scalars<<<(nd + 63) / 64, 64, 0, st>>>(ds, B->d_psys, chain < 0 ? nullptr : B->cdisks[chain], nd, DT);
+    const int *dl = chain < 0 ? nullptr : B->cdisks[chain];
+    if (nitems[ST_FORCE]) {   // planets that feel the disk, one planet index at a time
+      for (int n = 0; n < B->force_np; n++) {
+        kb_disk_force_rings<S><<<grid(ST_FORCE), 128, 0, st>>>(ds, B->d_psys, items[ST_FORCE], n);
+        kb_disk_force_fold<<<(nd + 63) / 64, 64, 0, st>>>(ds, B->d_psys, dl, nd, n);
+      }
+      pmark(st, "disk_force");
+    }
+    kb_scalars<<<(nd + 63) / 64, 64, 0, st>>>(ds, B->d_psys, dl, nd, DT);
   }
   pmark(st, "scalars");
   for (int f = 0; f < nf; f++) {

@@ -57,8 +57,8 @@ typedef struct {
   void *et, *e_a;
 } fb_fluid_dev;
 
-/* Per-step scalars (host-computed in FP64 mode, device-computed in the
- * batched mode).  Mirrors FbStepScalars in fb_common.cuh. */
+/* Per-step scalars (host-computed on the one-disk path, device-computed in
+ * batches). */
 typedef struct {
   double dt;
   double omegaframe, omegaframe0, domega;
@@ -92,6 +92,9 @@ typedef struct {
   double *dtmin;          /* device scalar: CFL minimum (bits as u64 min) */
   fb_scalars *scal_dev;   /* device copy of the per-step scalars */
   double *ringsum;        /* per-ring scratch of the mass reduction: 2 x rings + 2 doubles */
+  int feeldisk;           /* some planet feels the disk (AdvanceSystemFromDisk) */
+  double *ring3;          /* per-ring scratch of the disk's force on a planet: 3 x rings */
+  double *facc;           /* the disk's acceleration at each planet: 3 x FB_MAXPLANETS */
   double *bnd_tab;        /* boundary factor tables (double) */
   int bnd_tab_n;
   double *ramps;          /* Stockholm ramps: [sy] radial, [sz] zmed, [sz] zmin */

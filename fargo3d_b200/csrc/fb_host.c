@@ -655,6 +655,9 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
     fb_disk_destroy(D);
     return rc;
   }
+  D->d.feeldisk = D->feeldisk;
+  D->d.ring3 = D->d_ring3;
+  D->d.facc = D->d_facc;
   fb_psys_init(&D->ps, p->nplanets, p->pl_dist, p->pl_mass, p->pl_feeldisk, p->pl_feelothers, p->eccentricity, p->inclination,
                p->frame, p->omegaframe, p->indirect_term, p->roche_smoothing, p->aspectratio, p->flaringindex,
                p->thickness_smoothing);

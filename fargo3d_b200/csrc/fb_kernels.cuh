@@ -1932,11 +1932,10 @@ __global__ void __launch_bounds__(128) k_collisions(const fb_disk_dev D, Dims m,
 // radius) and the outer ones separately.  Density = the sum of the fluids'
 // densities in fluid order (ComputeTotalDensity).
 template <typename S>
-__global__ void __launch_bounds__(128) k_disk_force_rings(const fb_disk_dev D, double x, double y, double z,
-                                                          double rs, double *__restrict__ ring3) {
+__device__ __forceinline__ void b_disk_force_rings(const fb_disk_dev &D, double x, double y, double z, double rs,
+                                                   double *__restrict__ ring3, int r) {
   const Dims m = dims_of(D);
   const Geo<double> gd = geo_of<double>(D.geomd);
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= m.ny * (m.is3d ? m.nz : 1)) return;
   const int j = FB_NGH + r % m.ny, k = m.is3d ? FB_NGH + r / m.ny : 0;
   const double ym = ld(gd.ymed + j), syk = ld(gd.syk + k), ivj = ld(gd.invvj + j);
@@ -1970,11 +1969,15 @@ __global__ void __launch_bounds__(128) k_disk_force_rings(const fb_disk_dev D, d
   ring3[n2 + q] = sy;
   ring3[2 * n2 + q] = sz;
 }
+template <typename S>
+__global__ void __launch_bounds__(128) k_disk_force_rings(const fb_disk_dev D, double x, double y, double z,
+                                                          double rs, double *__restrict__ ring3) {
+  b_disk_force_rings<S>(D, x, y, z, rs, ring3, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
-// one thread: fold the ring sums into inner + outer (compute_force.c:161-214)
-static __global__ void k_disk_force_fold(const fb_disk_dev D, double x, double y, double z,
-                                  const double *__restrict__ ring3, double *__restrict__ out3) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// fold the ring sums into inner + outer (compute_force.c:161-214)
+__device__ __forceinline__ void b_disk_force_fold(const fb_disk_dev &D, double x, double y, double z,
+                                                  const double *__restrict__ ring3, double *__restrict__ out3) {
   const Dims m = dims_of(D);
   const Geo<double> gd = geo_of<double>(D.geomd);
   const int k0 = m.is3d ? FB_NGH : 0, k1 = m.is3d ? m.nz + FB_NGH : 1, n2 = m.sy * m.sz;
@@ -1994,6 +1997,12 @@ static __global__ void k_disk_force_fold(const fb_disk_dev D, double x, double y
       for (int j = olo; j < ohi; j++) fout = ring3[c * n2 + j + k * m.sy] + fout;
     out3[c] = fin + fout;
   }
+}
+// one thread
+static __global__ void k_disk_force_fold(const fb_disk_dev D, double x, double y, double z,
+                                         const double *__restrict__ ring3, double *__restrict__ out3) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  b_disk_force_fold(D, x, y, z, ring3, out3);
 }
 
 // ---------------------------------------------------------------------------
