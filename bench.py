@@ -494,8 +494,9 @@ def run_ours(args, rank, world, local_rank):
 # --------------------------------------------------------------------------
 def _ref_disk_worker(job):
     """One disk advanced by the reference's own sources (oracle/_ref, built
-    with the reference's stock -O3; the parity build if that is missing)."""
-    cfg, steps = job
+    with the reference's stock -O3; the parity build if that is missing):
+    `warmup` untimed steps, then `steps` timed ones."""
+    cfg, steps, warmup = job
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from fargo3d_b200 import initial_state
@@ -512,6 +513,8 @@ def _ref_disk_worker(job):
     for f in range(cfg.nfluids):
         d.set_state(*initial_state(cfg, f), fluid=f)
     d.initialize()
+    for _ in range(warmup):
+        d.step()
     t0 = time.time()
     for _ in range(steps):
         d.step()
@@ -520,7 +523,7 @@ def _ref_disk_worker(job):
     return cfg.active_cells * steps, t0, t1, kind
 
 
-def cpu_reference(cfgs, steps):
+def cpu_reference(cfgs, steps, warmup=0):
     """Throughput of the reference's CPU implementation: independent disks as
     independent single-threaded processes over the host's cores (the
     reference has no threading; MPI is absent on this image).  Returns
@@ -531,7 +534,7 @@ def cpu_reference(cfgs, steps):
         pyoracle.build()
     cores = max(1, min(len(cfgs), os.cpu_count() or 1))
     # largest disks first so the makespan is not set by a late big disk
-    jobs = sorted([(c, steps) for c in cfgs], key=lambda j: -j[0].active_cells)
+    jobs = sorted([(c, steps, warmup) for c in cfgs], key=lambda j: -j[0].active_cells)
     if cores == 1:
         res = [_ref_disk_worker(j) for j in jobs]
         wall = sum(r[2] - r[1] for r in res)
@@ -635,9 +638,10 @@ def main():
         gcfgs, wname = workload(args.workload, 0, 1)
         cores = max(1, min(len(gcfgs), os.cpu_count() or 1))
         steps = cpu_steps_for(gcfgs, args.steps, cores)
-        v, kind, cores, wall = cpu_reference(gcfgs, steps)
+        warm = min(args.warmup, steps)
+        v, kind, cores, wall = cpu_reference(gcfgs, steps, warm)
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": world,
-                "steps": steps, "warmup": 0, "ms_per_step": wall / steps * 1e3, "higher_is_better": True,
+                "steps": steps, "warmup": warm, "ms_per_step": wall / steps * 1e3, "higher_is_better": True,
                 "dtype": "f64", "data": "synthetic",
                 "config": {"workload": wname, "precision": "fp64 (the reference CPU build, stock -O3)"},
                 "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": kind,

@@ -59,30 +59,45 @@ static int launch_steps(fb_batch *B, double DT, int nsteps) {
 }
 
 static void free_lists(fb_batch *B) {
+  if (B->lists) cudaFree(B->lists);
+  B->lists = nullptr;
   for (int s = 0; s < ST_N; s++) {
-    if (B->items[s]) cudaFree(B->items[s]);
     B->items[s] = nullptr;
     B->nitems[s] = 0;
   }
   for (int c = 0; c < FB_MAX_CHAINS; c++) {
     for (int s = 0; s < ST_N; s++) {
-      if (B->citems[c][s]) cudaFree(B->citems[c][s]);
       B->citems[c][s] = nullptr;
       B->ncitems[c][s] = 0;
     }
-    if (B->cdisks[c]) cudaFree(B->cdisks[c]);
     B->cdisks[c] = nullptr;
     B->ncdisks[c] = 0;
   }
 }
 
-static int upload_list(int4 **dst, int *n, int count, const std::vector<int4> &v) {
-  *n = count;
-  if (count <= 0) return FB_OK;
-  if (cudaMalloc(dst, sizeof(int4) * v.size()) != cudaSuccess) return FB_ERR_NOMEM;
-  cudaError_t e = cudaMemcpy(*dst, v.data(), sizeof(int4) * v.size(), cudaMemcpyHostToDevice);
-  return e == cudaSuccess ? FB_OK : fb_internal_fail(FB_ERR_CUDA, "work list upload", (int)e);
-}
+// The work lists and chain disk lists of a rebuild, gathered on the host
+// and uploaded as one allocation with one copy (a batch rebuilds them for
+// every change of membership; dozens of small allocations and synchronous
+// copies would cost milliseconds).
+struct ListPack {
+  std::vector<unsigned char> host;
+  std::vector<std::pair<void **, size_t>> fix;   // pointer to set, offset in the pack
+  void add(void **dst, const void *src, size_t bytes) {
+    if (!bytes) { *dst = nullptr; return; }
+    const size_t off = (host.size() + 15) & ~(size_t)15;
+    host.resize(off + bytes);
+    memcpy(host.data() + off, src, bytes);
+    fix.push_back(std::make_pair(dst, off));
+  }
+  int upload(fb_batch *B) {
+    if (host.empty()) return FB_OK;
+    if (cudaMalloc(&B->lists, host.size()) != cudaSuccess) return FB_ERR_NOMEM;
+    cudaError_t e = cudaMemcpy(B->lists, host.data(), host.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fb_internal_fail(FB_ERR_CUDA, "work list upload", (int)e);
+    for (auto &f : fix) *f.first = (void *)((unsigned char *)B->lists + f.second);
+    return FB_OK;
+  }
+};
 
 // Work lists, chunk width and shared-memory size for the active set; drops
 // the captured graph.
@@ -107,11 +122,11 @@ static int rebuild(fb_batch *B) {
                              B->precision == FB_FP64 ? 8 : fb_batch_sweep_x_esz_f32());
     if (s > B->smem_x[k]) B->smem_x[k] = s;
   }
-  int rc;
+  ListPack pack;
   for (int s = 0; s < ST_N; s++) {
     std::vector<int4> v;
-    const int cnt = tiles(B, s, v);
-    if ((rc = upload_list(&B->items[s], &B->nitems[s], cnt, v))) return rc;
+    B->nitems[s] = tiles(B, s, v);
+    pack.add((void **)&B->items[s], v.data(), sizeof(int4) * v.size());
   }
   // the planet indices some member's disk force is needed for
   B->force_np = 0;
@@ -145,20 +160,15 @@ static int rebuild(fb_batch *B) {
     for (int c = 0; c < B->nchains; c++) {
       std::sort(members[c].begin(), members[c].end());
       B->ncdisks[c] = (int)members[c].size();
-      if (!members[c].empty()) {
-        if (cudaMalloc(&B->cdisks[c], sizeof(int) * members[c].size()) != cudaSuccess) return FB_ERR_NOMEM;
-        if (cudaMemcpy(B->cdisks[c], members[c].data(), sizeof(int) * members[c].size(), cudaMemcpyHostToDevice) !=
-            cudaSuccess)
-          return FB_ERR_CUDA;
-      }
+      pack.add((void **)&B->cdisks[c], members[c].data(), sizeof(int) * members[c].size());
       for (int s = 0; s < ST_N; s++) {
         std::vector<int4> v;
-        const int cnt = tiles(B, s, v, c);
-        if ((rc = upload_list(&B->citems[c][s], &B->ncitems[c][s], cnt, v))) return rc;
+        B->ncitems[c][s] = tiles(B, s, v, c);
+        pack.add((void **)&B->citems[c][s], v.data(), sizeof(int4) * v.size());
       }
     }
   }
-  return FB_OK;
+  return pack.upload(B);
 }
 
 extern "C" {

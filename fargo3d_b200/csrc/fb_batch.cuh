@@ -354,6 +354,7 @@ struct fb_batch {
      lists (chain c: citems[c], its disks cdisks[c]), so that one group's
      latency-bound launches (the scalar step, reductions, boundaries, launch
      tails) overlap another's throughput-bound ones */
+  void *lists;    /* one device allocation holding every work list below */
   int force_np;   /* planet indices that feel the disk in some member (0: none) */
   int nchains;
   cudaStream_t cstream[FB_MAX_CHAINS];
