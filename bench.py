@@ -438,12 +438,11 @@ def run_ours(args, rank, world, local_rank):
     t0 = time.perf_counter()
     if batched:
         r2 = Batch(cfgs, precision, device=local_rank)
-        for i, sts in enumerate(pinned):
-            for f, st in enumerate(sts):
-                r2.set_state(i, *[p.numpy() for p in st], fluid=f)
+        for f in range(nf):
+            r2.set_states([[p.numpy() for p in sts[f]] for sts in pinned], fluid=f)
         r2.initialize()
         r2.run(args.steps)
-        outs = [r2.state(i, fluid=f, out=results[i][f]) for i in range(len(cfgs)) for f in range(nf)]
+        outs = [o for f in range(nf) for o in r2.states(f, out=[results[i][f] for i in range(len(cfgs))])]
     else:
         r2 = Disk(cfgs[0], precision, device=local_rank)
         for f, st in enumerate(pinned[0]):

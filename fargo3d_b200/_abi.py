@@ -147,6 +147,9 @@ def bind_batch(L):
     L.fb_batch_set_tiles.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
     L.fb_batch_set_chains.argtypes = [C.c_void_p, C.c_int]
     L.fb_batch_get_chains.argtypes = [C.c_void_p]
+    _PP = C.POINTER(C.POINTER(C.c_double))
+    L.fb_batch_set_states.argtypes = [C.c_void_p, C.c_int, _PP, _PP, _PP, _PP, _PP]
+    L.fb_batch_get_states.argtypes = [C.c_void_p, C.c_int, _PP, _PP, _PP, _PP]
     L.fb_disk_set_tiles.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.fb_disk_get_tiles.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L._batch_bound = True

@@ -69,6 +69,47 @@ class Batch:
     def sync(self):
         _abi.check(_abi.lib().fb_batch_sync(self._h))
 
+    def set_states(self, states, fluid: int = 0):
+        """Every member's state of `fluid` in one library call: one
+        (rho, vx, vy, vz, cs) per member, FARGO3D layout (None skips a field
+        or a member).  Page-locked arrays move by DMA back to back."""
+        n = len(self.cfgs)
+        keep, cols = [], []
+        for q in range(5):
+            col = (C.POINTER(C.c_double) * n)()
+            any_ = False
+            for i, st in enumerate(states):
+                a = None if st is None else st[q]
+                if a is None:
+                    continue
+                a = np.ascontiguousarray(a, dtype=np.float64).reshape(self._members[i].shape)
+                keep.append(a)
+                col[i] = a.ctypes.data_as(C.POINTER(C.c_double))
+                any_ = True
+            cols.append(col if any_ else None)
+        _abi.check(_abi.lib().fb_batch_set_states(self._h, fluid, *cols))
+
+    def states(self, fluid: int = 0, out=None):
+        """Every member's fields of `fluid` (``out``: one dict of
+        preallocated arrays per member, as for :meth:`state`), read in one
+        library call."""
+        self.sync()
+        n = len(self.cfgs)
+        res = [_out_arrays(self._members[i].shape, self.cfgs[i].nz > 1, None if out is None else out[i])
+               for i in range(n)]
+        cols = []
+        for k in ("rho", "vx", "vy", "vz"):
+            col = (C.POINTER(C.c_double) * n)()
+            any_ = False
+            for i in range(n):
+                if k == "vz" and not self.cfgs[i].nz > 1:
+                    continue
+                col[i] = res[i][k].ctypes.data_as(C.POINTER(C.c_double))
+                any_ = True
+            cols.append(col if any_ else None)
+        _abi.check(_abi.lib().fb_batch_get_states(self._h, fluid, *cols))
+        return res
+
     def state(self, i, fluid: int = 0, out: dict | None = None):
         """Disk i's current fields as float64 arrays (``out``: preallocated
         arrays to fill, as for :meth:`Disk.state`)."""

@@ -357,7 +357,7 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
     int rc = rebuild(B);
     if (rc) return rc;
   }
-  if (B->nitems[ST_CFL] == 0) return FB_OK;
+  if (B->nitems[ST_ROWSUM] == 0) return FB_OK;
   const int chunk = 10;  // steps per captured graph; a remainder runs eagerly
   if (nsteps >= chunk && (!B->exec || B->graph_steps != chunk || B->graph_dt != DT)) {
     if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
@@ -396,6 +396,48 @@ int fb_batch_set_chains(fb_batch *B, int chains) {
 }
 
 int fb_batch_get_chains(fb_batch *B) { return B ? B->nchains : FB_ERR_ARG; }
+
+// Fluid f's state of every member at once: arrays indexed by slot (a NULL
+// array or entry skips that field or slot).  All transfers go through the
+// batch's stream with one wait at the end.
+static int gather(fb_batch *B, const void *const *a, std::vector<fb_disk *> &ds, std::vector<const void *> &out,
+                  std::vector<int> &slots) {
+  if (slots.empty())
+    for (int i = 0; i < B->n; i++)
+      if (B->disks[i]) slots.push_back(i);
+  if (ds.empty())
+    for (int i : slots) ds.push_back(B->disks[i]);
+  out.clear();
+  if (a)
+    for (int i : slots) out.push_back(a[i]);
+  return 0;
+}
+
+int fb_batch_set_states(fb_batch *B, int fluid, const double *const *rho, const double *const *vx,
+                        const double *const *vy, const double *const *vz, const double *const *cs) {
+  if (!B) return FB_ERR_ARG;
+  std::vector<fb_disk *> ds;
+  std::vector<int> slots;
+  std::vector<const void *> p[5];
+  const double *const *in[5] = {rho, vx, vy, vz, cs};
+  for (int q = 0; q < 5; q++) gather(B, (const void *const *)in[q], ds, p[q], slots);
+  if (ds.empty()) return FB_OK;
+  auto arr = [&](int q) { return in[q] ? (const double *const *)p[q].data() : nullptr; };
+  return fb_disks_set_state(ds.data(), (int)ds.size(), fluid, arr(0), arr(1), arr(2), arr(3), arr(4));
+}
+
+int fb_batch_get_states(fb_batch *B, int fluid, double *const *rho, double *const *vx, double *const *vy,
+                        double *const *vz) {
+  if (!B) return FB_ERR_ARG;
+  std::vector<fb_disk *> ds;
+  std::vector<int> slots;
+  std::vector<const void *> p[4];
+  double *const *in[4] = {rho, vx, vy, vz};
+  for (int q = 0; q < 4; q++) gather(B, (const void *const *)in[q], ds, p[q], slots);
+  if (ds.empty()) return FB_OK;
+  auto arr = [&](int q) { return in[q] ? (double *const *)p[q].data() : nullptr; };
+  return fb_disks_get_state(ds.data(), (int)ds.size(), fluid, arr(0), arr(1), arr(2), arr(3));
+}
 
 int fb_batch_sync(fb_batch *B) {
   if (!B) return FB_ERR_ARG;
@@ -448,7 +490,7 @@ int fb_batch_profile_step(fb_batch *B, double DT, float *ms, const char **names,
     int rc = rebuild(B);
     if (rc) return rc;
   }
-  if (B->nitems[ST_CFL] == 0) return 0;
+  if (B->nitems[ST_ROWSUM] == 0) return 0;
   Prof P;
   P.n = 0;
   g_prof = &P;

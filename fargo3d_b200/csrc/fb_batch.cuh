@@ -22,7 +22,7 @@ namespace fb {
 // ST_Y4 + k for NS = 4 << k).  Both are per-disk tile choices (disk_cx,
 // disk_ns; the autotuner sets them).
 enum { ST_ROWSUM, ST_CFL, ST_SOURCES, ST_BND_Z, ST_BND_Y, ST_COLL, ST_Z4, ST_Z8, ST_Z16, ST_Y4, ST_Y8, ST_Y16,
-       ST_X1, ST_X2, ST_X4, ST_X8, ST_X16, ST_NEWVEL, ST_FORCE, ST_N };
+       ST_X1, ST_X2, ST_X4, ST_X8, ST_X16, ST_NEWVEL, ST_FORCE, ST_CFL4, ST_NEWVEL4, ST_N };
 constexpr int NXC = 5, NNS = 3;
 
 // tile shapes shared with the one-disk launchers (fb_launch.cuh)
@@ -246,6 +246,19 @@ __global__ void __launch_bounds__(NV_BX) kb_newvel(const fb_disk_dev *ds, const 
 }
 
 // FP32 2D: column-marching rows (fb_sources32.cuh); 128 columns x NV32_R rows a tile
+static __global__ void __launch_bounds__(Q32_T) kb_cfl_cyl32q(const fb_disk_dev *ds, const int4 *items, int f) {
+  FB_TILE
+  b_cfl_cyl32q(dims_of(D), geo_of<float>(D.geom), (const float *)F.rho, (const float *)F.cs, (const float *)F.vx,
+               (const float *)F.vy, F.vxmed, F.vbg, (float)scp->nu, (float)scp->alpha, D.cfl, D.mindx,
+               (unsigned long long *)D.dtmin, (int)bid.x);
+}
+static __global__ void __launch_bounds__(Q32_T) kb_newvel_cyl32q(const fb_disk_dev *ds, const int4 *items, int f) {
+  FB_TILE
+  b_newvel_cyl32q(dims_of(D), geo_of<float>(D.geom), (const float *)F.rho_a, (const float *)F.mpx,
+                  (const float *)F.mmx, (const float *)F.mpy, (const float *)F.mmy, (float *)F.rho, (float *)F.vx,
+                  (float *)F.vy, (const float *)F.rho0, (const float *)F.vx0, (const float *)F.vy0, D.ramps,
+                  D.stockholm, scp, (int)bid.x);
+}
 static __global__ void __launch_bounds__(128, FB_NV32_MINB) kb_newvel_cyl32(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   b_newvel_cyl32(dims_of(D), geo_of<float>(D.geom), (const float *)F.rho_a, (const float *)F.mpx,
@@ -376,11 +389,15 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v, int chain = -1) {
     if (chain >= 0 && B->chain_of[di] != chain) continue;
     const fb_disk_dev &D = *fb_disk_internal_dev(B->disks[di]);
     const int nx = D.nx, ny = D.ny, nz = D.nz, sy = D.sy, sz = D.sz;
+    // FP32 2D disks whose rings hold a multiple of 4 cells: CFL and
+    // NewVelocity four cells a thread (fb_sources32.cuh)
+    const bool quad = !D.is3d && B->precision == FB_FP32 && nx % 4 == 0;
     dim3 g(1, 1, 1);
     switch (st) {
       case ST_ROWSUM: g = dim3(B->precision == FB_FP64 ? (sy * sz + 31) / 32 : (sy * sz + 7) / 8); break;
       case ST_CFL:
-        if (!D.is3d && B->precision == FB_FP32) g = dim3((nx + 127) / 128, (ny + CFL32_R - 1) / CFL32_R);
+        if (quad) g = dim3(0);
+        else if (!D.is3d && B->precision == FB_FP32) g = dim3((nx + 127) / 128, (ny + CFL32_R - 1) / CFL32_R);
         else g = dim3((ny + CFL_R - 1) / CFL_R, D.is3d ? nz : 1);
         break;
       case ST_SOURCES:
@@ -414,8 +431,12 @@ static int tiles(fb_batch *B, int st, std::vector<int4> &v, int chain = -1) {
         g = D.feeldisk ? dim3((nr + 127) / 128) : dim3(0);
         break;
       }
+      case ST_CFL4: case ST_NEWVEL4:
+        g = quad ? dim3((nx / 4 * ny + Q32_T - 1) / Q32_T) : dim3(0);
+        break;
       case ST_NEWVEL:
-        if (!D.is3d && B->precision == FB_FP32) g = dim3((nx + 127) / 128, (ny + NV32_R - 1) / NV32_R);
+        if (quad) g = dim3(0);
+        else if (!D.is3d && B->precision == FB_FP32) g = dim3((nx + 127) / 128, (ny + NV32_R - 1) / NV32_R);
         else g = dim3((nx + NV_BX - 1) / NV_BX, (ny + NV_R - 1) / NV_R, D.is3d ? nz : 1);
         break;
     }
@@ -466,7 +487,7 @@ template <typename T, typename S, typename TC = T, typename TX = T, typename TN 
 static int launch_step(fb_batch *B, double DT, int chain) {
   int4 *const *items = chain < 0 ? B->items : B->citems[chain];
   const int *nitems = chain < 0 ? B->nitems : B->ncitems[chain];
-  if (nitems[ST_CFL] == 0) return 0;  // no active disk
+  if (nitems[ST_ROWSUM] == 0) return 0;  // no active disk
   configure_sweep_x<TX, S>(B);
   cudaStream_t st = chain < 0 ? B->stream : B->cstream[chain];
   pmark(st, "start");
@@ -479,6 +500,8 @@ static int launch_step(fb_batch *B, double DT, int chain) {
   }
   pmark(st, "rowsum");
   for (int f = 0; f < nf; f++) {
+    if (nitems[ST_CFL4]) kb_cfl_cyl32q<<<grid(ST_CFL4), Q32_T, 0, st>>>(ds, items[ST_CFL4], f);
+    if (!nitems[ST_CFL]) continue;
     if (!B->is3d && sizeof(S) == 4) kb_cfl_cyl32<<<grid(ST_CFL), 128, 0, st>>>(ds, items[ST_CFL], f);
     else kb_cfl<TF, S><<<grid(ST_CFL), 256, 0, st>>>(ds, items[ST_CFL], f);
   }
@@ -553,8 +576,11 @@ static int launch_step(fb_batch *B, double DT, int chain) {
     pmark(st, "sweep_x");
   }
   for (int f = 0; f < nf; f++) {
-    if (!B->is3d && sizeof(S) == 4) kb_newvel_cyl32<<<grid(ST_NEWVEL), 128, 0, st>>>(ds, items[ST_NEWVEL], f);
-    else kb_newvel<TN, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, items[ST_NEWVEL], f);
+    if (nitems[ST_NEWVEL4]) kb_newvel_cyl32q<<<grid(ST_NEWVEL4), Q32_T, 0, st>>>(ds, items[ST_NEWVEL4], f);
+    if (nitems[ST_NEWVEL]) {
+      if (!B->is3d && sizeof(S) == 4) kb_newvel_cyl32<<<grid(ST_NEWVEL), 128, 0, st>>>(ds, items[ST_NEWVEL], f);
+      else kb_newvel<TN, S><<<grid(ST_NEWVEL), NV_BX, 0, st>>>(ds, items[ST_NEWVEL], f);
+    }
     pmark(st, "newvel");
     if (B->is3d) kb_bnd<T, S><<<grid(ST_BND_Z), BND_BX, 0, st>>>(ds, items[ST_BND_Z], f, 0, 1);
     kb_bnd<T, S><<<grid(ST_BND_Y), BND_BX, 0, st>>>(ds, items[ST_BND_Y], f, 0, 0);

@@ -822,6 +822,80 @@ int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, co
   return FB_OK;
 }
 
+/* Fluid f's state of n disks that share one stream (the members of a batch):
+ * every disk's transfers are queued on that stream (through the one device
+ * staging chunk for FP32 disks: the stream orders its reuse) and waited for
+ * once, instead of once per disk.  Arrays of n host pointers; a NULL array
+ * or entry leaves that field or disk as it is. */
+int fb_disks_set_state(fb_disk **ds, int n, int f, const double *const *rho, const double *const *vx,
+                       const double *const *vy, const double *const *vz, const double *const *cs) {
+  int i, q, rc = FB_OK;
+  double *st = NULL;
+  if (n <= 0) return FB_OK;
+  for (i = 0; i < n; i++)
+    if (!ds[i] || f < 0 || f >= ds[i]->p.nfluids || ds[i]->stream != ds[0]->stream ||
+        ds[i]->device != ds[0]->device || ds[i]->d.precision != ds[0]->d.precision)
+      return fail(FB_ERR_ARG, "disks of one stream, device and precision with fluid %d", f);
+  CU(cudaSetDevice(ds[0]->device));
+  if (ds[0]->d.precision == FB_FP32 && !(st = dstage_lock(ds[0]->device))) return fail(FB_ERR_CUDA, "device staging");
+  for (i = 0; i < n && !rc; i++) {
+    fb_disk *D = ds[i];
+    fb_fluid_dev *F = &D->d.fl[f];
+    const double *src[5] = {rho ? rho[i] : NULL, vx ? vx[i] : NULL, vy ? vy[i] : NULL,
+                            vz && D->d.is3d ? vz[i] : NULL, cs ? cs[i] : NULL};
+    void *dst[5] = {F->rho, F->vx, F->vy, F->vz, F->cs};
+    for (q = 0; q < 5 && !rc; q++) {
+      if (!src[q] || !dst[q]) continue;
+      if (st) {
+        if (q == 1 ? stage_move_vx(D, f, st, (double *)src[q], dst[q], 1)
+                   : stage_move(D, st, (double *)src[q], dst[q], (size_t)D->ncell, 1))
+          rc = fail(FB_ERR_CUDA, "state upload");
+      } else if (cudaMemcpyAsync(dst[q], src[q], (size_t)D->ncell * sizeof(double), cudaMemcpyHostToDevice,
+                                 D->stream) != cudaSuccess) {
+        rc = fail(FB_ERR_CUDA, "state upload");
+      }
+    }
+  }
+  if (cudaStreamSynchronize(ds[0]->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state upload");
+  if (st) stage_unlock();
+  return rc;
+}
+
+int fb_disks_get_state(fb_disk **ds, int n, int f, double *const *rho, double *const *vx, double *const *vy,
+                       double *const *vz) {
+  int i, q, rc = FB_OK;
+  double *st = NULL;
+  if (n <= 0) return FB_OK;
+  for (i = 0; i < n; i++)
+    if (!ds[i] || f < 0 || f >= ds[i]->p.nfluids || ds[i]->stream != ds[0]->stream ||
+        ds[i]->device != ds[0]->device || ds[i]->d.precision != ds[0]->d.precision)
+      return fail(FB_ERR_ARG, "disks of one stream, device and precision with fluid %d", f);
+  CU(cudaSetDevice(ds[0]->device));
+  if (ds[0]->d.precision == FB_FP32 && !(st = dstage_lock(ds[0]->device))) return fail(FB_ERR_CUDA, "device staging");
+  for (i = 0; i < n && !rc; i++) {
+    fb_disk *D = ds[i];
+    fb_fluid_dev *F = &D->d.fl[f];
+    double *dst[4] = {rho ? rho[i] : NULL, vx ? vx[i] : NULL, vy ? vy[i] : NULL, vz && D->d.is3d ? vz[i] : NULL};
+    const void *src[4] = {F->rho, F->vx, F->vy, F->vz};
+    for (q = 0; q < 4 && !rc; q++) {
+      if (!src[q] || !dst[q]) continue;
+      if (st) {
+        if (q == 1 ? stage_move_vx(D, f, st, dst[q], (void *)src[q], 0)
+                   : stage_move(D, st, dst[q], (void *)src[q], (size_t)D->ncell, 0))
+          rc = fail(FB_ERR_CUDA, "state download");
+      } else if (cudaMemcpyAsync(dst[q], src[q], (size_t)D->ncell * sizeof(double), cudaMemcpyDeviceToHost,
+                                 D->stream) != cudaSuccess) {
+        rc = fail(FB_ERR_CUDA, "state download");
+      }
+    }
+  }
+  if (cudaStreamSynchronize(ds[0]->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state download");
+  if (st) stage_unlock();
+  for (i = 0; i < n; i++)
+    if (!ds[i]->d.is3d && vz && vz[i]) memset(vz[i], 0, sizeof(double) * ds[i]->ncell);
+  return rc;
+}
+
 int fb_disk_get_energy(fb_disk *D, int f, double *e) {
   if (!D || !e || f < 0 || f >= D->p.nfluids) return fail(FB_ERR_ARG, "bad disk/fluid");
   CU(cudaSetDevice(D->device));

@@ -505,4 +505,120 @@ __device__ __forceinline__ void b_cfl_cyl32(const Dims m, const Geo<float> g, co
   cfl_commit(mnd, dtmin);
 }
 
+// ---------------------------------------------------------------------------
+// CFL limits and NewVelocity of FP32 2D disks whose rings hold a multiple of
+// four cells: a thread takes four consecutive cells of a row with 16-byte
+// loads (and stores), so the fields stream like a copy.  The x neighbour of
+// its last (CFL) or first (NewVelocity) cell comes from the next or previous
+// lane when that lane holds the adjacent four cells of the same row, else
+// from one load; the row above (CFL: vy) or below (NewVelocity: density and
+// radial momentum) by a second 16-byte load.  Per cell the arithmetic of
+// b_cfl_cyl32 / b_newvel_cyl32; a CTA of Q32_T threads takes 4 Q32_T cells.
+constexpr int Q32_T = 128;
+__device__ __forceinline__ float4 ld4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ float q4(const float4 &a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : (k == 2 ? a.z : a.w)); }
+
+__device__ __forceinline__ void b_cfl_cyl32q(const Dims m, const Geo<float> g, const float *__restrict__ rho,
+    const float *__restrict__ cs, const float *__restrict__ vx, const float *__restrict__ vy,
+    const double *__restrict__ vxmed, const double *__restrict__ vbg, float nu, float alpha, double cfl_num,
+    double mindx, unsigned long long *__restrict__ dtmin, int blk) {
+  const int lane = threadIdx.x & 31;
+  const int qpr = m.nx >> 2, nq = qpr * m.ny;
+  const int t = blk * Q32_T + (int)threadIdx.x;
+  const bool act = t < nq;
+  const int tc = act ? t : nq - 1;
+  const int j = FB_NGH + tc / qpr, q = tc - (j - FB_NGH) * qpr;
+  const long long l = m.l(4 * q, j, 0);
+  const float4 r4 = ld4(rho + l), c4 = ld4(cs + l), u4 = ld4(vx + l), v4 = ld4(vy + l), vp4 = ld4(vy + l + m.pitch);
+  // vx of cell 4q + 4: the next lane's first cell, or a load (ring wrap, warp edge)
+  float uxp3 = __shfl_down_sync(0xffffffffu, u4.x, 1);
+  if (lane == 31 || q == qpr - 1) uxp3 = vx[q == qpr - 1 ? m.l(0, j, 0) : l + 4];
+  const float cflf = (float)cfl_num;
+  const float vmf = (float)(vxmed[j] - bg_at(vbg, j));
+  const float izx = ld(g.invdiffxmed + 0) * ld(g.inv_ymed + j), izy = 1.0f / ld(g.sxj + j);
+  const float vj = ld(g.visc_j + j);
+  const float mx7 = fmaxf(izx, izy);
+  float mn = 1e20f;
+  bool bad = false;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const float c = q4(c4, k), u = q4(u4, k), v = q4(v4, k), vyp = q4(vp4, k);
+    const float uxp = k < 3 ? q4(u4, k + 1) : uxp3;
+    const float visc = m.alpha ? alpha * c * c * vj : nu;
+    const float c1 = fabsf(c) * mx7;
+    const float c2 = fmaxf(fabsf(u - vmf), fabsf(uxp - vmf)) * izx;
+    const float c3 = fmaxf(fabsf(v), fabsf(vyp)) * izy;
+    const float c5 = fmaxf(fabsf(uxp - u) * izx, fabsf(vyp - v) * izy) * (4.0f * (float)FB_CVNR);
+    const float c7 = 4.0f * visc * (mx7 * mx7);
+    const float dtc = cflf * rsqrtf(c1 * c1 + c2 * c2 + c3 * c3 + c5 * c5 + c7 * c7);
+    bad |= !(dtc == dtc) || !(q4(r4, k) > 0.0f);
+    mn = fminf(mn, dtc);
+  }
+  double mnd = act ? (double)mn : 1e20;
+  if (!act) bad = false;
+  if (act && q == 0) {   // the shear limit of row j (once per row)
+    const double shear = cfl_shear(g, vxmed, cfl_num, mindx, j, j);
+    if (shear < mnd) mnd = shear;
+  }
+  if (bad) atomicOr(dtmin + 1, 1ull);
+  cfl_commit(mnd, dtmin);
+}
+
+__device__ __forceinline__ void b_newvel_cyl32q(const Dims m, const Geo<float> g, const float *__restrict__ rt,
+    const float *__restrict__ mpx, const float *__restrict__ mmx, const float *__restrict__ mpy,
+    const float *__restrict__ mmy, float *__restrict__ rho, float *__restrict__ vx, float *__restrict__ vy,
+    const float *__restrict__ rho0, const float *__restrict__ vx0, const float *__restrict__ vy0,
+    const double *__restrict__ ramps, int stockholm, const fb_scalars *__restrict__ sc, int blk) {
+  const int lane = threadIdx.x & 31;
+  const int qpr = m.nx >> 2, nq = qpr * m.ny;
+  const int t = blk * Q32_T + (int)threadIdx.x;
+  const bool act = t < nq;
+  const int tc = act ? t : nq - 1;
+  const int j = FB_NGH + tc / qpr, q = tc - (j - FB_NGH) * qpr;
+  const long long l = m.l(4 * q, j, 0);
+  const float4 r4 = ld4(rt + l), mmx4 = ld4(mmx + l), mpx4 = ld4(mpx + l), mmy4 = ld4(mmy + l), mpy4 = ld4(mpy + l);
+  const float4 rm4 = ld4(rt + l - m.pitch), pym4 = ld4(mpy + l - m.pitch);
+  // cell 4q - 1: the previous lane's last cell, or a load (ring wrap, warp edge)
+  float rxm0 = __shfl_up_sync(0xffffffffu, r4.w, 1), pxm0 = __shfl_up_sync(0xffffffffu, mpx4.w, 1);
+  if (lane == 0 || q == 0) {
+    const long long lm = q > 0 ? l - 1 : m.l(m.nx - 1, j, 0);
+    rxm0 = rt[lm];
+    pxm0 = mpx[lm];
+  }
+  const float dt = (float)sc->dt, dof = (float)(sc->omegaframe - sc->omegaframe0);
+  const float ivj = ld(g.invvj + j), ivjm = ld(g.invvj + j - 1), rc = ld(g.ymed + j);
+  float ramp = 0.0f, taud = 0.0f, vx0t = 0.0f, r0 = 0.0f, vy0j = 0.0f;
+  if (stockholm) {
+    ramp = (float)ramps[j];
+    if (ramp > 0.0f) {
+      taud = ld(g.tau_j + j) / ramp;
+      vx0t = vx0[j] - dof * rc;
+      r0 = rho0[j];
+      vy0j = vy0[j];
+    }
+  }
+  float o_r[4], o_u[4], o_v[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const float r = q4(r4, k);
+    const float rxm = k > 0 ? q4(r4, k - 1) : rxm0, mpxm = k > 0 ? q4(mpx4, k - 1) : pxm0;
+    float nvx = __fdiv_rn(q4(mmx4, k) + mpxm, (r + rxm) * rc);
+    float nvy = __fdiv_rn(q4(mmy4, k) * ivjm + q4(pym4, k) * ivj, r * ivjm + q4(rm4, k) * ivj);
+    float nrho = r;
+    if (stockholm && ramp > 0.0f) {
+      nrho = (nrho * taud + r0 * dt) / (dt + taud);
+      nvx = (nvx * taud + vx0t * dt) / (dt + taud);
+      nvy = (nvy * taud + vy0j * dt) / (dt + taud);
+    }
+    o_r[k] = nrho;
+    o_u[k] = nvx;
+    o_v[k] = nvy;
+  }
+  if (act) {
+    reinterpret_cast<float4 *>(rho + l)[0] = make_float4(o_r[0], o_r[1], o_r[2], o_r[3]);
+    reinterpret_cast<float4 *>(vx + l)[0] = make_float4(o_u[0], o_u[1], o_u[2], o_u[3]);
+    reinterpret_cast<float4 *>(vy + l)[0] = make_float4(o_v[0], o_v[1], o_v[2], o_v[3]);
+  }
+}
+
 }  // namespace fb

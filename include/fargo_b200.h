@@ -250,6 +250,15 @@ int fb_batch_set_tiles(fb_batch *b, int slot, int sweep_x_cells, int col_segment
  * Results do not depend on it (each disk's arithmetic is the same). */
 int fb_batch_set_chains(fb_batch *b, int chains);
 int fb_batch_get_chains(fb_batch *b);
+/* Fluid `fluid`'s state of every member in one call (FARGO3D layout, as
+ * fb_disk_set_state / fb_disk_get_state): arrays of one host pointer per
+ * slot; a NULL array or entry skips that field or slot.  The transfers of all
+ * members are queued on the batch's stream and waited for once, so page-
+ * locked buffers move back to back by DMA. */
+int fb_batch_set_states(fb_batch *b, int fluid, const double *const *rho, const double *const *vx,
+                        const double *const *vy, const double *const *vz, const double *const *cs);
+int fb_batch_get_states(fb_batch *b, int fluid, double *const *rho, double *const *vx, double *const *vy,
+                        double *const *vz);
 
 /* Device bytes: an upper bound of what fb_disk_create requests for these
  * parameters, and what a disk actually requested. */

@@ -113,6 +113,43 @@ def test_concurrent_chains_give_the_same_bits(precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_state_transfers_of_all_members(precision):
+    """fb_batch_set_states / fb_batch_get_states move every member's state in
+    one call and give the same bits as the per-member calls, into page-locked
+    and ordinary buffers; a NULL entry leaves that member as it is."""
+    import torch
+    from fargo3d_b200 import Batch, initial_state
+    cfgs = small_mix()
+    sts = [initial_state(c) for c in cfgs]
+    a, b = Batch(cfgs, precision), Batch(cfgs, precision)
+    for i, st in enumerate(sts):
+        a.set_state(i, *st)
+    b.set_states([tuple(torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy() if x is not None else None
+                        for x in st) for st in sts])
+    a.initialize()
+    b.initialize()
+    a.run(4)
+    b.run(4)
+    outs = [{k: torch.empty(c.shape, dtype=torch.float64).pin_memory().numpy() for k in ("rho", "vx", "vy")}
+            for c in cfgs]
+    got = b.states(out=outs)
+    for i in range(len(cfgs)):
+        want = a.state(i)
+        assert np.shares_memory(got[i]["rho"], outs[i]["rho"])
+        for k in ("rho", "vx", "vy"):
+            assert np.array_equal(got[i][k], want[k]), (i, k)
+    # a NULL entry: member 1 keeps its state
+    before = b.state(1)
+    b.set_states([sts[0], None, sts[2], sts[3]])
+    after = b.state(1)
+    for k in ("rho", "vx", "vy"):
+        assert np.array_equal(before[k], after[k]), k
+    a.close()
+    b.close()
+
+
+@pytest.mark.gpu
 def test_batch_failing_member_is_frozen_others_continue():
     """Fault injection on the host: one member starts with a NaN density.
     It is frozen with FB_ERR_NONFINITE; the others match their solo runs."""
