@@ -535,7 +535,7 @@ void ref_initialize(void) {
 /* One pass of the DT loop body of main.c:361-448. */
 #ifdef FB_DROPIN
 /* fargo3d_b200/integration/b200_hydro.c: the FARGO3D-side binding of the
- * B200 library, compiled into this build in place of the step's body */
+ * B200 library, compiled into the reference build in place of the step's body */
 void B200_HydroStep(real DT_interval, real *dt);
 void B200_Sync(void);
 #endif
@@ -589,7 +589,7 @@ void ref_get_scalars(double *o) {
 }
 
 /* output.c is compiled in for its merged writer: the writers it can select
- * that this build leaves out, and its monitoring hook, are no-ops here. */
+ * that the reference build here leaves out, and its monitoring hook, are no-ops here. */
 void MakeDir(char *s) { (void)s; }
 void Summary(int n) { (void)n; }
 void WriteVTK(Field *f, int n) { (void)f; (void)n; }

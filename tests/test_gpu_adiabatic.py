@@ -1,4 +1,4 @@
-"""The adiabatic equation of state (SURVEY rows a10/f4): SubStep3, the
+"""The adiabatic equation of state: SubStep3, the
 adiabatic pressure and sound speed, the artificial viscosity's heating and
 the energy's transport, on the CUDA FP64 path, against the reference's own C
 sources compiled with ADIABATIC (oracle/_ref/libfargo_ref_cyl2d_ad.so: the

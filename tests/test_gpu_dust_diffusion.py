@@ -1,4 +1,4 @@
-"""Dust diffusion (SURVEY row f2: DustDiffusion_Main, dust_diffusion_main.c,
+"""Dust diffusion (DustDiffusion_Main, dust_diffusion_main.c,
 dust_diffusion_core.c, dust_diffusion_coefficients.c) on the CUDA FP64 path,
 against the reference's own C sources compiled with the stock
 fargo_multifluid flags including DUSTDIFFUSION (oracle/_ref/

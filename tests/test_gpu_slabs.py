@@ -1,6 +1,6 @@
-"""A disk stepped as radial slabs (fargo3d_b200/slabs.py, SURVEY row f3)
-gives the whole disk's result bit for bit: every slab here runs on the one
-GPU of this run with its halos exchanged through device buffers; the
+"""A disk stepped as radial slabs (fargo3d_b200/slabs.py)
+gives the whole disk's result bit for bit: every slab here runs on one GPU
+with its halos exchanged through device buffers; the
 multi-process form (one slab per GPU, NCCL) uses the same library calls and
 is tested on CPU ranks in tests/test_slabs.py."""
 import numpy as np
