@@ -139,6 +139,21 @@ size_t fb_disk_internal_esz(struct fb_disk *d);
 int fb_internal_fail(int code, const char *what, int cuda_err);
 /* FP64 <-> FP32 copy of n values on the device (fb_kernels_f64.cu) */
 int fb_launch_convert(void *dst, const void *src, size_t n, int to_f32, void *stream);
+/* several FP64 <-> FP32 conversions of a staging chunk in one launch: segment
+   k moves n values between staging offset off and the FP32 field f, less (to
+   FP32) or plus (to FP64) the per-ring offset bg[i / nx] when bg is set */
+#define FB_MAXSEG 48
+typedef struct {
+  float *f;
+  const double *bg;
+  long long off, n;
+  int nx;
+} fb_seg;
+typedef struct {
+  int n;
+  fb_seg s[FB_MAXSEG];
+} fb_segs;
+int fb_launch_convert_segs(double *st, const fb_segs *segs, int to_f32, void *stream);
 /* the same for values of whole rings of nx cells less (to FP32) or plus (to
  * FP64) the per-ring offset off[ring0 + i / nx] */
 int fb_launch_convert_off(void *dst, const void *src, size_t n, int to_f32, const double *off, int nx,

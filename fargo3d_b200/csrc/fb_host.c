@@ -496,7 +496,7 @@ size_t fb_disk_internal_arena_bytes(const fb_params *p, int precision) {
 
 int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out) {
   fb_disk *D;
-  int f, n, rc, ndev = 0;
+  int f, rc, ndev = 0;
   long long nc;
   cudaError_t e;
   *out = NULL;
@@ -764,35 +764,6 @@ static int stage_move(fb_disk *D, double *st, double *host, void *field, size_t 
   return 0;
 }
 
-/* The azimuthal velocity of an FP32 fluid crosses as vx - vbg(ring), whole
- * rings per chunk.  The first vx given sets the background: its rings' FP64
- * means (then vbg * R's neighbour differences for the column sweeps). */
-static int stage_move_vx(fb_disk *D, int f, double *st, double *host, void *field, int to_f32) {
-  fb_fluid_dev *F = &D->d.fl[f];
-  const size_t nx = (size_t)D->d.nx, rings = (size_t)D->d.sy * D->d.sz, rpc = DSTAGE_N / nx;
-  const int first = to_f32 && !F->has_bg;
-  size_t r0;
-  if (rpc == 0 || !F->vbg) return 1;
-  for (r0 = 0; r0 < rings; r0 += rpc) {
-    const size_t nr = rings - r0 < rpc ? rings - r0 : rpc, c = nr * nx, o = r0 * nx;
-    if (to_f32) {
-      if (cudaMemcpyAsync(st, host + o, c * sizeof(double), cudaMemcpyHostToDevice, D->stream) != cudaSuccess ||
-          (first && fb_launch_ring_mean(F->vbg + r0, st, (int)nx, (int)nr, D->stream) != cudaSuccess) ||
-          fb_launch_convert_off((float *)field + o, st, c, 1, F->vbg, (int)nx, (long long)r0, D->stream) != cudaSuccess)
-        return 1;
-    } else {
-      if (fb_launch_convert_off(st, (float *)field + o, c, 0, F->vbg, (int)nx, (long long)r0, D->stream) != cudaSuccess ||
-          cudaMemcpyAsync(host + o, st, c * sizeof(double), cudaMemcpyDeviceToHost, D->stream) != cudaSuccess)
-        return 1;
-    }
-  }
-  if (first) {
-    if (fb_launch_bg_diffs(&D->d, f, D->stream) != cudaSuccess) return 1;
-    F->has_bg = 1;
-  }
-  return 0;
-}
-
 int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, const double *vy, const double *vz,
                       const double *cs) {
   fb_fluid_dev *F;
@@ -801,18 +772,9 @@ int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, co
   CU(cudaSetDevice(D->device));
   F = &D->d.fl[f];
   if (D->d.precision == FB_FP32) {
-    const double *src[5] = {rho, vx, vy, D->d.is3d ? vz : NULL, cs};
-    void *dst[5] = {F->rho, F->vx, F->vy, F->vz, F->cs};
-    const size_t n = (size_t)D->ncell;
-    double *st = dstage_lock(D->device);
-    if (!st) return fail(FB_ERR_CUDA, "device staging");
-    for (q = 0; q < 5 && !rc; q++)
-      if (src[q] && dst[q] &&
-          (q == 1 ? stage_move_vx(D, f, st, (double *)src[q], dst[q], 1) : stage_move(D, st, (double *)src[q], dst[q], n, 1)))
-        rc = fail(FB_ERR_CUDA, "state upload");
-    if (cudaStreamSynchronize(D->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state upload");
-    stage_unlock();
-    return rc;
+    (void)F;
+    (void)q;
+    return fb_disks_set_state(&D, 1, f, &rho, &vx, &vy, &vz, &cs);
   }
   if ((rc = put(D, F->rho, rho)) || (rc = put(D, F->vx, vx)) || (rc = put(D, F->vy, vy)) ||
       (rc = put(D, F->cs, cs)))
@@ -820,6 +782,71 @@ int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, co
   if (D->d.is3d && (rc = put(D, F->vz, vz))) return rc;
   CU(cudaStreamSynchronize(D->stream));
   return FB_OK;
+}
+
+/* Chunked transfers for FP32 disks: the host doubles of many fields (of
+ * many disks) are packed back to back into the device staging chunk and
+ * converted by one launch per chunk (and the reverse for reads: one launch,
+ * then the chunk's copies back to back).  Pieces of a field with a per-ring
+ * background end at ring boundaries. */
+typedef struct {
+  fb_segs s;
+  size_t fill;
+  double *st;
+  cudaStream_t stream;
+  int to_f32;
+  double *host[FB_MAXSEG];   /* reads: where each segment's doubles go */
+} seg_chunk;
+
+static int chunk_flush(seg_chunk *c) {
+  int k;
+  if (!c->s.n) return 0;
+  if (fb_launch_convert_segs(c->st, &c->s, c->to_f32, c->stream) != 0) return 1;
+  if (!c->to_f32)
+    for (k = 0; k < c->s.n; k++)
+      if (cudaMemcpyAsync(c->host[k], c->st + c->s.s[k].off, (size_t)c->s.s[k].n * sizeof(double),
+                          cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+        return 1;
+  c->s.n = 0;
+  c->fill = 0;
+  return 0;
+}
+
+/* n values of one field between host and the FP32 field f; bg: the field's
+ * per-ring background (rings of nx values), first_bg: where the ring means of
+ * this first upload go (the background is then bg itself) */
+static int chunk_add(seg_chunk *c, float *f, double *host, size_t n, const double *bg, int nx, double *first_bg) {
+  const size_t unit = bg ? (size_t)nx : 1;
+  size_t o = 0;
+  if (unit == 0 || unit > DSTAGE_N) return 1;
+  while (o < n) {
+    size_t room = DSTAGE_N - c->fill, take;
+    fb_seg *g;
+    room -= room % unit;
+    if (room == 0 || c->s.n == FB_MAXSEG) {
+      if (chunk_flush(c)) return 1;
+      continue;
+    }
+    take = n - o < room ? n - o : room;
+    if (c->to_f32) {
+      if (cudaMemcpyAsync(c->st + c->fill, host + o, take * sizeof(double), cudaMemcpyHostToDevice, c->stream) !=
+          cudaSuccess)
+        return 1;
+      if (first_bg && fb_launch_ring_mean(first_bg + o / unit, c->st + c->fill, nx, (int)(take / unit), c->stream))
+        return 1;
+    } else {
+      c->host[c->s.n] = host + o;
+    }
+    g = &c->s.s[c->s.n++];
+    g->f = f + o;
+    g->bg = bg ? bg + o / unit : NULL;
+    g->off = (long long)c->fill;
+    g->n = (long long)take;
+    g->nx = nx;
+    c->fill += take;
+    o += take;
+  }
+  return 0;
 }
 
 /* Fluid f's state of n disks that share one stream (the members of a batch):
@@ -838,23 +865,39 @@ int fb_disks_set_state(fb_disk **ds, int n, int f, const double *const *rho, con
       return fail(FB_ERR_ARG, "disks of one stream, device and precision with fluid %d", f);
   CU(cudaSetDevice(ds[0]->device));
   if (ds[0]->d.precision == FB_FP32 && !(st = dstage_lock(ds[0]->device))) return fail(FB_ERR_CUDA, "device staging");
-  for (i = 0; i < n && !rc; i++) {
-    fb_disk *D = ds[i];
-    fb_fluid_dev *F = &D->d.fl[f];
-    const double *src[5] = {rho ? rho[i] : NULL, vx ? vx[i] : NULL, vy ? vy[i] : NULL,
-                            vz && D->d.is3d ? vz[i] : NULL, cs ? cs[i] : NULL};
-    void *dst[5] = {F->rho, F->vx, F->vy, F->vz, F->cs};
-    for (q = 0; q < 5 && !rc; q++) {
-      if (!src[q] || !dst[q]) continue;
-      if (st) {
-        if (q == 1 ? stage_move_vx(D, f, st, (double *)src[q], dst[q], 1)
-                   : stage_move(D, st, (double *)src[q], dst[q], (size_t)D->ncell, 1))
+  {
+    seg_chunk c;
+    memset(&c, 0, sizeof c);
+    c.st = st;
+    c.stream = ds[0]->stream;
+    c.to_f32 = 1;
+    for (i = 0; i < n && !rc; i++) {
+      fb_disk *D = ds[i];
+      fb_fluid_dev *F = &D->d.fl[f];
+      const double *src[5] = {rho ? rho[i] : NULL, vx ? vx[i] : NULL, vy ? vy[i] : NULL,
+                              vz && D->d.is3d ? vz[i] : NULL, cs ? cs[i] : NULL};
+      void *dst[5] = {F->rho, F->vx, F->vy, F->vz, F->cs};
+      for (q = 0; q < 5 && !rc; q++) {
+        if (!src[q] || !dst[q]) continue;
+        if (st) {
+          /* the azimuthal velocity crosses as vx - vbg(ring); the first vx
+             given sets the background (its rings' FP64 means) */
+          const int bgq = q == 1, first = bgq && !F->has_bg;
+          if (bgq && !F->vbg) { rc = fail(FB_ERR_CUDA, "state upload"); break; }
+          if (chunk_add(&c, (float *)dst[q], (double *)src[q], (size_t)D->ncell, bgq ? F->vbg : NULL, D->d.nx,
+                        first ? F->vbg : NULL))
+            rc = fail(FB_ERR_CUDA, "state upload");
+          else if (first) {
+            if (fb_launch_bg_diffs(&D->d, f, D->stream) != cudaSuccess) rc = fail(FB_ERR_CUDA, "state upload");
+            F->has_bg = 1;
+          }
+        } else if (cudaMemcpyAsync(dst[q], src[q], (size_t)D->ncell * sizeof(double), cudaMemcpyHostToDevice,
+                                   D->stream) != cudaSuccess) {
           rc = fail(FB_ERR_CUDA, "state upload");
-      } else if (cudaMemcpyAsync(dst[q], src[q], (size_t)D->ncell * sizeof(double), cudaMemcpyHostToDevice,
-                                 D->stream) != cudaSuccess) {
-        rc = fail(FB_ERR_CUDA, "state upload");
+        }
       }
     }
+    if (st && !rc && chunk_flush(&c)) rc = fail(FB_ERR_CUDA, "state upload");
   }
   if (cudaStreamSynchronize(ds[0]->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state upload");
   if (st) stage_unlock();
@@ -872,22 +915,30 @@ int fb_disks_get_state(fb_disk **ds, int n, int f, double *const *rho, double *c
       return fail(FB_ERR_ARG, "disks of one stream, device and precision with fluid %d", f);
   CU(cudaSetDevice(ds[0]->device));
   if (ds[0]->d.precision == FB_FP32 && !(st = dstage_lock(ds[0]->device))) return fail(FB_ERR_CUDA, "device staging");
-  for (i = 0; i < n && !rc; i++) {
-    fb_disk *D = ds[i];
-    fb_fluid_dev *F = &D->d.fl[f];
-    double *dst[4] = {rho ? rho[i] : NULL, vx ? vx[i] : NULL, vy ? vy[i] : NULL, vz && D->d.is3d ? vz[i] : NULL};
-    const void *src[4] = {F->rho, F->vx, F->vy, F->vz};
-    for (q = 0; q < 4 && !rc; q++) {
-      if (!src[q] || !dst[q]) continue;
-      if (st) {
-        if (q == 1 ? stage_move_vx(D, f, st, dst[q], (void *)src[q], 0)
-                   : stage_move(D, st, dst[q], (void *)src[q], (size_t)D->ncell, 0))
+  {
+    seg_chunk c;
+    memset(&c, 0, sizeof c);
+    c.st = st;
+    c.stream = ds[0]->stream;
+    c.to_f32 = 0;
+    for (i = 0; i < n && !rc; i++) {
+      fb_disk *D = ds[i];
+      fb_fluid_dev *F = &D->d.fl[f];
+      double *dst[4] = {rho ? rho[i] : NULL, vx ? vx[i] : NULL, vy ? vy[i] : NULL, vz && D->d.is3d ? vz[i] : NULL};
+      void *src[4] = {F->rho, F->vx, F->vy, F->vz};
+      for (q = 0; q < 4 && !rc; q++) {
+        if (!src[q] || !dst[q]) continue;
+        if (st) {
+          if (q == 1 && !F->vbg) { rc = fail(FB_ERR_CUDA, "state download"); break; }
+          if (chunk_add(&c, (float *)src[q], dst[q], (size_t)D->ncell, q == 1 ? F->vbg : NULL, D->d.nx, NULL))
+            rc = fail(FB_ERR_CUDA, "state download");
+        } else if (cudaMemcpyAsync(dst[q], src[q], (size_t)D->ncell * sizeof(double), cudaMemcpyDeviceToHost,
+                                   D->stream) != cudaSuccess) {
           rc = fail(FB_ERR_CUDA, "state download");
-      } else if (cudaMemcpyAsync(dst[q], src[q], (size_t)D->ncell * sizeof(double), cudaMemcpyDeviceToHost,
-                                 D->stream) != cudaSuccess) {
-        rc = fail(FB_ERR_CUDA, "state download");
+        }
       }
     }
+    if (st && !rc && chunk_flush(&c)) rc = fail(FB_ERR_CUDA, "state download");
   }
   if (cudaStreamSynchronize(ds[0]->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state download");
   if (st) stage_unlock();
@@ -918,19 +969,9 @@ int fb_disk_get_state(fb_disk *D, int f, double *rho, double *vx, double *vy, do
   CU(cudaSetDevice(D->device));
   F = &D->d.fl[f];
   if (D->d.precision == FB_FP32) {
-    double *dst[4] = {rho, vx, vy, D->d.is3d ? vz : NULL};
-    const void *src[4] = {F->rho, F->vx, F->vy, F->vz};
-    const size_t n = (size_t)D->ncell;
-    double *st = dstage_lock(D->device);
-    if (!st) return fail(FB_ERR_CUDA, "device staging");
-    for (q = 0; q < 4 && !rc; q++)
-      if (dst[q] && src[q] &&
-          (q == 1 ? stage_move_vx(D, f, st, dst[q], (void *)src[q], 0) : stage_move(D, st, dst[q], (void *)src[q], n, 0)))
-        rc = fail(FB_ERR_CUDA, "state download");
-    if (cudaStreamSynchronize(D->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state download");
-    stage_unlock();
-    if (!D->d.is3d && vz) memset(vz, 0, sizeof(double) * D->ncell);
-    return rc;
+    (void)F;
+    (void)q;
+    return fb_disks_get_state(&D, 1, f, &rho, &vx, &vy, &vz);
   }
   if ((rc = get(D, rho, F->rho)) || (rc = get(D, vx, F->vx)) || (rc = get(D, vy, F->vy))) return rc;
   if (D->d.is3d && (rc = get(D, vz, F->vz))) return rc;
@@ -1225,7 +1266,7 @@ int fb_disk_halo(fb_disk *D, int which, int side, int unpack, void *buf, int hos
   return FB_OK;
 }
 
-int fb_disk_get_scalars(fb_disk *D, double *o) {
+int fb_disk_get_scalars(fb_disk *D, double o[8]) {
   if (!D || !o) return fail(FB_ERR_ARG, "null");
   const fb_psys *S = &D->ps;
   o[0] = S->phys_time; o[1] = S->omegaframe; o[2] = S->last_dt;

@@ -30,6 +30,25 @@ extern "C" int fb_launch_convert(void *dst, const void *src, size_t n, int to_f3
   return (int)cudaGetLastError();
 }
 
+__global__ void k_convert_segs(double *__restrict__ st, const fb_segs S, int to_f32) {
+  const fb_seg g = S.s[blockIdx.y];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.n; i += (long long)gridDim.x * blockDim.x) {
+    if (to_f32)
+      g.f[i] = __double2float_rn(g.bg ? st[g.off + i] - g.bg[i / g.nx] : st[g.off + i]);
+    else
+      st[g.off + i] = g.bg ? (double)g.f[i] + g.bg[i / g.nx] : (double)g.f[i];
+  }
+}
+extern "C" int fb_launch_convert_segs(double *st, const fb_segs *segs, int to_f32, void *stream) {
+  if (segs->n <= 0) return 0;
+  long long mx = 0;
+  for (int k = 0; k < segs->n; k++) mx = segs->s[k].n > mx ? segs->s[k].n : mx;
+  const long long b = (mx + 255) / 256;
+  const dim3 grid((unsigned)(b < 148 * 2 ? b : 148 * 2), (unsigned)segs->n);
+  k_convert_segs<<<grid, 256, 0, (cudaStream_t)stream>>>(st, *segs, to_f32);
+  return (int)cudaGetLastError();
+}
+
 // FP32 disks keep each fluid's azimuthal velocity relative to a per-ring
 // background: the conversions subtract (to FP32) or add back (to FP64) the
 // ring's value off[ring0 + i / nx] in double before rounding.
