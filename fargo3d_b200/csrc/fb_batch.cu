@@ -186,6 +186,7 @@ int fb_batch_destroy(fb_batch *B) {
     if (B->ev_join[c]) cudaEventDestroy(B->ev_join[c]);
   }
   if (B->ev_fork) cudaEventDestroy(B->ev_fork);
+  if (B->h_act) cudaFreeHost(B->h_act);
   if (B->d_disks) cudaFree(B->d_disks);
   if (B->d_psys) cudaFree(B->d_psys);
   for (fb_disk *d : B->disks)
@@ -253,28 +254,46 @@ int fb_batch_add(fb_batch *B, const fb_params *p, double t_end, int *slot) {
   return FB_OK;
 }
 
-int fb_batch_activate(fb_batch *B, int s) {
-  if (!B || s < 0 || s >= B->n || B->state[s] != 1) return FB_ERR_ARG;
+// Slot s's initialisation and descriptor uploads queued on the batch's stream
+// (the member's own stream); the caller waits.
+struct ActivationStage {   // page-locked source of one slot's activation uploads
+  fb_disk_dev dd;
+  fb_psys ps;
+  unsigned long long init[2];
+};
+static int activate_async(fb_batch *B, int s) {
   fb_disk *d = B->disks[s];
-  int rc = fb_disk_initialize(d);
+  int rc = fb_disk_internal_initialize_async(d);
   if (rc) return rc;
   if (cudaSetDevice(B->device) != cudaSuccess) return FB_ERR_CUDA;
-  // CFL minimum start and flag word; the scalars were uploaded by
-  // fb_disk_initialize
-  unsigned long long init[2] = {0x4415AF1D78B58C40ULL, 0ull};
-  fb_psys ps = *fb_disk_internal_psys(d);
-  ps.t_end = B->t_end[s];
-  const fb_disk_dev *dd = fb_disk_internal_dev(d);
-  // the batch's stream may still be running other members: order the
-  // uploads on it
-  if (cudaMemcpyAsync(dd->dtmin, init, sizeof init, cudaMemcpyHostToDevice, B->stream) != cudaSuccess ||
-      cudaMemcpyAsync(B->d_psys + s, &ps, sizeof ps, cudaMemcpyHostToDevice, B->stream) != cudaSuccess ||
-      cudaMemcpyAsync(B->d_disks + s, dd, sizeof(fb_disk_dev), cudaMemcpyHostToDevice, B->stream) != cudaSuccess ||
-      cudaStreamSynchronize(B->stream) != cudaSuccess)
+  if (!B->h_act && cudaMallocHost(&B->h_act, sizeof(ActivationStage) * B->n) != cudaSuccess) {
+    B->h_act = nullptr;
+    return FB_ERR_NOMEM;
+  }
+  // CFL minimum start and flag word; the scalars were uploaded by the
+  // initialisation.  The uploads come from page-locked memory, so they are
+  // queued without waiting; the batch's stream may still be running other
+  // members: it orders them.
+  ActivationStage *a = (ActivationStage *)B->h_act + s;
+  a->init[0] = 0x4415AF1D78B58C40ULL;
+  a->init[1] = 0ull;
+  a->ps = *fb_disk_internal_psys(d);
+  a->ps.t_end = B->t_end[s];
+  a->dd = *fb_disk_internal_dev(d);
+  if (cudaMemcpyAsync(a->dd.dtmin, a->init, sizeof a->init, cudaMemcpyHostToDevice, B->stream) != cudaSuccess ||
+      cudaMemcpyAsync(B->d_psys + s, &a->ps, sizeof a->ps, cudaMemcpyHostToDevice, B->stream) != cudaSuccess ||
+      cudaMemcpyAsync(B->d_disks + s, &a->dd, sizeof(fb_disk_dev), cudaMemcpyHostToDevice, B->stream) != cudaSuccess)
     return FB_ERR_CUDA;
   B->state[s] = 2;
   B->dirty = 1;
   return FB_OK;
+}
+
+int fb_batch_activate(fb_batch *B, int s) {
+  if (!B || s < 0 || s >= B->n || B->state[s] != 1) return FB_ERR_ARG;
+  int rc = activate_async(B, s);
+  if (rc) return rc;
+  return cudaStreamSynchronize(B->stream) == cudaSuccess ? FB_OK : FB_ERR_CUDA;
 }
 
 int fb_batch_remove(fb_batch *B, int s) {
@@ -340,12 +359,13 @@ int fb_batch_disk(fb_batch *B, int i, fb_disk **d) {
 // Activate every reserved slot (the members' states set beforehand).
 int fb_batch_initialize(fb_batch *B) {
   if (!B) return FB_ERR_ARG;
-  for (int i = 0; i < B->n; i++) {
+  for (int i = 0; i < B->n; i++) {   // every reserved member, one wait
     if (B->state[i] != 1) continue;
-    int rc = fb_batch_activate(B, i);
+    int rc = activate_async(B, i);
     if (rc) return rc;
   }
-  return FB_OK;
+  cudaSetDevice(B->device);
+  return cudaStreamSynchronize(B->stream) == cudaSuccess ? FB_OK : FB_ERR_CUDA;
 }
 
 // Advance every active disk by nsteps hydro steps without host round trips.

@@ -368,6 +368,7 @@ struct fb_batch {
      latency-bound launches (the scalar step, reductions, boundaries, launch
      tails) overlap another's throughput-bound ones */
   void *lists;    /* one device allocation holding every work list below */
+  void *h_act;    /* page-locked staging of the members' activation uploads */
   int force_np;   /* planet indices that feel the disk in some member (0: none) */
   int nchains;
   cudaStream_t cstream[FB_MAX_CHAINS];

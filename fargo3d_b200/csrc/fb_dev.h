@@ -129,6 +129,7 @@ FB_DECL_LAUNCHERS(f32)
 struct fb_disk;
 fb_disk_dev *fb_disk_internal_dev(struct fb_disk *d);
 struct fb_psys_s *fb_disk_internal_psys(struct fb_disk *d);
+int fb_disk_internal_initialize_async(struct fb_disk *d);
 /* fluid f's state of n disks sharing one stream, one wait (fb_host.c) */
 int fb_disks_set_state(struct fb_disk **ds, int n, int f, const double *const *rho, const double *const *vx,
                        const double *const *vy, const double *const *vz, const double *const *cs);

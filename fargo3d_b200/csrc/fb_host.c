@@ -1082,7 +1082,9 @@ static int push_scalars(fb_disk *D) {
   return FB_OK;
 }
 
-int fb_disk_initialize(fb_disk *D) {
+/* fb_disk_initialize's work queued on the disk's stream without waiting (a
+ * batch initialises all its members this way and waits once) */
+int fb_disk_internal_initialize_async(fb_disk *D) {
   int f, rc;
   if (!D) return fail(FB_ERR_ARG, "null disk");
   CU(cudaSetDevice(D->device));
@@ -1099,6 +1101,12 @@ int fb_disk_initialize(fb_disk *D) {
                            cudaMemcpyDeviceToDevice, D->stream));
     }
   }
+  return FB_OK;
+}
+
+int fb_disk_initialize(fb_disk *D) {
+  int rc = fb_disk_internal_initialize_async(D);
+  if (rc) return rc;
   CU(cudaStreamSynchronize(D->stream));
   return FB_OK;
 }
