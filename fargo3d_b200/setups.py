@@ -63,6 +63,7 @@ class DiskConfig:
     inclination: float = 0.0
     nfluids: int = 1
     invstokes: Tuple[float, ...] = ()
+    epsilon: float = 0.0              # EPSILON, dust-to-gas ratio per dust fluid (0: 0.01 / (nfluids - 1))
     stockholm: bool = True
     dust_diffusion: bool = False      # DUSTDIFFUSION of the dust fluids (multifluid)
     adiabatic: bool = False           # ADIABATIC equation of state (else ISOTHERMAL)
@@ -160,9 +161,9 @@ def initial_state(cfg: DiskConfig, fluid: int = 0):
 
     2D: setups/fargo/condinit.c:23-45 with Sigma = Sigma0 r^-SigmaSlope
     (1 + noise U(-1,1)), v_phi from the pressure-supported rotation curve and
-    v_r = 0.  3D: setups/p3disof/condinit.c:21-50 (FlaringIndex = 0 branch),
-    with the same multiplicative density noise.  Dust fluids (fluid > 0) get
-    eps = 0.01 / (nfluids - 1) times the gas density, the Keplerian velocity
+    v_r = 0.  3D: setups/p3disof/condinit.c:21-50 (both FlaringIndex
+    branches), with the same multiplicative density noise.  Dust fluids (fluid > 0) get
+    eps = epsilon (default 0.01 / (nfluids - 1)) times the gas density, the Keplerian velocity
     without pressure support (2D) and no pressure (cs = 0)."""
     rng = np.random.default_rng(cfg.seed * 1000 + fluid)
     nzs, nys, nxs = cfg.shape
@@ -186,7 +187,11 @@ def initial_state(cfg: DiskConfig, fluid: int = 0):
         xi = ss + 1.0 + fi
         beta = 1.0 - 2.0 * fi
         hh = h * r ** fi
-        rho = cfg.sigma0 / math.sqrt(2.0 * math.pi) / h * r ** (-xi) * st ** (-beta - xi + 1.0 / (hh * hh)) * noise
+        if fi == 0.0:
+            rho = cfg.sigma0 / math.sqrt(2.0 * math.pi) / h * r ** (-xi) * st ** (-beta - xi + 1.0 / (hh * hh)) * noise
+        else:
+            rho = (cfg.sigma0 / math.sqrt(2.0 * math.pi) / h * r ** (-xi) * st ** (-xi - beta)
+                   * np.exp((1.0 - st ** (-2.0 * fi)) / 2.0 / fi / (hh * hh)) * noise)
         vx = omega * r * np.sqrt(st ** (-2.0 * fi) - (beta + xi) * hh * hh) - omegaframe * r * st
         cs = hh * np.sqrt(1.0 / r)
         vy = np.zeros(cfg.shape)
@@ -199,7 +204,7 @@ def initial_state(cfg: DiskConfig, fluid: int = 0):
         # dust (setups/fargo_multifluid/condinit.c:38-44): eps times the gas
         # density, Keplerian azimuthal velocity without pressure support, no
         # radial velocity, no sound speed
-        eps = 0.01 / max(cfg.nfluids - 1, 1)
+        eps = cfg.epsilon if cfg.epsilon > 0.0 else 0.01 / max(cfg.nfluids - 1, 1)
         rho = rho * eps
         cs = np.zeros(cfg.shape)
         if not cfg.is3d:

@@ -94,9 +94,11 @@ def ref_variant(cfg) -> str:
             raise ValueError("the compiled reference has one adiabatic variant: 2D, one fluid, alpha viscosity")
         return "cyl2d_ad"
     if cfg.nfluids > 1:
-        if cfg.nfluids != 5 or cfg.is3d or cfg.alpha_visc:
-            raise ValueError("the compiled reference has one multifluid variant: 2D, 5 fluids, constant nu")
-        return "mf5_dd" if getattr(cfg, "dust_diffusion", False) else "mf5"
+        dd = getattr(cfg, "dust_diffusion", False)
+        if cfg.is3d or cfg.alpha_visc or not (cfg.nfluids == 5 or (cfg.nfluids == 4 and dd)):
+            raise ValueError("the compiled reference's multifluid variants are 2D with constant nu: "
+                             "5 fluids, or 4 fluids with dust diffusion")
+        return "mf%d%s" % (cfg.nfluids, "_dd" if dd else "")
     if cfg.is3d:
         return "sph3d"
     return "cyl2d_alpha" if cfg.alpha_visc else "cyl2d"

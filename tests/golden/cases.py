@@ -1,8 +1,21 @@
-"""Small parity cases shared by the golden-vector generator and the tests."""
+"""Small parity cases shared by the golden-vector generator and the tests.
+
+The `*_par` cases are read from FARGO3D setup files (setups/<name>/<name>.par
+and .opt, planets/*.cfg beside them) by fargo3d_b200.parfile, with the mesh
+made small by a parameter redefinition, as FARGO3D's command line does."""
 import math
+import os
 
 from fargo3d_b200.setups import (DiskConfig, Planet, config_adiabatic2d, config_fargo2d, config_multifluid,
                                   config_p3disof)
+
+
+SETUPS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "setups")
+
+
+def _setup(name, redefine, seed):
+    from fargo3d_b200.parfile import load_setup
+    return load_setup(os.path.join(SETUPS, name), redefine=redefine, seed=seed).config
 
 
 def cases():
@@ -31,6 +44,12 @@ def cases():
         "cyl2d_ad": (config_adiabatic2d(48, 20, seed=9), 20, 0.2),
         # the multifluid flags with DUSTDIFFUSION
         "mf5_dd": (config_multifluid(32, 16, seed=10, dust_diffusion=True), 12, 1e30),
+        # read from setup files: the fargo disk (linear spacing, flat Sigma)
+        "fargo_par": (_setup("fargo_par", "Nx:32,Ny:16", 11), 20, 1e30),
+        # the p3disof disk: flared (FlaringIndex 0.5), Sigma ~ r^-1, q = 1e-5
+        "p3disof_par": (_setup("p3disof_par", "Nx:16,Ny:12,Nz:6", 12), 6, 1e30),
+        # the fargo_multifluid disk: 3 dust species as dense as the gas, diffusing
+        "mf4_par": (_setup("mf4_par", "Nx:32,Ny:16", 13), 12, 1e30),
     }
 
 

@@ -22,12 +22,16 @@ sys.path.insert(0, os.path.join(os.path.dirname(HERE), "oracle"))
 
 def configs():
     from fargo3d_b200 import Planet, config_adiabatic2d, config_fargo2d, config_multifluid, config_p3disof
+    from fargo3d_b200.parfile import load_setup
     return {
         "cyl2d": config_fargo2d(64, 24, seed=111).replace(planets=[Planet(1.0, 1e-3), Planet(1.4, 3e-4)]),
         "sph3d": config_p3disof(24, 12, 6, seed=112),
         "mf5": config_multifluid(48, 20, seed=113),
         "cyl2d_ad": config_adiabatic2d(48, 20, seed=114),
         "mf5_dd": config_multifluid(48, 20, seed=115, dust_diffusion=True),
+        # the fargo_multifluid disk as its setup files describe it (4 fluids, DUSTDIFFUSION)
+        "mf4_par": load_setup(os.path.join(HERE, "golden", "setups", "mf4_par"), redefine="Nx:48,Ny:20",
+                              seed=116).config,
     }
 
 
@@ -57,7 +61,7 @@ def _same(a, b, cfg):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["cyl2d", "sph3d", "mf5", "cyl2d_ad", "mf5_dd"])
+@pytest.mark.parametrize("name", ["cyl2d", "sph3d", "mf5", "cyl2d_ad", "mf5_dd", "mf4_par"])
 def test_stock_step_loop_on_the_b200(name):
     from fargo3d_b200 import initial_state
     cfg = configs()[name]
