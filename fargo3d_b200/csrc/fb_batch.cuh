@@ -151,7 +151,7 @@ static __global__ void __launch_bounds__(S32_WARPS * 32, FB_S32_MINB) kb_sources
 }
 
 template <typename T, typename S>
-__global__ void __launch_bounds__(SRC3_TX *SRC3_TY) kb_sources_sph(const fb_disk_dev *ds, const int4 *items, int f) {
+__global__ void __launch_bounds__(SRC3_TX *SRC3_TY, sizeof(T) == 4 ? 1 : FB_SPH64_MINB) kb_sources_sph(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   b_sources_sph<T, SRC3_TX, SRC3_TY, S>(dims_of(D), geo_of<T>(sizeof(T) == 8 ? D.geomd : D.geom), geo_of<double>(D.geomd), (const S *)F.rho,
                                      (const S *)F.cs, (const S *)F.vx, (const S *)F.vy, (const S *)F.vz, (S *)F.vxt,
@@ -186,7 +186,7 @@ static __global__ void __launch_bounds__(COL_BX, FB_COL32_MINB) kb_sweep_col32(c
 }
 
 template <typename T, int DIR, int COL_NS, typename S>
-__global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? FB_COL_MINB32 : 1) kb_sweep_col(const fb_disk_dev *ds, const int4 *items, int f) {
+__global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? FB_COL_MINB32 : FB_COL64_MINB) kb_sweep_col(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   Dims m = dims_of(D);
   const int ylo = FB_NGH - 1, yhi = m.ny + FB_NGH - 1;
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(COL_BX, sizeof(T) == 4 ? FB_COL_MINB32 : 1) kb
 }
 
 template <typename T, int C, typename S>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? FB_SX_MINB32 : 1) kb_sweep_x(const fb_disk_dev *ds, const int4 *items, int f) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? FB_SX_MINB32 : FB_SX64_MINB) kb_sweep_x(const fb_disk_dev *ds, const int4 *items, int f) {
   FB_TILE
   Dims m = dims_of(D);
   const bool b = m.is3d;

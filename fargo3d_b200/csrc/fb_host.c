@@ -459,7 +459,7 @@ int fb_disk_set_wait_limit(fb_disk *D, long long polls) {
 int fb_disk_get_tiles(fb_disk *D, int *cx, int *ns) {
   if (!D) return fail(FB_ERR_ARG, "null disk");
   if (cx) *cx = D->d.tile_cx ? D->d.tile_cx : default_cx(D->d.nx);
-  if (ns) *ns = D->d.tile_ns ? D->d.tile_ns : 8;
+  if (ns) *ns = D->d.tile_ns ? D->d.tile_ns : (D->d.precision == FB_FP64 ? 4 : 8);
   return FB_OK;
 }
 

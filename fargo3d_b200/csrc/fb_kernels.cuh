@@ -609,6 +609,12 @@ __device__ __forceinline__ void b_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
     et[l] = e;
   }
 }
+// resident CTAs per SM of the FP64 3D source stage (96 registers; the
+// shared-memory tiles allow 5): 1.36 -> 1.30 ms at 512x256x48
+#ifndef FB_SPH64_MINB
+#define FB_SPH64_MINB 5
+#endif
+
 template <typename T, int TX, int TY, typename S = T>
 __global__ void __launch_bounds__(TX *TY) k_sources_cyl(Dims m, Geo<T> g, Geo<double> gd,
     const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx,
@@ -1048,8 +1054,21 @@ __device__ __forceinline__ void b_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, in
   }
 }
 
+// resident CTAs per SM the FP64 sweeps are compiled for, i.e. their register
+// cap: 4 column-sweep CTAs of 128 threads and 2 azimuthal-sweep CTAs of 256
+// threads, 128 registers each.  Their FP64 arithmetic is latency-bound, so
+// the occupancy gained outweighs the few spilled values (3D 512x256x48: Y+Z
+// sweeps 2.98 -> 1.70 ms, azimuthal sweep 2.26 -> 1.72 ms with 2 cells per
+// thread; identical results, the register allocation changes no operation)
+#ifndef FB_COL64_MINB
+#define FB_COL64_MINB 4
+#endif
+#ifndef FB_SX64_MINB
+#define FB_SX64_MINB 2
+#endif
+
 template <typename T, int DIR, int NS, typename S = T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, int nq, int clo, int chi,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : FB_COL64_MINB) k_sweep_col(Dims m, Geo<T> g, QSrc<T, S> src, int nq, int clo, int chi,
                                                    int t2lo, S *__restrict__ rho_out, S *q_out0, S *q_out1,
                                                    S *q_out2, S *q_out3, S *q_out4, S *q_out5,
                                                    const fb_scalars *__restrict__ scp, const S *__restrict__ e_in,
@@ -1373,7 +1392,7 @@ __device__ __forceinline__ void b_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
   vzt[l] = az;
 }
 template <typename T, int TX, int TY, typename S = T>
-__global__ void __launch_bounds__(TX *TY) k_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 1 : FB_SPH64_MINB) k_sources_sph(Dims m, Geo<T> g, Geo<double> gd,
     const S *__restrict__ rho, const S *__restrict__ cs, const S *__restrict__ vx, const S *__restrict__ vy,
     const S *__restrict__ vz, S *__restrict__ vxt, S *__restrict__ vyt, S *__restrict__ vzt,
     const fb_scalars *__restrict__ scp, int dust, int viscous, const double *__restrict__ vbg) {
@@ -2075,7 +2094,10 @@ __host__ __device__ inline int sweep_x_chunk(int nx, int nt) {
 // Tile choices of a disk: the set value (fb_disk_set_tiles, usually from the
 // autotuner) or the default.
 inline int disk_cx(const fb_disk_dev &d) { return d.tile_cx ? d.tile_cx : sweep_x_chunk(d.nx, 256); }
-inline int disk_ns(const fb_disk_dev &d) { return d.tile_ns ? d.tile_ns : 8; }
+// FP64 column sweeps are compiled for 4 resident CTAs (128 registers), where
+// the 4-row segment needs no local memory; FP32 ones default to 8 rows
+inline int default_ns(int precision) { return precision == FB_FP64 ? 4 : 8; }
+inline int disk_ns(const fb_disk_dev &d) { return d.tile_ns ? d.tile_ns : default_ns(d.precision); }
 inline bool valid_cx(int nx, int c) { return (c == 1 || c == 2 || c == 4 || c == 8 || c == 16) && nx % c == 0 && nx / c <= 256; }
 inline bool valid_ns(int ns) { return ns == 4 || ns == 8 || ns == 16; }
 // polls of the staged-load wait before a disk is flagged (fb_disk_set_wait_limit)
@@ -2084,7 +2106,7 @@ __host__ __device__ inline long long wait_limit(const fb_disk_dev &d) {
 }
 
 template <typename T, int C, typename S = T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_sweep_x2(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : FB_SX64_MINB) k_sweep_x2(Dims m, Geo<T> g, Geo<double> gd, int nq, int jlo, int klo,
                                                   int nj, int nrings, S *rho, S *q0, S *q1, S *q2, S *q3, S *q4,
                                                   S *q5, const S *__restrict__ vxt,
                                                   const double *__restrict__ vxmed_t, int *__restrict__ nshift_out,
