@@ -427,26 +427,55 @@ def run_ours(args, rank, world, local_rank):
     dom_bytes = LAUNCH_WORDS[dim][dom] * esz * cells * (count[dom] if dom not in ("cfl", "rowsum") else nf)
     achieved = dom_bytes / (prof[dom] / 1e3) / 1e9
     runner.close()
-    # end-to-end through the public API from pinned host buffers
-    pinned = [[[torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in st] for st in sts]
-              for sts in inits]
-    # result buffers, page-locked like the inputs (vz only for 3D disks)
+    # end-to-end through the public API from page-locked host buffers: per
+    # fluid, one page-locked block holds every member's input fields and one
+    # its result fields, disk after disk in the order of the call (rho, vx,
+    # vy, [vz,] cs in; rho, vx, vy, [vz] out), as an application keeping a
+    # batch's state in one host buffer does
+    in_q = (0, 1, 2, 3, 4) if dim == "3d" else (0, 1, 2, 4)
     keys = ("rho", "vx", "vy", "vz") if dim == "3d" else ("rho", "vx", "vy")
-    results = [[{k: torch.empty(c.shape, dtype=torch.float64).pin_memory().numpy() for k in keys}
-                for _ in range(nf)] for c in cfgs]
+
+    def carve(block, shapes):
+        out, o = [], 0
+        for shp in shapes:
+            n = int(np.prod(shp))
+            out.append(block[o:o + n].view(*shp))
+            o += n
+        return out
+
+    pinned, results = [], [[None] * nf for _ in cfgs]
+    for f in range(nf):
+        shapes = [c.shape for c in cfgs for _ in in_q]
+        blk = torch.empty(sum(int(np.prod(s)) for s in shapes), dtype=torch.float64).pin_memory()
+        views = iter(carve(blk, shapes))
+        per = []
+        for i in range(len(cfgs)):
+            st = [None] * 5
+            for q in in_q:
+                v = next(views)
+                v.copy_(torch.from_numpy(np.ascontiguousarray(inits[i][f][q]).reshape(cfgs[i].shape)))
+                st[q] = v
+            per.append(st)
+        pinned.append(per)
+        shapes = [c.shape for c in cfgs for _ in keys]
+        rblk = torch.empty(sum(int(np.prod(s)) for s in shapes), dtype=torch.float64).pin_memory()
+        rviews = iter(carve(rblk, shapes))
+        for i in range(len(cfgs)):
+            results[i][f] = {k: next(rviews).numpy() for k in keys}
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    np_ = lambda st: [None if p is None else p.numpy() for p in st]
     if batched:
         r2 = Batch(cfgs, precision, device=local_rank)
         for f in range(nf):
-            r2.set_states([[p.numpy() for p in sts[f]] for sts in pinned], fluid=f)
+            r2.set_states([np_(st) for st in pinned[f]], fluid=f)
         r2.initialize()
         r2.run(args.steps)
         outs = [o for f in range(nf) for o in r2.states(f, out=[results[i][f] for i in range(len(cfgs))])]
     else:
         r2 = Disk(cfgs[0], precision, device=local_rank)
-        for f, st in enumerate(pinned[0]):
-            r2.set_state(*[p.numpy() for p in st], fluid=f)
+        for f in range(nf):
+            r2.set_state(*np_(pinned[f][0]), fluid=f)
         r2.initialize()
         r2.run(args.steps)
         outs = [r2.state(f, out=results[0][f]) for f in range(nf)]

@@ -787,8 +787,11 @@ int fb_disk_set_state(fb_disk *D, int f, const double *rho, const double *vx, co
 /* Chunked transfers for FP32 disks: the host doubles of many fields (of
  * many disks) are packed back to back into the device staging chunk and
  * converted by one launch per chunk (and the reverse for reads: one launch,
- * then the chunk's copies back to back).  Pieces of a field with a per-ring
- * background end at ring boundaries. */
+ * then the chunk's copies).  Pieces of a field with a per-ring background
+ * end at ring boundaries.  Pieces that lie back to back both in host memory
+ * and in the chunk (the fields of disks kept in one host buffer, in the
+ * order they are passed) cross in one copy: a DMA costs some microseconds
+ * besides its bytes, which dominate for the small fields of small disks. */
 typedef struct {
   fb_segs s;
   size_t fill;
@@ -796,17 +799,48 @@ typedef struct {
   cudaStream_t stream;
   int to_f32;
   double *host[FB_MAXSEG];   /* reads: where each segment's doubles go */
+  const double *pend_h;      /* uploads: the host->chunk copy not issued yet */
+  size_t pend_off, pend_n;
 } seg_chunk;
 
+static int pend_issue(seg_chunk *c) {
+  cudaError_t e;
+  if (!c->pend_n) return 0;
+  e = cudaMemcpyAsync(c->st + c->pend_off, c->pend_h, c->pend_n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  c->pend_n = 0;
+  return e != cudaSuccess;
+}
+
+/* queue n host doubles for chunk offset off, joining the pending copy when
+ * both sides continue it */
+static int pend_add(seg_chunk *c, const double *h, size_t off, size_t n) {
+  if (c->pend_n && c->pend_h + c->pend_n == h && c->pend_off + c->pend_n == off) {
+    c->pend_n += n;
+    return 0;
+  }
+  if (pend_issue(c)) return 1;
+  c->pend_h = h;
+  c->pend_off = off;
+  c->pend_n = n;
+  return 0;
+}
+
 static int chunk_flush(seg_chunk *c) {
-  int k;
+  int k, e;
   if (!c->s.n) return 0;
+  if (c->to_f32 && pend_issue(c)) return 1;
   if (fb_launch_convert_segs(c->st, &c->s, c->to_f32, c->stream) != 0) return 1;
   if (!c->to_f32)
-    for (k = 0; k < c->s.n; k++)
-      if (cudaMemcpyAsync(c->host[k], c->st + c->s.s[k].off, (size_t)c->s.s[k].n * sizeof(double),
-                          cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+    for (k = 0; k < c->s.n; k = e + 1) {
+      size_t len = (size_t)c->s.s[k].n;
+      for (e = k; e + 1 < c->s.n && c->host[e] + c->s.s[e].n == c->host[e + 1] &&
+                  c->s.s[e].off + c->s.s[e].n == c->s.s[e + 1].off;
+           e++)
+        len += (size_t)c->s.s[e + 1].n;
+      if (cudaMemcpyAsync(c->host[k], c->st + c->s.s[k].off, len * sizeof(double), cudaMemcpyDeviceToHost,
+                          c->stream) != cudaSuccess)
         return 1;
+    }
   c->s.n = 0;
   c->fill = 0;
   return 0;
@@ -829,10 +863,10 @@ static int chunk_add(seg_chunk *c, float *f, double *host, size_t n, const doubl
     }
     take = n - o < room ? n - o : room;
     if (c->to_f32) {
-      if (cudaMemcpyAsync(c->st + c->fill, host + o, take * sizeof(double), cudaMemcpyHostToDevice, c->stream) !=
-          cudaSuccess)
-        return 1;
-      if (first_bg && fb_launch_ring_mean(first_bg + o / unit, c->st + c->fill, nx, (int)(take / unit), c->stream))
+      if (pend_add(c, host + o, c->fill, take)) return 1;
+      /* the ring means read the chunk: the copy goes out first */
+      if (first_bg && (pend_issue(c) ||
+                       fb_launch_ring_mean(first_bg + o / unit, c->st + c->fill, nx, (int)(take / unit), c->stream)))
         return 1;
     } else {
       c->host[c->s.n] = host + o;

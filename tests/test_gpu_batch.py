@@ -150,6 +150,58 @@ def test_batch_state_transfers_of_all_members(precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("pinned", [False, True])
+def test_batch_transfers_through_one_host_block(pinned):
+    """Members whose fields lie back to back in one host buffer, in the
+    order of the call, cross in merged copies (more segments than one
+    staging chunk holds, so the merging restarts at chunk boundaries); the
+    state equals the one of per-member calls, and the fields read back into
+    one block equal the per-member reads."""
+    import torch
+    from fargo3d_b200 import Batch, initial_state
+    cfgs = [c.replace(seed=c.seed + 100 * k) for k in range(5) for c in small_mix()]
+    sts = [initial_state(c) for c in cfgs]
+    a, b = Batch(cfgs, "fp32"), Batch(cfgs, "fp32")
+    for i, st in enumerate(sts):
+        a.set_state(i, *st)
+    n = [int(np.prod(c.shape)) for c in cfgs]
+    blk = torch.empty(4 * sum(n), dtype=torch.float64)
+    blk = blk.pin_memory() if pinned else blk
+    blk = blk.numpy()
+    views, o = [], 0
+    for i, st in enumerate(sts):
+        v = []
+        for q in (0, 1, 2, 4):                  # rho, vx, vy, cs: the upload order of a 2D disk
+            x = blk[o:o + n[i]].reshape(cfgs[i].shape)
+            x[...] = st[q]
+            v.append(x)
+            o += n[i]
+        views.append((v[0], v[1], v[2], None, v[3]))
+    b.set_states(views)
+    a.initialize()
+    b.initialize()
+    a.run(3)
+    b.run(3)
+    out = torch.empty(3 * sum(n), dtype=torch.float64)
+    out = (out.pin_memory() if pinned else out).numpy()
+    outs, o = [], 0
+    for i, c in enumerate(cfgs):
+        d = {}
+        for k in ("rho", "vx", "vy"):
+            d[k] = out[o:o + n[i]].reshape(c.shape)
+            o += n[i]
+        outs.append(d)
+    got = b.states(out=outs)
+    for i in range(len(cfgs)):
+        want = a.state(i)
+        for k in ("rho", "vx", "vy"):
+            assert np.shares_memory(got[i][k], out)
+            assert np.array_equal(got[i][k], want[k]), (i, k)
+    a.close()
+    b.close()
+
+
+@pytest.mark.gpu
 def test_batch_failing_member_is_frozen_others_continue():
     """Fault injection on the host: one member starts with a NaN density.
     It is frozen with FB_ERR_NONFINITE; the others match their solo runs."""
