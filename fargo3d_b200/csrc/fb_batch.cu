@@ -346,6 +346,8 @@ int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_ba
     fb_disk_internal_provide(nullptr, 0, nullptr);
     if (rc) { fb_batch_destroy(B); return rc; }
   }
+  // the members' table uploads, queued on the batch's stream, waited for once
+  if (cudaStreamSynchronize(B->stream) != cudaSuccess) { fb_batch_destroy(B); return FB_ERR_CUDA; }
   *out = B;
   return FB_OK;
 }
@@ -380,6 +382,11 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
   if (B->nitems[ST_ROWSUM] == 0) return FB_OK;
   const int chunk = 10;  // steps per captured graph; a remainder runs eagerly
   if (nsteps >= chunk && (!B->exec || B->graph_steps != chunk || B->graph_dt != DT)) {
+    // the first chunk runs eagerly, so the device works while the host
+    // captures and instantiates the graph of the following ones
+    const int e0 = launch_steps(B, DT, chunk);
+    if (e0) return fb_internal_fail(FB_ERR_CUDA, "batched step launch", e0);
+    nsteps -= chunk;
     if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
     cudaGraph_t g;
     if (cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FB_ERR_CUDA;

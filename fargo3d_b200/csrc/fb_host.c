@@ -599,8 +599,12 @@ int fb_disk_create(const fb_params *p, int precision, int device, fb_disk **out)
   }
   rc = upload_geometry(D);
   if (!rc) rc = upload_tables(D);
+  /* an asynchronous copy from pageable memory has taken the bytes when it
+     returns (the image can be freed); a disk on its own stream waits for
+     the copy here, a batch's member once for all members (fb_batch_create) */
   if (!rc && D->hstage && D->hstage_hi > 0 &&
-      cudaMemcpy(D->arena, D->hstage, D->hstage_hi, cudaMemcpyHostToDevice) != cudaSuccess)
+      (cudaMemcpyAsync(D->arena, D->hstage, D->hstage_hi, cudaMemcpyHostToDevice, D->stream) != cudaSuccess ||
+       (D->stream_owned && cudaStreamSynchronize(D->stream) != cudaSuccess)))
     rc = fail(FB_ERR_CUDA, "table upload");
   free(D->hstage);
   D->hstage = NULL;
