@@ -22,6 +22,15 @@ class _Member:
         self._h, self.shape = h, shape
 
 
+def _ptr_array(addr):
+    """A C array of double pointers from addresses (None: NULL), or None when
+    every entry is NULL."""
+    if all(a is None for a in addr):
+        return None
+    arr = (C.c_void_p * len(addr))(*addr)
+    return C.cast(arr, C.POINTER(C.POINTER(C.c_double)))
+
+
 class Batch:
     """`tiles`: "table" applies the autotuner's table (fargo3d_b200/autotune.py)
     to every member whose shape it lists, None keeps the defaults."""
@@ -76,17 +85,15 @@ class Batch:
         n = len(self.cfgs)
         keep, cols = [], []
         for q in range(5):
-            col = (C.POINTER(C.c_double) * n)()
-            any_ = False
+            addr = [None] * n
             for i, st in enumerate(states):
                 a = None if st is None else st[q]
                 if a is None:
                     continue
                 a = np.ascontiguousarray(a, dtype=np.float64).reshape(self._members[i].shape)
                 keep.append(a)
-                col[i] = a.ctypes.data_as(C.POINTER(C.c_double))
-                any_ = True
-            cols.append(col if any_ else None)
+                addr[i] = a.__array_interface__["data"][0]
+            cols.append(_ptr_array(addr))
         _abi.check(_abi.lib().fb_batch_set_states(self._h, fluid, *cols))
 
     def states(self, fluid: int = 0, out=None):
@@ -97,16 +104,8 @@ class Batch:
         n = len(self.cfgs)
         res = [_out_arrays(self._members[i].shape, self.cfgs[i].nz > 1, None if out is None else out[i])
                for i in range(n)]
-        cols = []
-        for k in ("rho", "vx", "vy", "vz"):
-            col = (C.POINTER(C.c_double) * n)()
-            any_ = False
-            for i in range(n):
-                if k == "vz" and not self.cfgs[i].nz > 1:
-                    continue
-                col[i] = res[i][k].ctypes.data_as(C.POINTER(C.c_double))
-                any_ = True
-            cols.append(col if any_ else None)
+        cols = [_ptr_array([res[i][k].__array_interface__["data"][0] if (k != "vz" or self.cfgs[i].nz > 1) else None
+                            for i in range(n)]) for k in ("rho", "vx", "vy", "vz")]
         _abi.check(_abi.lib().fb_batch_get_states(self._h, fluid, *cols))
         return res
 

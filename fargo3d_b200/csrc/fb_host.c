@@ -730,7 +730,9 @@ static int get(fb_disk *D, double *dst, const void *src) {
  * field by a kernel on the disk's stream (and the reverse for reads), so a
  * page-locked caller buffer moves by DMA with no host-side conversion. */
 #define FB_MAXDEV 64
+#ifndef DSTAGE_N
 #define DSTAGE_N ((size_t)4 << 20) /* doubles per chunk (32 MB) */
+#endif
 static pthread_mutex_t g_stage_mu = PTHREAD_MUTEX_INITIALIZER;
 static double *g_dstage[FB_MAXDEV];
 

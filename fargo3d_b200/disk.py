@@ -7,6 +7,7 @@ and advances hydro steps (main.c:361-448) on the GPU.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -15,13 +16,17 @@ from .setups import DiskConfig, initial_state
 
 
 def _out_arrays(shape, is3d: bool, out):
+    """Result arrays: the caller's (``out``) or new ones.  The vz of a 2D
+    disk, when the caller gives none, is a read-only zero view (no
+    allocation)."""
     res = {}
+    size = math.prod(shape)
     for k in ("rho", "vx", "vy", "vz"):
         a = None if out is None else out.get(k)
         if a is None:
-            a = np.empty(shape) if (k != "vz" or is3d) else np.zeros(shape)
-        elif not (a.dtype == np.float64 and a.flags.c_contiguous and a.size == int(np.prod(shape))):
-            raise ValueError("out[%r] must be a C-contiguous float64 array of %d values" % (k, int(np.prod(shape))))
+            a = np.empty(shape) if (k != "vz" or is3d) else np.broadcast_to(np.float64(0.0), shape)
+        elif not (a.dtype == np.float64 and a.flags.c_contiguous and a.size == size):
+            raise ValueError("out[%r] must be a C-contiguous float64 array of %d values" % (k, size))
         elif k == "vz" and not is3d:
             a.fill(0.0)
         res[k] = a.reshape(shape)
