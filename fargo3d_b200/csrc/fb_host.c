@@ -807,6 +807,10 @@ typedef struct {
   double *host[FB_MAXSEG];   /* reads: where each segment's doubles go */
   const double *pend_h;      /* uploads: the host->chunk copy not issued yet */
   size_t pend_off, pend_n;
+  /* uploads: ring means of first backgrounds, formed from the chunk at the
+     flush (after its copy, before its conversion) */
+  struct { double *out; size_t off; int nx, nrings; } rm[FB_MAXSEG];
+  int nrm;
 } seg_chunk;
 
 static int pend_issue(seg_chunk *c) {
@@ -835,6 +839,9 @@ static int chunk_flush(seg_chunk *c) {
   int k, e;
   if (!c->s.n) return 0;
   if (c->to_f32 && pend_issue(c)) return 1;
+  for (k = 0; k < c->nrm; k++)
+    if (fb_launch_ring_mean(c->rm[k].out, c->st + c->rm[k].off, c->rm[k].nx, c->rm[k].nrings, c->stream)) return 1;
+  c->nrm = 0;
   if (fb_launch_convert_segs(c->st, &c->s, c->to_f32, c->stream) != 0) return 1;
   if (!c->to_f32)
     for (k = 0; k < c->s.n; k = e + 1) {
@@ -870,10 +877,13 @@ static int chunk_add(seg_chunk *c, float *f, double *host, size_t n, const doubl
     take = n - o < room ? n - o : room;
     if (c->to_f32) {
       if (pend_add(c, host + o, c->fill, take)) return 1;
-      /* the ring means read the chunk: the copy goes out first */
-      if (first_bg && (pend_issue(c) ||
-                       fb_launch_ring_mean(first_bg + o / unit, c->st + c->fill, nx, (int)(take / unit), c->stream)))
-        return 1;
+      if (first_bg) {   /* one piece is one segment: the list cannot overflow */
+        c->rm[c->nrm].out = first_bg + o / unit;
+        c->rm[c->nrm].off = c->fill;
+        c->rm[c->nrm].nx = nx;
+        c->rm[c->nrm].nrings = (int)(take / unit);
+        c->nrm++;
+      }
     } else {
       c->host[c->s.n] = host + o;
     }
@@ -928,8 +938,7 @@ int fb_disks_set_state(fb_disk **ds, int n, int f, const double *const *rho, con
                         first ? F->vbg : NULL))
             rc = fail(FB_ERR_CUDA, "state upload");
           else if (first) {
-            if (fb_launch_bg_diffs(&D->d, f, D->stream) != cudaSuccess) rc = fail(FB_ERR_CUDA, "state upload");
-            F->has_bg = 1;
+            F->has_bg = 2;   /* its differences follow the last flush */
           }
         } else if (cudaMemcpyAsync(dst[q], src[q], (size_t)D->ncell * sizeof(double), cudaMemcpyHostToDevice,
                                    D->stream) != cudaSuccess) {
@@ -938,6 +947,14 @@ int fb_disks_set_state(fb_disk **ds, int n, int f, const double *const *rho, con
       }
     }
     if (st && !rc && chunk_flush(&c)) rc = fail(FB_ERR_CUDA, "state upload");
+    /* the neighbour differences of the new backgrounds (every ring mean of
+       a background is formed by now) */
+    for (i = 0; i < n; i++) {
+      fb_fluid_dev *F = &ds[i]->d.fl[f];
+      if (F->has_bg != 2) continue;
+      F->has_bg = 1;
+      if (!rc && fb_launch_bg_diffs(&ds[i]->d, f, ds[i]->stream) != cudaSuccess) rc = fail(FB_ERR_CUDA, "state upload");
+    }
   }
   if (cudaStreamSynchronize(ds[0]->stream) != cudaSuccess && !rc) rc = fail(FB_ERR_CUDA, "state upload");
   if (st) stage_unlock();
