@@ -382,11 +382,15 @@ int fb_batch_run(fb_batch *B, int nsteps, double DT) {
   if (B->nitems[ST_ROWSUM] == 0) return FB_OK;
   const int chunk = 10;  // steps per captured graph; a remainder runs eagerly
   if (nsteps >= chunk && (!B->exec || B->graph_steps != chunk || B->graph_dt != DT)) {
-    // the first chunk runs eagerly, so the device works while the host
-    // captures and instantiates the graph of the following ones
-    const int e0 = launch_steps(B, DT, chunk);
-    if (e0) return fb_internal_fail(FB_ERR_CUDA, "batched step launch", e0);
-    nsteps -= chunk;
+    // a run of two chunks or more takes its first chunk eagerly, so the
+    // device works while the host captures and instantiates the graph of
+    // the following ones (a one-chunk run, e.g. the server's, replays the
+    // graph it captures)
+    if (nsteps >= 2 * chunk) {
+      const int e0 = launch_steps(B, DT, chunk);
+      if (e0) return fb_internal_fail(FB_ERR_CUDA, "batched step launch", e0);
+      nsteps -= chunk;
+    }
     if (B->exec) { cudaGraphExecDestroy(B->exec); B->exec = nullptr; }
     cudaGraph_t g;
     if (cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FB_ERR_CUDA;
