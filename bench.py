@@ -28,7 +28,7 @@ value       cell-updates/s of the whole job, device-timed with CUDA events on
             the launching stream, state resident in HBM (max over ranks)
 e2e         the same through the public API from pinned host buffers: create,
             H2D of the initial state, K steps, D2H of the final state (the
-            median of three such runs)
+            median of five such runs)
 roofline    the dominant launch group of a step against the measured HBM copy
             peak (MEASURED_PEAKS.json)
 cpu_baseline  the reference's own C sources (oracle/_ref, built from the
@@ -187,7 +187,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-E2E_REPS = 3   # end-to-end runs per bench line (the median is reported)
+E2E_REPS = 5   # end-to-end runs per bench line (the median is reported)
 
 
 def read_profile(L, fn, h, *extra):
@@ -494,8 +494,9 @@ def run_ours(args, rank, world, local_rank):
             t = max_over_ranks(t, device="cuda")
         return t
 
-    # the whole job (create, upload, K steps, read-back) three times; the
-    # median (each run's host-side set-up and PCIe timing vary by a few ms)
+    # the whole job (create, upload, K steps, read-back) E2E_REPS times; the
+    # median (a run's host-side set-up and PCIe timing vary with the load
+    # other jobs put on the shared host)
     e2e_samples = [e2e_once() for _ in range(E2E_REPS)]
     t_e2e = float(np.median(e2e_samples))
     nstored = sum(int(np.prod(c.shape)) for c in cfgs) * nf
