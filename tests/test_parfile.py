@@ -215,3 +215,26 @@ def test_round_trip(tmp_path, precision):
         assert s.precision == precision
         diff = {f.name for f in dataclasses.fields(want) if getattr(want, f.name) != getattr(s.config, f.name)}
         assert not diff, (name, diff)
+
+
+@pytest.mark.skipif(not os.environ.get("FARGO_REFERENCE"), reason="FARGO_REFERENCE (a FARGO3D tree) not set")
+def test_reference_setups():
+    """The FARGO3D tree's own setups: the three this library integrates load
+    with their stock values; the others stop on an option outside the hydro
+    step."""
+    root = os.environ["FARGO_REFERENCE"]
+    s = pf.load_setup(os.path.join(root, "setups", "fargo"))
+    c = s.config
+    assert (c.nx, c.ny, c.frame, c.omegaframe, c.indirect_term, c.log_spacing) == (384, 128, "G", 1.0005, True, False)
+    assert c.planets == [Planet(1.0, 0.001, False, False)] and c.nu == 1e-5 and c.stockholm
+    s = pf.load_setup(os.path.join(root, "setups", "fargo_multifluid"))
+    c = s.config
+    assert c.nfluids == 4 and c.invstokes == (10.0, 1.0, 0.1) and c.epsilon == 1.0 and c.dust_diffusion
+    s = pf.load_setup(os.path.join(root, "setups", "p3disof"))
+    c = s.config
+    assert c.is3d and c.spherical and (c.nx, c.ny, c.nz) == (100, 80, 40) and c.flaringindex == 0.5
+    assert c.planets[0].mass == 1e-5
+    for name in ("mri", "otvortex", "sod1d", "fargo_nu", "binary"):
+        if os.path.isdir(os.path.join(root, "setups", name)):
+            with pytest.raises(NotImplementedError):
+                pf.load_setup(os.path.join(root, "setups", name))
