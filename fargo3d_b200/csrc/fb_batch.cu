@@ -21,6 +21,9 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <atomic>
+#include <string>
+#include <thread>
 
 Prof *g_prof = nullptr;
 
@@ -339,12 +342,46 @@ int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_ba
     B->arena = nullptr;   // members allocate their own
     cudaGetLastError();
   }
+  for (int i = 0; i < n; i++)   // what fb_batch_add refuses, before any member exists
+    if ((ps[i].nz > 1) != (B->is3d != 0) || ps[i].nfluids != B->nfluids || ps[i].adiabatic || ps[i].dust_diffusion) {
+      fb_batch_destroy(B);
+      return fb_internal_fail(FB_ERR_ARG, ps[i].adiabatic || ps[i].dust_diffusion
+                                              ? "adiabatic disks and dust diffusion run on the one-disk path (fb_disk_step)"
+                                              : "batch members share dimensionality and fluid count", 0);
+    }
+  // Members are independent: their host-side set-up (mesh, libm tables, the
+  // table image and its upload on the batch's stream) runs on up to 8 host
+  // threads, each disk in its own region of the arena.
+  std::vector<fb_disk *> made(n, nullptr);
+  std::vector<int> rcs(n, 0);
+  std::vector<std::string> errs(n);
+  std::atomic<int> next(0);
+  auto work = [&]() {
+    for (int i; (i = next++) < n;) {
+      if (B->arena) fb_disk_internal_provide(B->arena + off[i], off[i + 1] - off[i], B->stream);
+      rcs[i] = fb_disk_create(&ps[i], precision, device, &made[i]);
+      fb_disk_internal_provide(nullptr, 0, nullptr);
+      if (rcs[i]) errs[i] = fb_last_error();
+    }
+  };
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = std::min(n, std::max(1, std::min(8, (int)(hw ? hw : 1))));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; t++) pool.emplace_back(work);
+  work();
+  for (auto &t : pool) t.join();
+  cudaSetDevice(device);
   for (int i = 0; i < n; i++) {
-    int s;
-    if (B->arena) fb_disk_internal_provide(B->arena + off[i], off[i + 1] - off[i], B->stream);
-    rc = fb_batch_add(B, &ps[i], 0.0, &s);
-    fb_disk_internal_provide(nullptr, 0, nullptr);
-    if (rc) { fb_batch_destroy(B); return rc; }
+    if (!rcs[i]) continue;
+    for (int k = 0; k < n; k++)
+      if (made[k]) fb_disk_destroy(made[k]);
+    fb_batch_destroy(B);
+    return fb_internal_fail(rcs[i], errs[i].c_str(), 0);
+  }
+  for (int i = 0; i < n; i++) {
+    B->disks[i] = made[i];
+    B->state[i] = 1;
+    B->t_end[i] = 0.0;
   }
   // the members' table uploads, queued on the batch's stream, waited for once
   if (cudaStreamSynchronize(B->stream) != cudaSuccess) { fb_batch_destroy(B); return FB_ERR_CUDA; }
