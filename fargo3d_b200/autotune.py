@@ -54,6 +54,9 @@ def cx_candidates(nx: int, precision: str = "fp32", is3d: bool = False):
     return out
 
 
+_DEFAULT = [None, None]   # (file modification times, table) of TileTable.default()
+
+
 class TileTable:
     def __init__(self, entries=None):
         self.entries = dict(entries or {})
@@ -69,7 +72,12 @@ class TileTable:
 
     @classmethod
     def default(cls):
-        return cls.load(SHIPPED, LOCAL)
+        """The shipped table under the machine-local one, read again only
+        when either file changes."""
+        key = tuple(os.stat(p).st_mtime_ns if os.path.exists(p) else None for p in (SHIPPED, LOCAL))
+        if _DEFAULT[0] != key:
+            _DEFAULT[:] = [key, cls.load(SHIPPED, LOCAL)]
+        return cls(_DEFAULT[1].entries)
 
     def get(self, cfg, precision: str):
         e = self.entries.get(shape_key(cfg, precision))

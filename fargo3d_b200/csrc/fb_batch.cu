@@ -367,7 +367,13 @@ int fb_batch_create(const fb_params *ps, int n, int precision, int device, fb_ba
   const unsigned hw = std::thread::hardware_concurrency();
   const int nt = std::min(n, std::max(1, std::min(8, (int)(hw ? hw : 1))));
   std::vector<std::thread> pool;
-  for (int t = 1; t < nt; t++) pool.emplace_back(work);
+  for (int t = 1; t < nt; t++) {
+    try {
+      pool.emplace_back(work);
+    } catch (...) {   // no thread to be had: the calling thread does the rest
+      break;
+    }
+  }
   work();
   for (auto &t : pool) t.join();
   cudaSetDevice(device);
