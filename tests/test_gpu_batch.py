@@ -202,6 +202,28 @@ def test_batch_transfers_through_one_host_block(pinned):
 
 
 @pytest.mark.gpu
+def test_batch_creation_refuses_a_bad_member():
+    """Members are set up on several host threads; one member the library
+    refuses fails the whole creation with that member's error text, and a
+    batch created afterwards works."""
+    from fargo3d_b200 import Batch, _abi
+    cfgs = small_mix() * 3
+    bad = cfgs[:5] + [cfgs[5].replace(planets=[], frame="G")] + cfgs[6:]
+    with pytest.raises(_abi.FargoError, match="rotating frame needs a planet"):
+        Batch(bad, "fp32")
+    with pytest.raises(_abi.FargoError, match="one-disk path"):
+        Batch(cfgs[:3] + [cfgs[3].replace(adiabatic=True, alpha_visc=True, alpha=1e-3, nu=0.0)], "fp64")
+    b = Batch(cfgs, "fp32")
+    b.load_initial_states()
+    b.initialize()
+    b.run(3)
+    b.sync()
+    for i in range(len(cfgs)):
+        assert b.scalars(i)[1] == 0
+    b.close()
+
+
+@pytest.mark.gpu
 def test_batch_failing_member_is_frozen_others_continue():
     """Fault injection on the host: one member starts with a NaN density.
     It is frozen with FB_ERR_NONFINITE; the others match their solo runs."""
